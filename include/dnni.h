@@ -1,0 +1,154 @@
+/*
+ * dnni.h -- C ABI of the B200 discrete natural-neighbour interpolation engine.
+ *
+ * This is the drop-in boundary for TerraNNI's hot path, the per-work-package
+ * call nni::performNNI (nni.h:93-95, implemented nni.cpp:870-944) together
+ * with the calls that bracket it (nni.h:83-97).  Plain pointers and sizes
+ * only; every entry point returns a dnni_status; one context per host thread.
+ *
+ * Semantics (canonical mode; the reference approximates the same quantity
+ * with GL rasterisation, nni.cpp:171-230 and nni.cpp:483-534):
+ *   - points are int32 LAS-unit coordinates (x, y, z), n x 3, row-major, with
+ *     an optional uint32 global id per point (NULL: the id is the index);
+ *   - cell (i, j) of the output grid sits at LAS position
+ *     (origin_x + i*cell_size, origin_y + j*cell_size); raster pixels use the
+ *     same lattice (the reference's `scaling` is 1);
+ *   - s(p), the nearest site of raster pixel p, minimises (d^2, gid, z) with
+ *     d^2 computed exactly in int64 (ties go to the lowest global id);
+ *   - every grid cell q with |q-p|^2 <= floor(d^2(p,s(p)) / cell_size^2)
+ *     (cell-index units) receives z(s(p)) and a count of one;
+ *   - h[q] = float((double)Z / (double)C * z_scale + z_offset), or nodata when
+ *     no pixel reaches q.  Z is an exact int64 sum, so heights are
+ *     deterministic and independent of launch order.
+ *   Output grids are row-major, nrows x ncols, row 0 = smallest y.  The site
+ *   map holds one gid per raster pixel (DNNI_NO_SITE when there are no points).
+ *
+ * Coordinates relative to (origin_x, origin_y) must lie within +-2^30 LAS
+ * units for points and raster pixels; grid and raster sides are at most
+ * 32767 cells.
+ */
+#ifndef DNNI_H
+#define DNNI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DNNI_NO_SITE 0xFFFFFFFFu
+#define DNNI_VERSION 10000
+
+typedef enum dnni_status {
+    DNNI_OK = 0,
+    DNNI_E_INVAL = 1,      /* bad argument or work package */
+    DNNI_E_NOMEM = 2,      /* device or host allocation failed / over budget */
+    DNNI_E_TIMEOUT = 3,    /* a bounded wait expired */
+    DNNI_E_CUDA = 4,       /* CUDA runtime error (see dnni_last_error) */
+    DNNI_E_RANGE = 5,      /* coordinates outside the supported range */
+    DNNI_E_STATE = 6,      /* call out of order (e.g. no setup) */
+    DNNI_E_IO = 7,         /* file could not be read / parsed */
+    DNNI_E_CANCELLED = 8,  /* request cancelled before completion */
+    DNNI_E_BUSY = 9        /* admission refused: no slot or memory free now */
+} dnni_status;
+
+typedef struct dnni_ctx dnni_ctx;
+
+/* Replaces nni::Settings (nni.h:72-81) for the engine.  The reference's
+ * scale/site_radius/query_radius/zMultiplier fields have no counterpart in
+ * canonical mode (scaling 1, unbounded discs, exact int64 sums). */
+typedef struct dnni_settings {
+    int32_t device;         /* CUDA device ordinal */
+    int32_t small_radius;   /* pixels with floor(d^2/cell^2) <= r^2 use the
+                               per-tile stencil, others the span scatter;
+                               1..6, 0 = default (3) */
+    int32_t bin_target;     /* mean points per search bin; 0 = default (2) */
+    int32_t flags;          /* DNNI_F_* */
+    uint64_t mem_budget;    /* bytes of device scratch a context may hold;
+                               0 = no limit */
+} dnni_settings;
+
+#define DNNI_F_TIMING 1     /* record per-phase CUDA-event times in dnni_stats */
+
+/* One work package: the output grid and the raster of pixels that scatter
+ * into it.  Replaces nni::WorkPackage (nni.h:66-70), whose float origins are
+ * replaced by int32 LAS units.  raster_* are cell indices relative to cell
+ * (0,0), half-open; all four zero means "the grid itself". */
+typedef struct dnni_workpackage {
+    int32_t ncols, nrows;
+    int32_t cell_size;              /* LAS units per cell edge, > 0 */
+    int32_t origin_x, origin_y;     /* LAS position of cell (0,0) */
+    int32_t raster_x0, raster_y0, raster_x1, raster_y1;
+    int32_t pad0;
+    double z_scale, z_offset;       /* metres = z_scale * LAS z + z_offset */
+    float nodata;                   /* value for cells no pixel reaches */
+    int32_t pad1;
+} dnni_workpackage;
+
+typedef struct dnni_stats {
+    double ms_total;        /* device time of the call (CUDA events) */
+    double ms_bin, ms_nearest, ms_scatter, ms_finalize;
+    int64_t n_points, n_cells, n_pixels;
+    int64_t big_pixels;     /* pixels scattered by the span path */
+    int64_t spans;          /* row spans those pixels cover (unclipped) */
+    int64_t nodata_cells;
+    int64_t h2d_bytes, d2h_bytes;
+    int32_t max_r2;         /* largest floor(d^2/cell^2) over the raster */
+    int32_t packed;         /* 1 when (Z,C) shared one 64-bit accumulator */
+    int32_t bin_size;       /* search-bin edge chosen, LAS units */
+    int32_t pad;
+} dnni_stats;
+
+/* ---- lifecycle: nni::init / nni::cleanup (nni.h:83-85, nni.cpp:563-598) ---- */
+
+int32_t dnni_version(void);
+/* Create a context bound to settings->device (NULL settings: defaults). */
+dnni_status dnni_init(const dnni_settings *settings, dnni_ctx **out);
+/* Release every device and host resource of the context. */
+dnni_status dnni_destroy(dnni_ctx *ctx);
+/* Message for the last failing call on this context ("" if none). */
+const char *dnni_last_error(const dnni_ctx *ctx);
+
+/* ---- per work package: nni::setupRun (nni.h:91, nni.cpp:601-668) ---- */
+
+/* Optional: reserve device scratch for work packages up to this size and
+ * point count, so that the first interpolate call does not allocate. */
+dnni_status dnni_setup_run(dnni_ctx *ctx, const dnni_workpackage *wp, int64_t max_points);
+
+/* ---- hot path: nni::performNNI (nni.h:93-95, nni.cpp:870-944) ---- */
+
+/* Host buffers: copies the points in, interpolates, copies h (nrows*ncols
+ * floats) and, if out_site is not NULL, the site map (raster pixels) out.
+ * Returns after the results are in host memory. */
+dnni_status dnni_interpolate_segment(dnni_ctx *ctx, const dnni_workpackage *wp,
+                                     const int32_t *xyz, const uint32_t *gid, int64_t n,
+                                     float *out_h, uint32_t *out_site, dnni_stats *stats);
+
+/* Device buffers on the context's device.  Work is queued on `stream`
+ * (a cudaStream_t; NULL = the context's own stream).  The call synchronises
+ * once, after the point bounding box, to size the search bins; it returns
+ * with the remaining work queued unless stats is non-NULL, in which case it
+ * waits for completion to fill the counters. */
+dnni_status dnni_interpolate_segment_device(dnni_ctx *ctx, const dnni_workpackage *wp,
+                                            const int32_t *d_xyz, const uint32_t *d_gid, int64_t n,
+                                            float *d_h, uint32_t *d_site, void *stream,
+                                            dnni_stats *stats);
+
+/* ---- nni::clearRenderbuffers / nni::printTimes (nni.h:87-97) ---- */
+
+/* Free the context's scratch (it is re-created on demand). */
+dnni_status dnni_clear(dnni_ctx *ctx);
+/* Print accumulated per-phase device times to stdout (needs DNNI_F_TIMING). */
+dnni_status dnni_print_times(dnni_ctx *ctx);
+
+/* ---- pinned host memory for the host-buffer entry points ---- */
+
+dnni_status dnni_host_alloc(size_t bytes, void **out);
+dnni_status dnni_host_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DNNI_H */

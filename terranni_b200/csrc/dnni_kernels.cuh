@@ -1,0 +1,666 @@
+// dnni_kernels.cuh -- sm_100a kernels of the discrete natural-neighbour
+// interpolation hot path (one work package per launch sequence).
+//
+// Replaces, per work package:
+//   nni.cpp:722-790 renderInputPoints / nni.cpp:171-230 drawPlane (the GL
+//     depth-tested site planes that leave each pixel's nearest site in the
+//     colour buffer)                       -> k_bin_* + k_nearest
+//   nni.cpp:794-820 performNNIQueries / nni.cpp:483-534 makeBlocks and
+//     cuda_nni.cu:407-488 calcNNI (query planes OR-blended into bit masks,
+//     then per-pixel int32 atomics)        -> k_scatter_spans + k_final stencil
+//   cuda_nni.cu:491-503 divide, cuda_nni.cu:399-402 zeroValues
+//                                          -> k_rowscan + k_final
+//
+// Data layout in HBM (per call):
+//   sorted points  int4 {x-ox, y-oy, z, gid}, grouped by search bin;
+//   bin starts     int32 [nbins+1], bins ordered superblock (64x64 bins) ->
+//                  block (8x8 bins) -> bin, so any bin, block or superblock is
+//                  one contiguous point range;
+//   pixel records  int2 {z of nearest site, R2 = floor(d^2/cell^2)} per
+//                  raster pixel (R2 = -1: no site);
+//   span sums      one 64-bit word per grid cell holding (Zrel << K) + C, or
+//                  int64 Z plus int32 C when the packed form cannot hold the
+//                  largest possible per-cell sums.
+#pragma once
+
+#include <climits>
+#include <cstdint>
+#include <cstdlib>
+#include <cmath>
+#include <cuda_runtime.h>
+
+// Helpers below are __host__ __device__ so that a host build of the same code
+// can be checked against the CPU oracle without a GPU.
+#ifdef __CUDA_ARCH__
+#define DNNI_LDG(p) __ldg(p)
+#else
+#define DNNI_LDG(p) (*(p))
+#endif
+#define DNNI_HD __host__ __device__ __forceinline__
+
+namespace dnni {
+
+constexpr int kBinsPerBlockEdge = 8;      // bins per block edge
+constexpr int kBinsPerSuperEdge = 64;     // bins per superblock edge
+constexpr int kBinsPerBlock = 64;
+constexpr int kBinsPerSuper = 4096;
+constexpr int kRingsBins = 2;             // bin rings searched before blocks
+constexpr int kRingsBlocks = 1;           // block rings searched before superblocks
+constexpr int kMaxSmallRadius = 6;
+constexpr int kStatSlots = 32;
+constexpr long long kCoordLimit = 1LL << 30;
+constexpr long long kDistCap = (1LL << 31) - 1;
+
+enum ErrBits { kErrRange = 1 };
+
+struct BinGrid {
+    int32_t gx0, gy0;    // bin grid origin, LAS units relative to the WP origin
+    int32_t bs;          // bin edge, LAS units
+    int32_t nbx, nby;    // bins per axis, multiples of 64
+    int32_t n2x, n2y;    // superblocks per axis
+    int32_t pad;
+    int64_t nbins;
+};
+
+struct TileParams {
+    int32_t ncols, nrows, cs;
+    int32_t ox, oy;              // absolute LAS origin of cell (0,0)
+    int32_t rx0, ry0, rw, rh;    // raster origin (cell index) and size
+    int32_t r2cap;               // no pixel/cell pair is farther apart (cell units^2)
+    int32_t rs;                  // small-disc radius of the stencil path
+    int32_t has_gid;
+    int64_t npts;
+    double z_scale, z_offset;
+    float nodata;
+    int32_t pad;
+    BinGrid bg;
+};
+
+struct Scalars {
+    int32_t bbox[6];             // min/max of x-ox, y-oy, z
+    int32_t err;
+    int32_t packed;              // decided after the nearest-site pass
+    int32_t kbits;
+    int32_t pad;
+    long long zbase;
+    int32_t max_r2[kStatSlots];
+    unsigned long long big_pixels[kStatSlots];
+    unsigned long long spans[kStatSlots];
+    unsigned long long nodata[kStatSlots];
+};
+
+// ---------------------------------------------------------------------------
+// small device helpers
+// ---------------------------------------------------------------------------
+
+DNNI_HD int isqrt_i32(int v) {
+    // floor(sqrt(v)) for 0 <= v < 2^31: float estimate, exact integer fix-up
+    int s = (int)sqrtf((float)v);
+    while ((long long)s * s > v) --s;
+    while ((long long)(s + 1) * (s + 1) <= v) ++s;
+    return s;
+}
+
+DNNI_HD int64_t bin_id(const BinGrid& g, int bx, int by) {
+    const int sx = bx >> 6, sy = by >> 6;
+    const int bkx = (bx >> 3) & 7, bky = (by >> 3) & 7;
+    const int lx = bx & 7, ly = by & 7;
+    return ((int64_t)(sy * g.n2x + sx) << 12) | (int64_t)(((bky << 3) | bkx) << 6) | (int64_t)((ly << 3) | lx);
+}
+
+DNNI_HD int rel_coord(int32_t a, int32_t o) {
+    // a - o, exact when the true difference fits in int32 (checked by k_bbox)
+    return (int)((uint32_t)a - (uint32_t)o);
+}
+
+struct Best {
+    long long d2;
+    uint32_t gid;
+    int z;
+};
+
+DNNI_HD void consider(Best& b, const int4 p, int px, int py) {
+    const int dx = p.x - px, dy = p.y - py;      // |p.x|, |px| < 2^30
+    const long long d2 = (long long)dx * dx + (long long)dy * dy;
+    const uint32_t g = (uint32_t)p.w;
+    if (d2 < b.d2 || (d2 == b.d2 && (g < b.gid || (g == b.gid && p.z < b.z)))) {
+        b.d2 = d2;
+        b.gid = g;
+        b.z = p.z;
+    }
+}
+
+DNNI_HD long long axis_gap(long long p, long long lo, long long hi) {
+    long long d = p < lo ? lo - p : (p > hi ? p - hi : 0);
+    return d < kDistCap ? d : kDistCap;
+}
+
+// squared distance lower bound from (px,py) to the box [x0,x1] x [y0,y1]
+DNNI_HD long long box_lb(long long px, long long py, long long x0, long long x1,
+                                            long long y0, long long y1) {
+    const long long dx = axis_gap(px, x0, x1), dy = axis_gap(py, y0, y1);
+    return dx * dx + dy * dy;
+}
+
+// Cell e (0 <= e < ring_size(k)) of the Chebyshev ring k around (cx,cy):
+// bottom row, top row, then the left/right columns in between.
+DNNI_HD int ring_size(int k) { return k ? 8 * k : 1; }
+
+DNNI_HD void ring_cell(int cx, int cy, int k, int e, int& x, int& y) {
+    const int side = 2 * k + 1;
+    if (e < side) {
+        x = cx - k + e;
+        y = cy - k;
+    } else if (e < 2 * side) {
+        x = cx - k + (e - side);
+        y = cy + k;
+    } else {
+        const int f = e - 2 * side;
+        x = (f & 1) ? cx + k : cx - k;
+        y = cy - k + 1 + (f >> 1);
+    }
+}
+
+// After visiting every cell of the (unclipped) box [x0,x1]x[y0,y1] of a level
+// whose cells are u LAS units wide, every unvisited point lies at distance
+// >= m from (px,py); the search may stop once best < m^2.  Sides at the grid
+// border are closed (nothing lies beyond them).
+DNNI_HD bool ring_done(long long best, long long px, long long py, long long gx0,
+                                          long long gy0, long long u, int x0, int x1, int y0, int y1,
+                                          int nx, int ny) {
+    long long m = LLONG_MAX;
+    bool open = false;
+    if (x0 > 0) { long long v = px - (gx0 + (long long)x0 * u) + 1; m = v < m ? v : m; open = true; }
+    if (x1 < nx - 1) { long long v = gx0 + (long long)(x1 + 1) * u - px; m = v < m ? v : m; open = true; }
+    if (y0 > 0) { long long v = py - (gy0 + (long long)y0 * u) + 1; m = v < m ? v : m; open = true; }
+    if (y1 < ny - 1) { long long v = gy0 + (long long)(y1 + 1) * u - py; m = v < m ? v : m; open = true; }
+    if (!open) return true;
+    if (m > kDistCap) m = kDistCap;
+    return best < m * m;
+}
+
+DNNI_HD void scan_points(Best& b, const int4* __restrict__ pts, int s, int e, int px, int py) {
+    for (int q = s; q < e; ++q) consider(b, DNNI_LDG(&pts[q]), px, py);
+}
+
+// Exact nearest site of the pixel at (px,py) (LAS units relative to the WP
+// origin): bin rings, then block rings, then superblock rings, each level
+// pruned by box lower bounds and empty ranges, each stopping on ring_done.
+__host__ __device__ inline void nearest_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                               int px, int py, Best& b) {
+    const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    int bx = (int)(((long long)px - gx0) / bs);
+    int by = (int)(((long long)py - gy0) / bs);
+    bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
+    by = by < g.nby - 1 ? by : g.nby - 1;
+
+    // level 0: bins
+    for (int k = 0; k <= kRingsBins; ++k) {
+        const int ne = ring_size(k);
+        for (int e = 0; e < ne; ++e) {
+            int x, y;
+            ring_cell(bx, by, k, e, x, y);
+            if (x < 0 || y < 0 || x >= g.nbx || y >= g.nby) continue;
+            const long long X0 = gx0 + (long long)x * bs, Y0 = gy0 + (long long)y * bs;
+            if (k > 0 && box_lb(px, py, X0, X0 + bs - 1, Y0, Y0 + bs - 1) > b.d2) continue;
+            const int64_t id = bin_id(g, x, y);
+            scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
+        }
+        if (ring_done(b.d2, px, py, gx0, gy0, bs, bx - k, bx + k, by - k, by + k, g.nbx, g.nby)) return;
+    }
+
+    // level 1: blocks of 8x8 bins
+    const int n1x = g.nbx >> 3, n1y = g.nby >> 3, c1x = bx >> 3, c1y = by >> 3;
+    const long long u1 = bs * kBinsPerBlockEdge;
+    for (int K = 0; K <= kRingsBlocks; ++K) {
+        const int ne = ring_size(K);
+        for (int e = 0; e < ne; ++e) {
+            int x, y;
+            ring_cell(c1x, c1y, K, e, x, y);
+            if (x < 0 || y < 0 || x >= n1x || y >= n1y) continue;
+            const long long X0 = gx0 + (long long)x * u1, Y0 = gy0 + (long long)y * u1;
+            if (box_lb(px, py, X0, X0 + u1 - 1, Y0, Y0 + u1 - 1) > b.d2) continue;
+            const int64_t first = bin_id(g, x * 8, y * 8);
+            if (DNNI_LDG(&start[first]) == DNNI_LDG(&start[first + kBinsPerBlock])) continue;
+            for (int l = 0; l < kBinsPerBlock; ++l) {
+                const int gbx = x * 8 + (l & 7), gby = y * 8 + (l >> 3);
+                if (abs(gbx - bx) <= kRingsBins && abs(gby - by) <= kRingsBins) continue;
+                const long long BX0 = gx0 + (long long)gbx * bs, BY0 = gy0 + (long long)gby * bs;
+                if (box_lb(px, py, BX0, BX0 + bs - 1, BY0, BY0 + bs - 1) > b.d2) continue;
+                const int64_t id = first + l;
+                scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
+            }
+        }
+        if (ring_done(b.d2, px, py, gx0, gy0, u1, c1x - K, c1x + K, c1y - K, c1y + K, n1x, n1y)) return;
+    }
+
+    // level 2: superblocks of 8x8 blocks
+    const int c2x = bx >> 6, c2y = by >> 6;
+    const long long u2 = bs * kBinsPerSuperEdge;
+    for (int K = 0;; ++K) {
+        const int ne = ring_size(K);
+        for (int e = 0; e < ne; ++e) {
+            int x, y;
+            ring_cell(c2x, c2y, K, e, x, y);
+            if (x < 0 || y < 0 || x >= g.n2x || y >= g.n2y) continue;
+            const long long X0 = gx0 + (long long)x * u2, Y0 = gy0 + (long long)y * u2;
+            if (box_lb(px, py, X0, X0 + u2 - 1, Y0, Y0 + u2 - 1) > b.d2) continue;
+            const int64_t sfirst = (int64_t)(y * g.n2x + x) << 12;
+            if (DNNI_LDG(&start[sfirst]) == DNNI_LDG(&start[sfirst + kBinsPerSuper])) continue;
+            for (int m = 0; m < 64; ++m) {
+                const int gcx = x * 8 + (m & 7), gcy = y * 8 + (m >> 3);
+                if (abs(gcx - c1x) <= kRingsBlocks && abs(gcy - c1y) <= kRingsBlocks) continue;
+                const long long CX0 = gx0 + (long long)gcx * u1, CY0 = gy0 + (long long)gcy * u1;
+                if (box_lb(px, py, CX0, CX0 + u1 - 1, CY0, CY0 + u1 - 1) > b.d2) continue;
+                const int64_t first = sfirst + ((int64_t)m << 6);
+                if (DNNI_LDG(&start[first]) == DNNI_LDG(&start[first + kBinsPerBlock])) continue;
+                for (int l = 0; l < kBinsPerBlock; ++l) {
+                    const long long BX0 = CX0 + (long long)(l & 7) * bs, BY0 = CY0 + (long long)(l >> 3) * bs;
+                    if (box_lb(px, py, BX0, BX0 + bs - 1, BY0, BY0 + bs - 1) > b.d2) continue;
+                    const int64_t id = first + l;
+                    scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
+                }
+            }
+        }
+        if (ring_done(b.d2, px, py, gx0, gy0, u2, c2x - K, c2x + K, c2y - K, c2y + K, g.n2x, g.n2y)) return;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+__global__ void k_init_scalars(Scalars* sc) {
+    const int l = threadIdx.x;
+    if (l == 0) {
+        sc->bbox[0] = INT_MAX; sc->bbox[1] = INT_MIN;
+        sc->bbox[2] = INT_MAX; sc->bbox[3] = INT_MIN;
+        sc->bbox[4] = INT_MAX; sc->bbox[5] = INT_MIN;
+        sc->err = 0; sc->packed = 0; sc->kbits = 0; sc->zbase = 0;
+    }
+    if (l < kStatSlots) {
+        sc->max_r2[l] = -1; sc->big_pixels[l] = 0; sc->spans[l] = 0; sc->nodata[l] = 0;
+    }
+}
+
+// Bounding box of the points relative to the WP origin, with range checks.
+__global__ void k_bbox(const int32_t* __restrict__ xyz, int64_t n, int32_t ox, int32_t oy, Scalars* sc) {
+    int mnx = INT_MAX, mxx = INT_MIN, mny = INT_MAX, mxy = INT_MIN, mnz = INT_MAX, mxz = INT_MIN;
+    unsigned bad = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const long long x = (long long)xyz[3 * i] - ox, y = (long long)xyz[3 * i + 1] - oy;
+        const long long z = xyz[3 * i + 2];
+        if (x <= -kCoordLimit || x >= kCoordLimit || y <= -kCoordLimit || y >= kCoordLimit ||
+            z <= -kCoordLimit || z >= kCoordLimit) {
+            bad = 1;
+            continue;
+        }
+        mnx = min(mnx, (int)x); mxx = max(mxx, (int)x);
+        mny = min(mny, (int)y); mxy = max(mxy, (int)y);
+        mnz = min(mnz, (int)z); mxz = max(mxz, (int)z);
+    }
+    mnx = __reduce_min_sync(0xffffffffu, mnx); mxx = __reduce_max_sync(0xffffffffu, mxx);
+    mny = __reduce_min_sync(0xffffffffu, mny); mxy = __reduce_max_sync(0xffffffffu, mxy);
+    mnz = __reduce_min_sync(0xffffffffu, mnz); mxz = __reduce_max_sync(0xffffffffu, mxz);
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&sc->bbox[0], mnx); atomicMax(&sc->bbox[1], mxx);
+        atomicMin(&sc->bbox[2], mny); atomicMax(&sc->bbox[3], mxy);
+        atomicMin(&sc->bbox[4], mnz); atomicMax(&sc->bbox[5], mxz);
+        if (bad) atomicOr(&sc->err, kErrRange);
+    }
+}
+
+DNNI_HD int64_t point_bin(const BinGrid& g, int xr, int yr) {
+    int bx = (int)((uint32_t)(xr - g.gx0) / (uint32_t)g.bs);
+    int by = (int)((uint32_t)(yr - g.gy0) / (uint32_t)g.bs);
+    bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
+    by = by < g.nby - 1 ? by : g.nby - 1;
+    return bin_id(g, bx, by);
+}
+
+// Counting-sort pass 1: per-bin counts; each point keeps its rank in its bin.
+__global__ void k_bin_count(const int32_t* __restrict__ xyz, int64_t n, int32_t ox, int32_t oy, BinGrid g,
+                            int* __restrict__ cnt, int* __restrict__ rank) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int xr = rel_coord(xyz[3 * i], ox), yr = rel_coord(xyz[3 * i + 1], oy);
+        rank[i] = atomicAdd(&cnt[point_bin(g, xr, yr)], 1);
+    }
+}
+
+// Counting-sort pass 3: place every point at start[bin] + rank.
+__global__ void k_bin_scatter(const int32_t* __restrict__ xyz, const uint32_t* __restrict__ gid, int64_t n,
+                              int32_t ox, int32_t oy, BinGrid g, const int* __restrict__ start,
+                              const int* __restrict__ rank, int4* __restrict__ sorted) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int xr = rel_coord(xyz[3 * i], ox), yr = rel_coord(xyz[3 * i + 1], oy);
+        const int pos = start[point_bin(g, xr, yr)] + rank[i];
+        sorted[pos] = make_int4(xr, yr, xyz[3 * i + 2], (int)(gid ? gid[i] : (uint32_t)i));
+    }
+}
+
+// ---- exclusive scan of the bin counts (three passes, 4096 items per block) ----
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <typename T>
+__device__ __forceinline__ T block_exclusive_sum(T v, T* wsum, T& total) {
+    // blockDim.x == kScanThreads (8 warps)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < 8 ? wsum[lane] : T(0);
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            T y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < 8) wsum[lane] = w;
+    }
+    __syncthreads();
+    total = wsum[7];
+    const T excl = x - v + (warp ? wsum[warp - 1] : T(0));
+    __syncthreads();
+    return excl;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_partial(const int* __restrict__ cnt, int64_t m, int* __restrict__ bsum) {
+    __shared__ int wsum[8];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t idx = base + k * kScanThreads + threadIdx.x;
+        if (idx < m) s += cnt[idx];
+    }
+    int total;
+    block_exclusive_sum(s, wsum, total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_bsum(int* __restrict__ bsum, int nb) {
+    __shared__ int wsum[32];
+    const int per = (nb + 1023) / 1024;
+    const int b0 = threadIdx.x * per;
+    int s = 0;
+    for (int k = 0; k < per; ++k) if (b0 + k < nb) s += bsum[b0 + k];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = s;
+    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, w, o); if (lane >= o) w += y; }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    int run = x - s + (warp ? wsum[warp - 1] : 0);
+    for (int k = 0; k < per; ++k)
+        if (b0 + k < nb) { const int v = bsum[b0 + k]; bsum[b0 + k] = run; run += v; }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restrict__ cnt, int64_t m,
+                                                             const int* __restrict__ bsum, int* __restrict__ start) {
+    __shared__ int tile[kScanTile];
+    __shared__ int wsum[8];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int li = k * kScanThreads + threadIdx.x;
+        const int64_t idx = base + li;
+        tile[li] = idx < m ? cnt[idx] : 0;
+    }
+    __syncthreads();
+    int v[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) { v[k] = tile[threadIdx.x * kScanItems + k]; s += v[k]; }
+    int total;
+    int run = block_exclusive_sum(s, wsum, total) + bsum[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) { tile[threadIdx.x * kScanItems + k] = run; run += v[k]; }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int li = k * kScanThreads + threadIdx.x;
+        const int64_t idx = base + li;
+        if (idx < m) start[idx] = tile[li];
+    }
+}
+
+// ---- nearest site per raster pixel ----
+
+// Block 32x8: each warp is 32 consecutive pixels of one raster row.
+__global__ void __launch_bounds__(256) k_nearest(TileParams t, const int4* __restrict__ pts,
+                                                 const int* __restrict__ start, int2* __restrict__ pix,
+                                                 uint32_t* __restrict__ site, Scalars* __restrict__ sc) {
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    const bool valid = i < t.rw && j < t.rh;
+    int R2 = -1, z = 0;
+    uint32_t gid = 0xFFFFFFFFu;
+    if (valid && t.npts > 0) {
+        const int px = (t.rx0 + i) * t.cs;
+        const int py = (t.ry0 + j) * t.cs;
+        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX};
+        nearest_search(t.bg, pts, start, px, py, b);
+        const long long q = b.d2 / ((long long)t.cs * t.cs);
+        R2 = (int)(q < t.r2cap ? q : t.r2cap);
+        z = b.z;
+        gid = b.gid;
+    }
+    if (valid) {
+        const int64_t o = (int64_t)j * t.rw + i;
+        pix[o] = make_int2(z, R2);
+        if (site) site[o] = gid;
+    }
+    const int rs2 = t.rs * t.rs;
+    const unsigned big = (R2 > rs2) ? 1u : 0u;
+    const unsigned sp = big ? 2u * (unsigned)isqrt_i32(R2) + 1u : 0u;
+    const unsigned nbig = __reduce_add_sync(0xffffffffu, big);
+    const unsigned nsp = __reduce_add_sync(0xffffffffu, sp);
+    const int mx = __reduce_max_sync(0xffffffffu, R2);
+    if (threadIdx.x == 0) {
+        const int slot = (blockIdx.x + blockIdx.y * 7 + threadIdx.y) & (kStatSlots - 1);
+        if (nbig) { atomicAdd(&sc->big_pixels[slot], (unsigned long long)nbig); atomicAdd(&sc->spans[slot], (unsigned long long)nsp); }
+        if (mx >= 0) atomicMax(&sc->max_r2[slot], mx);
+    }
+}
+
+// Picks the accumulator form for the span path.  The per-cell count from big
+// discs is at most the lattice points of a disc of radius^2 max_r2, (2r+1)^2,
+// and at most the raster size; z enters relative to zbase (the mid-range),
+// so |Zrel| <= C * zabs.  Packed: word = (Zrel << K) + C with C < 2^K and
+// |Zrel| < 2^(62-K); otherwise separate int64 Z and int32 C.
+DNNI_HD void decide_packing(int max_r2, long long npix, long long zmin, long long zmax, int& packed, int& K,
+                            long long& zbase) {
+    long long cb = 0;
+    if (max_r2 >= 0) {
+        const long long r = isqrt_i32(max_r2);
+        cb = (2 * r + 1) * (2 * r + 1);
+        if (cb > npix) cb = npix;
+    }
+    K = 1;
+    while (K < 62 && (1LL << K) <= cb) ++K;
+    zbase = 0;
+    long long zabs = 0;
+    if (zmin <= zmax) {
+        zbase = (zmin + zmax) >> 1;
+        zabs = (zmax - zbase) > (zbase - zmin) ? (zmax - zbase) : (zbase - zmin);
+    }
+    packed = (K <= 40 && cb * zabs < (1LL << (62 - K))) ? 1 : 0;
+}
+
+DNNI_HD unsigned long long span_word(int z, long long zbase, int K) {
+    return ((unsigned long long)((long long)z - zbase) << K) + 1ull;
+}
+
+DNNI_HD void decode_span_word(unsigned long long w, int K, long long zbase, long long& Z, long long& C) {
+    const long long cb = (long long)(w & ((1ull << K) - 1ull));
+    const long long zrel = ((long long)(w - (unsigned long long)cb)) >> K;
+    Z = zrel + cb * zbase;
+    C = cb;
+}
+
+__global__ void k_decide(Scalars* sc, long long npix) {
+    const int l = threadIdx.x;
+    int mx = sc->max_r2[l];
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (l == 0) {
+        int packed, K;
+        long long zbase;
+        decide_packing(mx, npix, sc->bbox[4], sc->bbox[5], packed, K, zbase);
+        sc->packed = packed;
+        sc->kbits = K;
+        sc->zbase = zbase;
+    }
+}
+
+__device__ __forceinline__ void emit_span(int row, int a, int b, int ncols, int nrows, bool packed,
+                                          unsigned long long v, long long z,
+                                          unsigned long long* __restrict__ D, int* __restrict__ Dc) {
+    if (row < 0 || row >= nrows) return;
+    a = a > 0 ? a : 0;
+    b = b < ncols - 1 ? b : ncols - 1;
+    if (a > b) return;
+    const int64_t base = (int64_t)row * ncols;
+    if (packed) {
+        atomicAdd(&D[base + a], v);
+        if (b + 1 < ncols) atomicAdd(&D[base + b + 1], (unsigned long long)(-(long long)v));
+    } else {
+        atomicAdd(&D[base + a], (unsigned long long)z);
+        atomicAdd(&Dc[base + a], 1);
+        if (b + 1 < ncols) {
+            atomicAdd(&D[base + b + 1], (unsigned long long)(-z));
+            atomicAdd(&Dc[base + b + 1], -1);
+        }
+    }
+}
+
+// Span path: every pixel with R2 > rs^2 adds its disc as row spans
+// (+v at the first cell, -v after the last) to the per-row difference array.
+// Warp = 32 consecutive pixels of one raster row, so one iteration's markers
+// fall on two rows near each other in memory.
+__global__ void __launch_bounds__(256) k_scatter_spans(TileParams t, const int2* __restrict__ pix,
+                                                       const Scalars* __restrict__ sc,
+                                                       unsigned long long* __restrict__ D, int* __restrict__ Dc) {
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    int R2 = -1, z = 0;
+    if (i < t.rw && j < t.rh) {
+        const int2 r = pix[(int64_t)j * t.rw + i];
+        z = r.x;
+        R2 = r.y;
+    }
+    const bool big = R2 > t.rs * t.rs;
+    if (!__any_sync(0xffffffffu, big)) return;
+    const int r = big ? isqrt_i32(R2) : -1;
+    const int rmax = __reduce_max_sync(0xffffffffu, r);
+    const bool packed = sc->packed != 0;
+    const int K = sc->kbits;
+    const unsigned long long v = span_word(z, sc->zbase, K);
+    const int px = t.rx0 + i, py = t.ry0 + j;
+    int w = r;
+    for (int dy = 0; dy <= rmax; ++dy) {
+        if (dy <= r) {
+            const long long t2 = (long long)R2 - (long long)dy * dy;
+            while ((long long)w * w > t2) --w;
+            emit_span(py + dy, px - w, px + w, t.ncols, t.nrows, packed, v, z, D, Dc);
+            if (dy) emit_span(py - dy, px - w, px + w, t.ncols, t.nrows, packed, v, z, D, Dc);
+        }
+    }
+}
+
+// In-place inclusive prefix along each grid row.  which: 0 = the 64-bit
+// words (always), 1 = the int32 counts (only when not packed).
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) k_rowscan(T* __restrict__ D, int ncols, const Scalars* __restrict__ sc,
+                                                          int which) {
+    if (which == 1 && sc->packed) return;
+    __shared__ T wsum[8];
+    T* row = D + (int64_t)blockIdx.x * ncols;
+    T carry = 0;
+    for (int base = 0; base < ncols; base += kScanThreads * 4) {
+        const int idx = base + threadIdx.x * 4;
+        T v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = (idx + k < ncols) ? row[idx + k] : T(0);
+        v[1] += v[0]; v[2] += v[1]; v[3] += v[2];
+        T total;
+        const T excl = block_exclusive_sum(v[3], wsum, total) + carry;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) if (idx + k < ncols) row[idx + k] = v[k] + excl;
+        carry += total;
+    }
+}
+
+__device__ __forceinline__ float finalize_height(long long Z, long long C, double zs, double zo, float nodata) {
+    if (C <= 0) return nodata;
+    const double q = __ddiv_rn(__ll2double_rn(Z), __ll2double_rn(C));
+    return __double2float_rn(__dadd_rn(__dmul_rn(q, zs), zo));
+}
+
+// Stencil path + finalize: each cell gathers the small discs (R2 <= H^2) of
+// the pixels within H, adds the prefix-summed span words, and divides.
+template <int H>
+__global__ void __launch_bounds__(512) k_final(TileParams t, const int2* __restrict__ pix,
+                                               Scalars* __restrict__ sc,
+                                               const unsigned long long* __restrict__ S,
+                                               const int* __restrict__ Sc, float* __restrict__ h) {
+    constexpr int TX = 32, TY = 16, SW = TX + 2 * H, SH = TY + 2 * H;
+    __shared__ int2 tile[SH][SW];
+    const int cx0 = blockIdx.x * TX, cy0 = blockIdx.y * TY;
+    for (int idx = threadIdx.y * TX + threadIdx.x; idx < SW * SH; idx += TX * TY) {
+        const int ly = idx / SW, lx = idx - ly * SW;
+        const int rxi = cx0 - H + lx - t.rx0, ryi = cy0 - H + ly - t.ry0;
+        int2 v = make_int2(0, -1);
+        if (rxi >= 0 && rxi < t.rw && ryi >= 0 && ryi < t.rh) v = pix[(int64_t)ryi * t.rw + rxi];
+        tile[ly][lx] = v;
+    }
+    __syncthreads();
+    const int qx = cx0 + threadIdx.x, qy = cy0 + threadIdx.y;
+    const bool in = qx < t.ncols && qy < t.nrows;
+    long long Z = 0, C = 0;
+#pragma unroll
+    for (int dy = -H; dy <= H; ++dy)
+#pragma unroll
+        for (int dx = -H; dx <= H; ++dx) {
+            if (dx * dx + dy * dy > H * H) continue;
+            const int2 p = tile[threadIdx.y + H + dy][threadIdx.x + H + dx];
+            if (p.y >= dx * dx + dy * dy && p.y <= H * H) { Z += p.x; C += 1; }
+        }
+    unsigned nod = 0;
+    if (in) {
+        const int64_t q = (int64_t)qy * t.ncols + qx;
+        const unsigned long long w = S[q];
+        if (sc->packed) {
+            long long zb, cb;
+            decode_span_word(w, sc->kbits, sc->zbase, zb, cb);
+            Z += zb;
+            C += cb;
+        } else {
+            Z += (long long)w;
+            C += Sc[q];
+        }
+        const float hv = finalize_height(Z, C, t.z_scale, t.z_offset, t.nodata);
+        h[q] = hv;
+        nod = C <= 0 ? 1u : 0u;
+    }
+    nod = __reduce_add_sync(0xffffffffu, nod);
+    if ((threadIdx.x & 31) == 0 && nod) {
+        const int slot = (blockIdx.x + blockIdx.y * 5 + threadIdx.y) & (kStatSlots - 1);
+        atomicAdd(&sc->nodata[slot], (unsigned long long)nod);
+    }
+}
+
+}  // namespace dnni

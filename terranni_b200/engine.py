@@ -1,0 +1,200 @@
+"""Python binding of the engine's C ABI (include/dnni.h) via ctypes.
+
+This is plumbing for the test suite, the smoke entry and ``bench.py``; the
+drop-in boundary itself is the C ABI and the C++ ``nni::`` shim.  The native
+library is required: if ``libdnni.so`` is missing every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdnni.so")
+
+NO_SITE = 0xFFFFFFFF
+F_TIMING = 1
+
+STATUS = {
+    0: "DNNI_OK", 1: "DNNI_E_INVAL", 2: "DNNI_E_NOMEM", 3: "DNNI_E_TIMEOUT", 4: "DNNI_E_CUDA",
+    5: "DNNI_E_RANGE", 6: "DNNI_E_STATE", 7: "DNNI_E_IO", 8: "DNNI_E_CANCELLED", 9: "DNNI_E_BUSY",
+}
+
+
+class DnniError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+
+
+class Settings(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("small_radius", ctypes.c_int32),
+                ("bin_target", ctypes.c_int32), ("flags", ctypes.c_int32),
+                ("mem_budget", ctypes.c_uint64)]
+
+
+class WorkPackage(ctypes.Structure):
+    _fields_ = [
+        ("ncols", ctypes.c_int32), ("nrows", ctypes.c_int32),
+        ("cell_size", ctypes.c_int32),
+        ("origin_x", ctypes.c_int32), ("origin_y", ctypes.c_int32),
+        ("raster_x0", ctypes.c_int32), ("raster_y0", ctypes.c_int32),
+        ("raster_x1", ctypes.c_int32), ("raster_y1", ctypes.c_int32),
+        ("pad0", ctypes.c_int32),
+        ("z_scale", ctypes.c_double), ("z_offset", ctypes.c_double),
+        ("nodata", ctypes.c_float), ("pad1", ctypes.c_int32),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("ms_total", ctypes.c_double), ("ms_bin", ctypes.c_double), ("ms_nearest", ctypes.c_double),
+        ("ms_scatter", ctypes.c_double), ("ms_finalize", ctypes.c_double),
+        ("n_points", ctypes.c_int64), ("n_cells", ctypes.c_int64), ("n_pixels", ctypes.c_int64),
+        ("big_pixels", ctypes.c_int64), ("spans", ctypes.c_int64), ("nodata_cells", ctypes.c_int64),
+        ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+        ("max_r2", ctypes.c_int32), ("packed", ctypes.c_int32), ("bin_size", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+# every symbol include/dnni.h declares, with (argtypes, restype)
+_P = ctypes.c_void_p
+_SIGS = {
+    "dnni_version": ([], ctypes.c_int32),
+    "dnni_init": ([ctypes.POINTER(Settings), ctypes.POINTER(_P)], ctypes.c_int),
+    "dnni_destroy": ([_P], ctypes.c_int),
+    "dnni_last_error": ([_P], ctypes.c_char_p),
+    "dnni_setup_run": ([_P, ctypes.POINTER(WorkPackage), ctypes.c_int64], ctypes.c_int),
+    "dnni_interpolate_segment": ([_P, ctypes.POINTER(WorkPackage), _P, _P, ctypes.c_int64, _P, _P,
+                                  ctypes.POINTER(Stats)], ctypes.c_int),
+    "dnni_interpolate_segment_device": ([_P, ctypes.POINTER(WorkPackage), _P, _P, ctypes.c_int64, _P, _P, _P,
+                                         ctypes.POINTER(Stats)], ctypes.c_int),
+    "dnni_clear": ([_P], ctypes.c_int),
+    "dnni_print_times": ([_P], ctypes.c_int),
+    "dnni_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(_P)], ctypes.c_int),
+    "dnni_host_free": ([_P], ctypes.c_int),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"native engine not built: {LIB_PATH} is missing (run python -m terranni_b200.build)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def make_wp(ncols, nrows, cell_size, origin_x=0, origin_y=0, raster=None, z_scale=0.01, z_offset=0.0,
+            nodata=-9999.0) -> WorkPackage:
+    wp = WorkPackage()
+    wp.ncols, wp.nrows, wp.cell_size = int(ncols), int(nrows), int(cell_size)
+    wp.origin_x, wp.origin_y = int(origin_x), int(origin_y)
+    if raster is not None:
+        wp.raster_x0, wp.raster_y0, wp.raster_x1, wp.raster_y1 = (int(v) for v in raster)
+    wp.z_scale, wp.z_offset, wp.nodata = float(z_scale), float(z_offset), float(nodata)
+    return wp
+
+
+def raster_box(wp: WorkPackage):
+    if (wp.raster_x0, wp.raster_y0, wp.raster_x1, wp.raster_y1) == (0, 0, 0, 0):
+        return 0, 0, wp.ncols, wp.nrows
+    return wp.raster_x0, wp.raster_y0, wp.raster_x1, wp.raster_y1
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):          # torch tensor
+        return a.data_ptr()
+    return a.ctypes.data_as(ctypes.c_void_p).value
+
+
+class Engine:
+    """One dnni context (one device, one host thread at a time)."""
+
+    def __init__(self, device=0, small_radius=0, bin_target=0, flags=0, mem_budget=0):
+        s = Settings(device, small_radius, bin_target, flags, mem_budget)
+        h = _P()
+        rc = lib().dnni_init(ctypes.byref(s), ctypes.byref(h))
+        if rc:
+            raise DnniError(rc, "dnni_init failed")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().dnni_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc:
+            msg = lib().dnni_last_error(self._h)
+            raise DnniError(rc, msg.decode() if msg else "")
+
+    def setup_run(self, wp, max_points):
+        self._check(lib().dnni_setup_run(self._h, ctypes.byref(wp), int(max_points)))
+
+    def interpolate(self, wp: WorkPackage, xyz, gid=None, site=False, out_h=None):
+        """Host-buffer call (dnni_interpolate_segment) -> (h, site_map, stats)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1, 3)
+        if gid is not None:
+            gid = np.ascontiguousarray(gid, dtype=np.uint32)
+        h = out_h if out_h is not None else np.empty((wp.nrows, wp.ncols), np.float32)
+        x0, y0, x1, y1 = raster_box(wp)
+        sm = np.empty((y1 - y0, x1 - x0), np.uint32) if site else None
+        st = Stats()
+        self._check(lib().dnni_interpolate_segment(self._h, ctypes.byref(wp), _ptr(xyz), _ptr(gid),
+                                                   xyz.shape[0], _ptr(h), _ptr(sm), ctypes.byref(st)))
+        return h, sm, st
+
+    def interpolate_device(self, wp: WorkPackage, d_xyz, n, d_h, d_gid=None, d_site=None, stream=None,
+                           stats=True):
+        """Device-buffer call (dnni_interpolate_segment_device).  Buffers are
+        torch CUDA tensors or raw device addresses; stream is a raw
+        cudaStream_t value (e.g. torch.cuda.current_stream().cuda_stream)."""
+        st = Stats() if stats else None
+        self._check(lib().dnni_interpolate_segment_device(
+            self._h, ctypes.byref(wp), _ptr(d_xyz), _ptr(d_gid), int(n), _ptr(d_h), _ptr(d_site),
+            stream, ctypes.byref(st) if st is not None else None))
+        return st
+
+    def clear(self):
+        self._check(lib().dnni_clear(self._h))
+
+    def print_times(self):
+        self._check(lib().dnni_print_times(self._h))

@@ -1,0 +1,112 @@
+"""Seeded synthetic workloads (binding of csrc/synth.c).
+
+The workloads are the five benchmark configurations of this engine: seeded
+stand-ins with the stated shapes, sizes and value distributions; no public
+dataset is involved.  All coordinates are int32 LAS units at 0.01 m.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdnni_synth.so")
+BASE_SEED = 20261203
+XY_SCALE = 0.01
+Z_SCALE = 0.01
+
+
+class SynthParams(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint64), ("n", ctypes.c_int64),
+        ("width", ctypes.c_double), ("height", ctypes.c_double),
+        ("xy_scale", ctypes.c_double), ("z_scale", ctypes.c_double),
+        ("kind", ctypes.c_int32), ("nclusters", ctypes.c_int32),
+        ("frac_uniform", ctypes.c_double), ("cluster_sigma", ctypes.c_double),
+        ("nlakes", ctypes.c_int32), ("octaves", ctypes.c_int32),
+        ("lake_rmin", ctypes.c_double), ("lake_rmax", ctypes.c_double),
+        ("relief", ctypes.c_double), ("z_noise", ctypes.c_double),
+        ("hurst", ctypes.c_double), ("base_wavelength", ctypes.c_double),
+        ("nthreads", ctypes.c_int32), ("pad", ctypes.c_int32),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing (run python -m terranni_b200.build)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.synth_generate.argtypes = [ctypes.POINTER(SynthParams), ctypes.c_void_p, ctypes.c_void_p]
+        L.synth_generate.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def generate(seed, n, width, height, kind="terrain", nclusters=64, frac_uniform=0.7, cluster_sigma=20.0,
+             nlakes=16, lake_rmin=50.0, lake_rmax=400.0, relief=300.0, z_noise=0.1, hurst=0.8, octaves=8,
+             base_wavelength=None, nthreads=0):
+    """-> (xyz int32 (n,3), lakes float64 (nlakes,3) as cx, cy, r in metres)."""
+    p = SynthParams()
+    p.seed, p.n, p.width, p.height = int(seed), int(n), float(width), float(height)
+    p.xy_scale, p.z_scale = XY_SCALE, Z_SCALE
+    p.kind = 1 if kind == "sinusoid" else 0
+    p.nclusters, p.frac_uniform, p.cluster_sigma = int(nclusters), float(frac_uniform), float(cluster_sigma)
+    p.nlakes, p.octaves = int(nlakes), int(octaves)
+    p.lake_rmin, p.lake_rmax = float(lake_rmin), float(lake_rmax)
+    p.relief, p.z_noise, p.hurst = float(relief), float(z_noise), float(hurst)
+    p.base_wavelength = float(base_wavelength if base_wavelength else max(width, height) / 2.0)
+    p.nthreads = int(nthreads)
+    xyz = np.empty((int(n), 3), np.int32)
+    lakes = np.zeros((max(int(nlakes), 1), 3), np.float64)
+    rc = lib().synth_generate(ctypes.byref(p), xyz.ctypes.data_as(ctypes.c_void_p),
+                              lakes.ctypes.data_as(ctypes.c_void_p))
+    if rc:
+        raise ValueError("synth_generate: bad parameters")
+    return xyz, lakes[: int(nlakes)] if p.kind == 0 else lakes[:0]
+
+
+def config1(seed=BASE_SEED):
+    """512 x 512 grid at 1 m, 200k points, z = 4 sinusoids + N(0, 0.05 m)."""
+    xyz, _ = generate(seed, 200_000, 512.0, 512.0, kind="sinusoid", z_noise=0.05)
+    return {"xyz": xyz, "ncols": 512, "nrows": 512, "cell": 100,
+            "las_offset": (500000.0, 4000000.0, 0.0)}
+
+
+def config2(seed=BASE_SEED + 2, n=20_000_000, side=4096):
+    """4096 x 4096 at 1 m, 20M points, 70% uniform + 30% in 64 clusters
+    (sigma 20 m), 16 lakes of radius 50-400 m, fBm z (H 0.8, 8 octaves, 0-300 m)
+    + N(0, 0.1 m)."""
+    xyz, lakes = generate(seed, n, float(side), float(side), kind="terrain", nclusters=64, frac_uniform=0.7,
+                          cluster_sigma=20.0, nlakes=16, lake_rmin=50.0, lake_rmax=400.0, relief=300.0,
+                          z_noise=0.1)
+    return {"xyz": xyz, "ncols": side, "nrows": side, "cell": 100, "lakes": lakes}
+
+
+def mixed_tiles(count=4096, seed=BASE_SEED + 4, max_points=1_000_000):
+    """Tile specs of the mixed batch: side log-uniform in [64, 1024] cells,
+    cell 0.5/1/2 m, density log-uniform in [0.05, 8] points/cell,
+    N = clamp(density * side^2, 1e3, 1e6), 0-4 lakes (radius 5-30 % of side)."""
+    rng = np.random.default_rng(seed)
+    side = np.exp(rng.uniform(math.log(64), math.log(1024), count)).astype(np.int64)
+    cell = rng.choice(np.array([50, 100, 200]), count)
+    dens = np.exp(rng.uniform(math.log(0.05), math.log(8.0), count))
+    n = np.clip((dens * side * side).astype(np.int64), 1000, max_points)
+    lakes = rng.integers(0, 5, count)
+    seeds = rng.integers(1, 2 ** 62, count)
+    return [{"side": int(side[i]), "cell": int(cell[i]), "n": int(n[i]), "lakes": int(lakes[i]),
+             "seed": int(seeds[i])} for i in range(count)]
+
+
+def tile_points(spec):
+    ext = spec["side"] * spec["cell"] * XY_SCALE
+    xyz, _ = generate(spec["seed"], spec["n"], ext, ext, kind="terrain", nclusters=8, frac_uniform=0.7,
+                      cluster_sigma=max(ext / 50.0, 1.0), nlakes=spec["lakes"], lake_rmin=0.05 * ext,
+                      lake_rmax=0.3 * ext, relief=300.0, z_noise=0.1)
+    return xyz

@@ -1,0 +1,72 @@
+"""The C ABI library loads and exports every symbol its headers declare."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"//[^\n]*", "", src)
+    return sorted(set(re.findall(r"\b(dnni_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_libdnni_exports_every_declared_symbol():
+    from terranni_b200 import engine
+    L = engine.lib()
+    names = declared("dnni.h")
+    assert len(names) >= 11
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(names) <= set(engine.exported_symbols())
+
+
+def test_version():
+    from terranni_b200 import engine
+    assert engine.lib().dnni_version() == 10000
+
+
+def test_init_without_device_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        return
+    from terranni_b200 import engine
+    h = ctypes.c_void_p()
+    assert engine.lib().dnni_init(None, ctypes.byref(h)) == 4   # DNNI_E_CUDA
+    assert not h.value
+
+
+def test_null_arguments_rejected():
+    from terranni_b200 import engine
+    L = engine.lib()
+    assert L.dnni_init(None, None) == 1
+    assert L.dnni_destroy(None) == 1
+    assert L.dnni_last_error(None) == b"context is NULL"
+
+
+def test_synth_is_seeded_and_thread_independent():
+    from terranni_b200 import synth
+    a, la = synth.generate(42, 20000, 300.0, 200.0, nlakes=3, lake_rmin=10, lake_rmax=40, nthreads=1)
+    b, lb = synth.generate(42, 20000, 300.0, 200.0, nlakes=3, lake_rmin=10, lake_rmax=40, nthreads=4)
+    assert np.array_equal(a, b) and np.array_equal(la, lb)
+    assert a[:, 0].min() >= 0 and a[:, 0].max() < 30000 and a[:, 1].max() < 20000
+    # no point inside a lake
+    for cx, cy, r in la:
+        d2 = (a[:, 0] * 0.01 - cx) ** 2 + (a[:, 1] * 0.01 - cy) ** 2
+        assert (d2 >= (r - 0.01) ** 2).all()
+    c, _ = synth.generate(43, 20000, 300.0, 200.0, nlakes=3, lake_rmin=10, lake_rmax=40)
+    assert not np.array_equal(a, c)
+
+
+def test_sinusoid_workload_shape():
+    from terranni_b200 import synth
+    w = synth.config1()
+    xyz = w["xyz"]
+    assert xyz.shape == (200000, 3)
+    assert xyz[:, :2].min() >= 0 and xyz[:, :2].max() < 51200
+    z = xyz[:, 2] * 0.01
+    assert -80.5 < z.min() < 0 < z.max() < 80.5
