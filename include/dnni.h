@@ -50,7 +50,9 @@ typedef enum dnni_status {
     DNNI_E_STATE = 6,      /* call out of order (e.g. no setup) */
     DNNI_E_IO = 7,         /* file could not be read / parsed */
     DNNI_E_CANCELLED = 8,  /* request cancelled before completion */
-    DNNI_E_BUSY = 9        /* admission refused: no slot or memory free now */
+    DNNI_E_BUSY = 9,       /* admission refused: no slot or memory free now */
+    DNNI_E_SCRATCH = 10    /* work package needs more than the fixed scratch of
+                              dnni_interpolate_segment_device_noalloc */
 } dnni_status;
 
 typedef struct dnni_ctx dnni_ctx;
@@ -134,6 +136,35 @@ dnni_status dnni_interpolate_segment_device(dnni_ctx *ctx, const dnni_workpackag
                                             const int32_t *d_xyz, const uint32_t *d_gid, int64_t n,
                                             float *d_h, uint32_t *d_site, void *stream,
                                             dnni_stats *stats);
+
+/* ---- the same call without any allocation (no counterpart in the reference) ----
+ *
+ * For callers that cannot let a library call cudaMalloc or cudaFree: host
+ * applications that own all device memory through their own pool and forbid
+ * libraries from allocating (plug-in hosts with a fixed device budget), and
+ * latency-critical callers that cannot absorb the implicit device-wide
+ * synchronisation of those calls.  Needs no context.  All scratch comes from
+ * one fixed 32 MiB device array compiled into this library; every GPU that
+ * loads the library holds it until the process exits.
+ *
+ * Limit: the work package must fit that array, at about 12 B per grid cell +
+ * 8 B per raster pixel + 20 B per point + 8 B per search bin (about one bin
+ * per two points), each region rounded up to 256 B; e.g. a 512 x 512 grid
+ * with 500k points fits.  Larger work packages return DNNI_E_SCRATCH, before
+ * any work is queued or, for the search bins (sized from the point bounding
+ * box), right after the bounding-box pass.
+ *
+ * Runs on the calling thread's current device and queues on `stream`
+ * (a cudaStream_t, NULL = the legacy default stream); it waits once, for the
+ * bounding box, and returns with the rest queued.  The first call on each
+ * device looks up the array's device address; make that first call before
+ * any stream capture.  Every call shares the one array and overwrites what
+ * the previous call left in it (what must start at zero is cleared on each
+ * call), so calls whose work overlaps on the GPU race: serialise them, e.g.
+ * on one stream. */
+dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpackage *wp, const int32_t *d_xyz,
+                                                    const uint32_t *d_gid, int64_t n, float *d_h,
+                                                    uint32_t *d_site, void *stream);
 
 /* ---- nni::clearRenderbuffers / nni::printTimes (nni.h:87-97) ---- */
 

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../../include/dnni.h"
@@ -403,4 +404,142 @@ void dnni_free_all(dnni_ctx* c) {
     DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc,
                       &c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
     for (DevBuf* b : bufs) dnni_release(*b, c);
+}
+
+// ---------------------------------------------------------------------------
+// Entry point that allocates nothing (no counterpart in the reference).
+//
+// Some callers cannot let a library call cudaMalloc: a host application that
+// manages all device memory through its own pool and forbids libraries from
+// allocating behind its back (a GIS or database plug-in host with a fixed
+// device budget), or a latency-critical caller that cannot absorb the implicit
+// device-wide synchronisation of cudaMalloc/cudaFree.  For them,
+// dnni_interpolate_segment_device_noalloc runs the same kernels as
+// dnni_interpolate_segment_device with every byte of scratch taken from the
+// file-scope device array below.  The module that holds the array is loaded on
+// every GPU that uses this library, and that GPU keeps the 32 MiB until the
+// process exits.
+// ---------------------------------------------------------------------------
+
+constexpr size_t kNoAllocScratchBytes = 32u << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// In host code g_noalloc_scratch is only a host-side stand-in for the array,
+// not a device address: a kernel given it would fault or, where the GPU can
+// reach host memory, silently use the wrong memory.  The device address is
+// looked up once per device, with that device current, on the first call.
+dnni_status noalloc_base(int dev, unsigned char** out) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return DNNI_E_INVAL;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return DNNI_E_CUDA;
+        }
+        g_noalloc_base[dev] = (unsigned char*)p;
+    }
+    *out = g_noalloc_base[dev];
+    return DNNI_OK;
+}
+
+struct ArenaCursor {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        const size_t o = off;
+        off = (off + bytes + 255) & ~(size_t)255;
+        return o;
+    }
+    bool fits() const { return off <= kNoAllocScratchBytes; }
+};
+
+}  // namespace
+
+extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpackage* wp, const int32_t* d_xyz,
+                                                               const uint32_t* d_gid, int64_t n, float* d_h,
+                                                               uint32_t* d_site, void* stream) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return DNNI_E_CUDA;
+    }
+    unsigned char* base = nullptr;
+    dnni_status rs = noalloc_base(dev, &base);
+    if (rs) return rs;
+    TileParams t;
+    const char* msg = "";
+    rs = plan_geometry(wp, n, 3, t, &msg);
+    if (rs) return rs;
+    if (!d_h || (n > 0 && !d_xyz)) return DNNI_E_INVAL;
+    t.has_gid = d_gid ? 1 : 0;
+    const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
+    ArenaCursor a;
+    const size_t o_sc = a.take(sizeof(Scalars));
+    const size_t o_pix = a.take(sizeof(int2) * npix);
+    const size_t o_D = a.take(sizeof(unsigned long long) * cells);
+    const size_t o_Dc = a.take(sizeof(int) * cells);
+    const size_t o_rank = n > 0 ? a.take(sizeof(int) * n) : 0;
+    const size_t o_sorted = n > 0 ? a.take(sizeof(int4) * n) : 0;
+    if (!a.fits()) return DNNI_E_SCRATCH;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    Scalars* sc = (Scalars*)(base + o_sc);
+    int2* pix = (int2*)(base + o_pix);
+    unsigned long long* D = (unsigned long long*)(base + o_D);
+    int* Dc = (int*)(base + o_Dc);
+    int* rank = (int*)(base + o_rank);
+    int4* sorted = (int4*)(base + o_sorted);
+    // the array keeps the previous call's contents: every region that must
+    // start at zero (scalars, bin counts, span words) is cleared below
+    k_init_scalars<<<1, 32, 0, st>>>(sc);
+    Scalars hsc;
+    memset(&hsc, 0, sizeof(hsc));
+    if (n > 0) {
+        k_bbox<<<grid_for(n, 256, sms * 8), 256, 0, st>>>(d_xyz, n, t.ox, t.oy, sc);
+        if (cudaMemcpyAsync(&hsc, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            cudaGetLastError();
+            return DNNI_E_CUDA;
+        }
+        if (hsc.err & kErrRange) return DNNI_E_RANGE;
+    }
+    plan_bins(hsc.bbox, n, 2.0, t);
+    int* start = nullptr;
+    if (n > 0) {
+        const int64_t m = t.bg.nbins + 1;
+        const int nb = (int)((m + kScanTile - 1) / kScanTile);
+        int* cnt = (int*)(base + a.take(sizeof(int) * m));
+        start = (int*)(base + a.take(sizeof(int) * m));
+        int* bsum = (int*)(base + a.take(sizeof(int) * nb));
+        if (!a.fits()) return DNNI_E_SCRATCH;
+        if (cudaMemsetAsync(cnt, 0, sizeof(int) * m, st) != cudaSuccess) return DNNI_E_CUDA;
+        const int g = grid_for(n, 256, sms * 16);
+        k_bin_count<<<g, 256, 0, st>>>(d_xyz, n, t.ox, t.oy, t.bg, cnt, rank);
+        k_scan_partial<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum);
+        k_scan_bsum<<<1, 1024, 0, st>>>(bsum, nb);
+        k_scan_final<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum, start);
+        k_bin_scatter<<<g, 256, 0, st>>>(d_xyz, d_gid, n, t.ox, t.oy, t.bg, start, rank, sorted);
+    }
+    {
+        dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
+        k_nearest<<<grd, blk, 0, st>>>(t, sorted, start, pix, d_site, sc);
+        k_decide<<<1, 32, 0, st>>>(sc, npix);
+        if (cudaMemsetAsync(D, 0, sizeof(unsigned long long) * cells, st) != cudaSuccess ||
+            cudaMemsetAsync(Dc, 0, sizeof(int) * cells, st) != cudaSuccess)
+            return DNNI_E_CUDA;
+        k_scatter_spans<<<grd, blk, 0, st>>>(t, pix, sc, D, Dc);
+    }
+    k_rowscan<unsigned long long><<<t.nrows, kScanThreads, 0, st>>>(D, t.ncols, sc, 0);
+    k_rowscan<int><<<t.nrows, kScanThreads, 0, st>>>(Dc, t.ncols, sc, 1);
+    launch_final(t, pix, sc, D, Dc, d_h, st);
+    if (cudaGetLastError() != cudaSuccess) return DNNI_E_CUDA;
+    return DNNI_OK;
 }

@@ -20,6 +20,7 @@ F_TIMING = 1
 STATUS = {
     0: "DNNI_OK", 1: "DNNI_E_INVAL", 2: "DNNI_E_NOMEM", 3: "DNNI_E_TIMEOUT", 4: "DNNI_E_CUDA",
     5: "DNNI_E_RANGE", 6: "DNNI_E_STATE", 7: "DNNI_E_IO", 8: "DNNI_E_CANCELLED", 9: "DNNI_E_BUSY",
+    10: "DNNI_E_SCRATCH",
 }
 
 
@@ -75,6 +76,8 @@ _SIGS = {
                                   ctypes.POINTER(Stats)], ctypes.c_int),
     "dnni_interpolate_segment_device": ([_P, ctypes.POINTER(WorkPackage), _P, _P, ctypes.c_int64, _P, _P, _P,
                                          ctypes.POINTER(Stats)], ctypes.c_int),
+    "dnni_interpolate_segment_device_noalloc": ([ctypes.POINTER(WorkPackage), _P, _P, ctypes.c_int64, _P, _P, _P],
+                                                ctypes.c_int),
     "dnni_clear": ([_P], ctypes.c_int),
     "dnni_print_times": ([_P], ctypes.c_int),
     "dnni_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(_P)], ctypes.c_int),
