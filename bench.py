@@ -84,7 +84,11 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, which):
+        """Record the start or end of the timed region (host clock)."""
+        setattr(self, which, time.time())
 
     def __exit__(self, *exc):
         if self.proc:
@@ -96,9 +100,15 @@ class ClockSampler:
             self.t.join(timeout=2)
 
     def summary(self):
+        """Samples that arrived inside the timed region (the nearest one when
+        the region is shorter than the 200 ms sampling period)."""
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = getattr(self, "t_start", 0.0), getattr(self, "t_end", float("inf"))
+        inside = [ln for ts, ln in self.lines if t0 <= ts <= t1 + 0.2]
+        if not inside and self.lines:
+            inside = [min(self.lines, key=lambda x: abs(x[0] - t1))[1]]
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -214,24 +224,25 @@ def run_engine(args, world, rank, local):
     eng = engine.Engine(device=local, flags=engine.F_TIMING)
     d_xyz = torch.from_numpy(xyz).cuda()
     d_h = torch.empty((side, side), dtype=torch.float32, device="cuda")
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()           # the engine launches on exactly this stream
     sp = stream.cuda_stream
 
     phases = []
-    last = None
-    for _ in range(args.warmup):
-        last = eng.interpolate_device(wp, d_xyz, npts, d_h, stream=sp, stats=True)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            eng.interpolate_device(wp, d_xyz, npts, d_h, stream=sp, stats=True)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clk.mark("t_start")
         ev0.record(stream)
         for _ in range(args.steps):
             st = eng.interpolate_device(wp, d_xyz, npts, d_h, stream=sp, stats=True)
             phases.append(st)
         ev1.record(stream)
         torch.cuda.synchronize()
+        clk.mark("t_end")
     barrier()
     ms = ev0.elapsed_time(ev1)
     ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")

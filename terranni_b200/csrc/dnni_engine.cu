@@ -173,8 +173,16 @@ dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32
     }
     if (timing) CK(cudaEventRecord(c->ev[1], st));
     {
+        int* seeds = nullptr;
+        if (n > 0) {
+            const int ns = seed_dim(t.rw) * seed_dim(t.rh);
+            if ((rs = dnni_ensure(c, c->seeds, sizeof(int) * ns))) return rs;
+            seeds = (int*)c->seeds.p;
+            k_seeds<<<(ns + 127) / 128, 128, 0, st>>>(t, (const int4*)c->sorted.p, (const int*)c->start.p, seeds);
+        }
         dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        k_nearest<<<grd, blk, 0, st>>>(t, (const int4*)c->sorted.p, (const int*)c->start.p, (int2*)c->pix.p, d_site, sc);
+        k_nearest<<<grd, blk, 0, st>>>(t, (const int4*)c->sorted.p, (const int*)c->start.p, seeds, (int2*)c->pix.p,
+                                       d_site, sc);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         CK(cudaGetLastError());
     }
@@ -401,7 +409,7 @@ dnni_status dnni_host_free(void* p) {
 }  // extern "C"
 
 void dnni_free_all(dnni_ctx* c) {
-    DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc,
+    DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc, &c->seeds,
                       &c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
@@ -530,7 +538,7 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     }
     {
         dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        k_nearest<<<grd, blk, 0, st>>>(t, sorted, start, pix, d_site, sc);
+        k_nearest<<<grd, blk, 0, st>>>(t, sorted, start, nullptr, pix, d_site, sc);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         if (cudaMemsetAsync(D, 0, sizeof(unsigned long long) * cells, st) != cudaSuccess ||
             cudaMemsetAsync(Dc, 0, sizeof(int) * cells, st) != cudaSuccess)

@@ -117,9 +117,10 @@ struct Best {
     long long d2;
     uint32_t gid;
     int z;
+    int idx;      // position of the site in the sorted point array
 };
 
-DNNI_HD void consider(Best& b, const int4 p, int px, int py) {
+DNNI_HD void consider(Best& b, const int4 p, int q, int px, int py) {
     const int dx = p.x - px, dy = p.y - py;      // |p.x|, |px| < 2^30
     const long long d2 = (long long)dx * dx + (long long)dy * dy;
     const uint32_t g = (uint32_t)p.w;
@@ -127,6 +128,7 @@ DNNI_HD void consider(Best& b, const int4 p, int px, int py) {
         b.d2 = d2;
         b.gid = g;
         b.z = p.z;
+        b.idx = q;
     }
 }
 
@@ -180,21 +182,35 @@ DNNI_HD bool ring_done(long long best, long long px, long long py, long long gx0
 }
 
 DNNI_HD void scan_points(Best& b, const int4* __restrict__ pts, int s, int e, int px, int py) {
-    for (int q = s; q < e; ++q) consider(b, DNNI_LDG(&pts[q]), px, py);
+    for (int q = s; q < e; ++q) consider(b, DNNI_LDG(&pts[q]), q, px, py);
 }
 
-// Exact nearest site of the pixel at (px,py) (LAS units relative to the WP
-// origin): bin rings, then block rings, then superblock rings, each level
-// pruned by box lower bounds and empty ranges, each stopping on ring_done.
-__host__ __device__ inline void nearest_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
-                               int px, int py, Best& b) {
+// Conservative bound on the distance reach of a squared bound v >= 0:
+// floor(sqrt(v)) + 1 (the double square root is correctly rounded; the +1
+// absorbs its rounding, so no cell within the disc is ever left out).
+DNNI_HD long long reach_of(long long v) { return (long long)sqrt((double)v) + 1; }
+
+// Range [lo,hi] of cell indices (cells u wide from origin o, n of them)
+// that the interval [c-w, c+w] touches; empty when lo > hi.
+DNNI_HD void cell_range(long long c, long long w, long long o, long long u, int n, int& lo, int& hi) {
+    long long a = c - w, b = c + w;
+    const long long end = o + (long long)n * u - 1;
+    if (b < o || a > end) { lo = 1; hi = 0; return; }
+    if (a < o) a = o;
+    if (b > end) b = end;
+    lo = (int)((a - o) / u);
+    hi = (int)((b - o) / u);
+}
+
+// Level 0 of the search: bin rings 0..kRingsBins around the pixel's bin.
+// Returns true when the nearest site is certain.
+DNNI_HD bool search_bins(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                         int px, int py, Best& b) {
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
     int bx = (int)(((long long)px - gx0) / bs);
     int by = (int)(((long long)py - gy0) / bs);
     bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
     by = by < g.nby - 1 ? by : g.nby - 1;
-
-    // level 0: bins
     for (int k = 0; k <= kRingsBins; ++k) {
         const int ne = ring_size(k);
         for (int e = 0; e < ne; ++e) {
@@ -206,64 +222,126 @@ __host__ __device__ inline void nearest_search(const BinGrid& g, const int4* __r
             const int64_t id = bin_id(g, x, y);
             scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
         }
-        if (ring_done(b.d2, px, py, gx0, gy0, bs, bx - k, bx + k, by - k, by + k, g.nbx, g.nby)) return;
+        if (ring_done(b.d2, px, py, gx0, gy0, bs, bx - k, bx + k, by - k, by + k, g.nbx, g.nby)) return true;
     }
+    return false;
+}
 
-    // level 1: blocks of 8x8 bins
-    const int n1x = g.nbx >> 3, n1y = g.nby >> 3, c1x = bx >> 3, c1y = by >> 3;
-    const long long u1 = bs * kBinsPerBlockEdge;
-    for (int K = 0; K <= kRingsBlocks; ++K) {
-        const int ne = ring_size(K);
+// Any site at all, for a pixel whose bound is still infinite: the first point
+// of the nearest non-empty superblock in ring order.  Needs n > 0.
+DNNI_HD void seed_from_superblocks(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                                   int px, int py, Best& b) {
+    const long long u2 = (long long)g.bs * kBinsPerSuperEdge;
+    int cx = (int)(((long long)px - g.gx0) / u2), cy = (int)(((long long)py - g.gy0) / u2);
+    cx = cx < g.n2x - 1 ? cx : g.n2x - 1;
+    cy = cy < g.n2y - 1 ? cy : g.n2y - 1;
+    const int kmax = (g.n2x > g.n2y ? g.n2x : g.n2y);
+    for (int k = 0; k <= kmax; ++k) {
+        const int ne = ring_size(k);
         for (int e = 0; e < ne; ++e) {
             int x, y;
-            ring_cell(c1x, c1y, K, e, x, y);
-            if (x < 0 || y < 0 || x >= n1x || y >= n1y) continue;
-            const long long X0 = gx0 + (long long)x * u1, Y0 = gy0 + (long long)y * u1;
-            if (box_lb(px, py, X0, X0 + u1 - 1, Y0, Y0 + u1 - 1) > b.d2) continue;
-            const int64_t first = bin_id(g, x * 8, y * 8);
-            if (DNNI_LDG(&start[first]) == DNNI_LDG(&start[first + kBinsPerBlock])) continue;
-            for (int l = 0; l < kBinsPerBlock; ++l) {
-                const int gbx = x * 8 + (l & 7), gby = y * 8 + (l >> 3);
-                if (abs(gbx - bx) <= kRingsBins && abs(gby - by) <= kRingsBins) continue;
-                const long long BX0 = gx0 + (long long)gbx * bs, BY0 = gy0 + (long long)gby * bs;
-                if (box_lb(px, py, BX0, BX0 + bs - 1, BY0, BY0 + bs - 1) > b.d2) continue;
-                const int64_t id = first + l;
-                scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
+            ring_cell(cx, cy, k, e, x, y);
+            if (x < 0 || y < 0 || x >= g.n2x || y >= g.n2y) continue;
+            const int64_t sfirst = (int64_t)(y * g.n2x + x) << 12;
+            const int s = DNNI_LDG(&start[sfirst]);
+            if (s != DNNI_LDG(&start[sfirst + kBinsPerSuper])) {
+                consider(b, DNNI_LDG(&pts[s]), s, px, py);
+                return;
             }
         }
-        if (ring_done(b.d2, px, py, gx0, gy0, u1, c1x - K, c1x + K, c1y - K, c1y + K, n1x, n1y)) return;
     }
+}
 
-    // level 2: superblocks of 8x8 blocks
-    const int c2x = bx >> 6, c2y = by >> 6;
-    const long long u2 = bs * kBinsPerSuperEdge;
-    for (int K = 0;; ++K) {
-        const int ne = ring_size(K);
-        for (int e = 0; e < ne; ++e) {
-            int x, y;
-            ring_cell(c2x, c2y, K, e, x, y);
-            if (x < 0 || y < 0 || x >= g.n2x || y >= g.n2y) continue;
-            const long long X0 = gx0 + (long long)x * u2, Y0 = gy0 + (long long)y * u2;
-            if (box_lb(px, py, X0, X0 + u2 - 1, Y0, Y0 + u2 - 1) > b.d2) continue;
-            const int64_t sfirst = (int64_t)(y * g.n2x + x) << 12;
+// Exact search inside the disc of the current bound: every superblock, block
+// and bin the disc touches is visited (rows in order of distance from the
+// pixel, columns narrowed per row to the disc's chord), and nothing else.  The
+// bound only shrinks, so cells left out when their row was reached can never
+// hold a closer site.  Complete whenever b holds a real site on entry.
+DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                         int px, int py, Best& b) {
+    const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
+    int sy0, sy1;
+    cell_range(py, reach_of(b.d2), gy0, u2, g.n2y, sy0, sy1);
+    if (sy0 > sy1) return;
+    int csy = (int)(((long long)py - gy0) / u2);
+    csy = csy < sy0 ? sy0 : (csy > sy1 ? sy1 : csy);
+    const int span = (csy - sy0) > (sy1 - csy) ? (csy - sy0) : (sy1 - csy);
+    for (int r = 0; r <= 2 * span; ++r) {
+        // superblock rows outward from the pixel's own row: csy, csy-1, csy+1, ...
+        const int sy = csy + ((r & 1) ? -((r + 1) >> 1) : (r >> 1));
+        if (sy < sy0 || sy > sy1) continue;
+        const long long SY0 = gy0 + (long long)sy * u2;
+        const long long gy = axis_gap(py, SY0, SY0 + u2 - 1);
+        if (gy * gy > b.d2) continue;
+        int sx0, sx1;
+        cell_range(px, reach_of(b.d2 - gy * gy), gx0, u2, g.n2x, sx0, sx1);
+        for (int sx = sx0; sx <= sx1; ++sx) {
+            const long long SX0 = gx0 + (long long)sx * u2;
+            if (box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) > b.d2) continue;
+            const int64_t sfirst = (int64_t)(sy * g.n2x + sx) << 12;
             if (DNNI_LDG(&start[sfirst]) == DNNI_LDG(&start[sfirst + kBinsPerSuper])) continue;
-            for (int m = 0; m < 64; ++m) {
-                const int gcx = x * 8 + (m & 7), gcy = y * 8 + (m >> 3);
-                if (abs(gcx - c1x) <= kRingsBlocks && abs(gcy - c1y) <= kRingsBlocks) continue;
-                const long long CX0 = gx0 + (long long)gcx * u1, CY0 = gy0 + (long long)gcy * u1;
-                if (box_lb(px, py, CX0, CX0 + u1 - 1, CY0, CY0 + u1 - 1) > b.d2) continue;
-                const int64_t first = sfirst + ((int64_t)m << 6);
-                if (DNNI_LDG(&start[first]) == DNNI_LDG(&start[first + kBinsPerBlock])) continue;
-                for (int l = 0; l < kBinsPerBlock; ++l) {
-                    const long long BX0 = CX0 + (long long)(l & 7) * bs, BY0 = CY0 + (long long)(l >> 3) * bs;
-                    if (box_lb(px, py, BX0, BX0 + bs - 1, BY0, BY0 + bs - 1) > b.d2) continue;
-                    const int64_t id = first + l;
-                    scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
+            // blocks of this superblock inside the disc
+            for (int ly = 0; ly < kBinsPerBlockEdge; ++ly) {
+                const long long BY0 = SY0 + (long long)ly * u1;
+                const long long gyb = axis_gap(py, BY0, BY0 + u1 - 1);
+                if (gyb * gyb > b.d2) continue;
+                int bx0, bx1;
+                cell_range(px - SX0, reach_of(b.d2 - gyb * gyb), 0, u1, kBinsPerBlockEdge, bx0, bx1);
+                for (int lx = bx0; lx <= bx1; ++lx) {
+                    const int64_t bfirst = sfirst + ((int64_t)(ly * 8 + lx) << 6);
+                    if (DNNI_LDG(&start[bfirst]) == DNNI_LDG(&start[bfirst + kBinsPerBlock])) continue;
+                    const long long BX0 = SX0 + (long long)lx * u1;
+                    // bins of this block inside the disc
+                    for (int qy = 0; qy < kBinsPerBlockEdge; ++qy) {
+                        const long long QY0 = BY0 + (long long)qy * bs;
+                        const long long gq = axis_gap(py, QY0, QY0 + bs - 1);
+                        if (gq * gq > b.d2) continue;
+                        int qx0, qx1;
+                        cell_range(px - BX0, reach_of(b.d2 - gq * gq), 0, bs, kBinsPerBlockEdge, qx0, qx1);
+                        if (qx0 > qx1) continue;
+                        const int64_t id0 = bfirst + qy * 8;
+                        scan_points(b, pts, DNNI_LDG(&start[id0 + qx0]), DNNI_LDG(&start[id0 + qx1 + 1]), px, py);
+                    }
                 }
             }
         }
-        if (ring_done(b.d2, px, py, gx0, gy0, u2, c2x - K, c2x + K, c2y - K, c2y + K, g.n2x, g.n2y)) return;
     }
+}
+
+// Sites of a coarse lattice of raster pixels (every kSeedStride-th pixel in
+// each direction, offset by half a stride), solved exactly first; their sites
+// bound the nearest-site distance of the pixels around them.
+constexpr int kSeedStride = 16;
+
+struct SeedGrid {
+    const int* idx;     // sorted-array position of each lattice pixel's site
+    int nx, ny;
+};
+
+DNNI_HD int seed_dim(int n) { return (n + kSeedStride - 1) / kSeedStride; }
+
+// Exact nearest site of raster pixel (i,j) at (px,py) (LAS units relative to
+// the WP origin).  Bin rings settle pixels among dense points; otherwise the
+// bound is seeded from the four surrounding lattice sites (or, without a seed
+// grid, from the nearest non-empty superblock) and the disc of that bound is
+// searched exhaustively.
+DNNI_HD void nearest_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                            int px, int py, Best& b, const SeedGrid* sg = nullptr, int i = 0, int j = 0) {
+    if (search_bins(g, pts, start, px, py, b)) return;
+    if (sg) {
+        int a = (i - kSeedStride / 2) / kSeedStride, c = (j - kSeedStride / 2) / kSeedStride;
+        a = a < 0 ? 0 : (a > sg->nx - 1 ? sg->nx - 1 : a);
+        c = c < 0 ? 0 : (c > sg->ny - 1 ? sg->ny - 1 : c);
+        const int a1 = a + 1 < sg->nx ? a + 1 : a, c1 = c + 1 < sg->ny ? c + 1 : c;
+        const int cand[4] = {c * sg->nx + a, c * sg->nx + a1, c1 * sg->nx + a, c1 * sg->nx + a1};
+        for (int k = 0; k < 4; ++k) {
+            const int q = DNNI_LDG(&sg->idx[cand[k]]);
+            if (q >= 0) consider(b, DNNI_LDG(&pts[q]), q, px, py);
+        }
+    }
+    if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, px, py, b);
+    search_disc(g, pts, start, px, py, b);
 }
 
 // ---------------------------------------------------------------------------
@@ -440,10 +518,26 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restri
 
 // ---- nearest site per raster pixel ----
 
+// Exact sites of the seed lattice (no seeds of its own).
+__global__ void __launch_bounds__(128) k_seeds(TileParams t, const int4* __restrict__ pts,
+                                               const int* __restrict__ start, int* __restrict__ seed) {
+    const int nx = seed_dim(t.rw), ny = seed_dim(t.rh);
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nx * ny) return;
+    const int sx = a % nx, sy = a / nx;
+    int i = sx * kSeedStride + kSeedStride / 2, j = sy * kSeedStride + kSeedStride / 2;
+    i = i < t.rw - 1 ? i : t.rw - 1;
+    j = j < t.rh - 1 ? j : t.rh - 1;
+    Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+    nearest_search(t.bg, pts, start, (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b);
+    seed[a] = b.idx;
+}
+
 // Block 32x8: each warp is 32 consecutive pixels of one raster row.
 __global__ void __launch_bounds__(256) k_nearest(TileParams t, const int4* __restrict__ pts,
-                                                 const int* __restrict__ start, int2* __restrict__ pix,
-                                                 uint32_t* __restrict__ site, Scalars* __restrict__ sc) {
+                                                 const int* __restrict__ start, const int* __restrict__ seed,
+                                                 int2* __restrict__ pix, uint32_t* __restrict__ site,
+                                                 Scalars* __restrict__ sc) {
     const int i = blockIdx.x * 32 + threadIdx.x;
     const int j = blockIdx.y * 8 + threadIdx.y;
     const bool valid = i < t.rw && j < t.rh;
@@ -452,8 +546,9 @@ __global__ void __launch_bounds__(256) k_nearest(TileParams t, const int4* __res
     if (valid && t.npts > 0) {
         const int px = (t.rx0 + i) * t.cs;
         const int py = (t.ry0 + j) * t.cs;
-        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX};
-        nearest_search(t.bg, pts, start, px, py, b);
+        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+        const SeedGrid sg{seed, seed_dim(t.rw), seed_dim(t.rh)};
+        nearest_search(t.bg, pts, start, px, py, b, seed ? &sg : nullptr, i, j);
         const long long q = b.d2 / ((long long)t.cs * t.cs);
         R2 = (int)(q < t.r2cap ? q : t.r2cap);
         z = b.z;

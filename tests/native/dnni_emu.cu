@@ -24,7 +24,7 @@ static float host_height(long long Z, long long C, double zs, double zo, float n
 
 extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, const uint32_t* gid, int64_t n,
                                int small_radius, int bin_target, float* h, uint32_t* site, int32_t* r2_out,
-                               int64_t* info) {
+                               int64_t* info, int seeded) {
     TileParams t;
     const char* msg;
     int rs = small_radius ? small_radius : 3;
@@ -58,13 +58,26 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
     const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
     std::vector<int2> pix(npix);
     int max_r2 = -1;
+    const int snx = seed_dim(t.rw), sny = seed_dim(t.rh);
+    std::vector<int> seeds(n > 0 ? snx * sny : 1, -1);
+    if (n > 0)
+        for (int a = 0; a < snx * sny; ++a) {
+            int i = (a % snx) * kSeedStride + kSeedStride / 2, j = (a / snx) * kSeedStride + kSeedStride / 2;
+            i = std::min(i, t.rw - 1);
+            j = std::min(j, t.rh - 1);
+            Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+            nearest_search(g, sorted.data(), start.data(), (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b);
+            seeds[a] = b.idx;
+        }
+    const SeedGrid seedg{seeds.data(), snx, sny};
     for (int j = 0; j < t.rh; ++j)
         for (int i = 0; i < t.rw; ++i) {
             int R2 = -1, z = 0;
             uint32_t sg = 0xFFFFFFFFu;
             if (n > 0) {
-                Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX};
-                nearest_search(g, sorted.data(), start.data(), (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b);
+                Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+                nearest_search(g, sorted.data(), start.data(), (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b,
+                               seeded ? &seedg : nullptr, i, j);
                 const long long q = b.d2 / ((long long)t.cs * t.cs);
                 R2 = (int)(q < t.r2cap ? q : t.r2cap);
                 z = b.z;
