@@ -169,6 +169,12 @@ dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32
         k_scan_final<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum, start);
         k_bin_scatter<<<g, 256, 0, st>>>(d_xyz, d_gid, n, t.ox, t.oy, t.bg, start, (int*)c->rank.p,
                                          (int4*)c->sorted.p);
+        const int64_t nblk = t.bg.nbins / kBinsPerBlock, nsup = t.bg.nbins / kBinsPerSuper;
+        if ((rs = dnni_ensure(c, c->bmask, sizeof(uint64_t) * nblk))) return rs;
+        if ((rs = dnni_ensure(c, c->smask, sizeof(uint64_t) * nsup))) return rs;
+        k_block_masks<<<(int)((nblk * 32 + 255) / 256), 256, 0, st>>>(start, nblk, (uint64_t*)c->bmask.p);
+        k_super_masks<<<(int)((nsup * 32 + 255) / 256), 256, 0, st>>>((const uint64_t*)c->bmask.p, nsup,
+                                                                      (uint64_t*)c->smask.p);
         CK(cudaGetLastError());
     }
     if (timing) CK(cudaEventRecord(c->ev[1], st));
@@ -178,11 +184,13 @@ dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32
             const int ns = seed_dim(t.rw) * seed_dim(t.rh);
             if ((rs = dnni_ensure(c, c->seeds, sizeof(int) * ns))) return rs;
             seeds = (int*)c->seeds.p;
-            k_seeds<<<(ns + 127) / 128, 128, 0, st>>>(t, (const int4*)c->sorted.p, (const int*)c->start.p, seeds);
+            k_seeds<<<(ns + 127) / 128, 128, 0, st>>>(t, (const int4*)c->sorted.p, (const int*)c->start.p,
+                                                      (const uint64_t*)c->bmask.p, (const uint64_t*)c->smask.p, seeds);
         }
         dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        k_nearest<<<grd, blk, 0, st>>>(t, (const int4*)c->sorted.p, (const int*)c->start.p, seeds, (int2*)c->pix.p,
-                                       d_site, sc);
+        k_nearest<<<grd, blk, 0, st>>>(t, (const int4*)c->sorted.p, (const int*)c->start.p,
+                                       (const uint64_t*)c->bmask.p, (const uint64_t*)c->smask.p, seeds,
+                                       (int2*)c->pix.p, d_site, sc);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         CK(cudaGetLastError());
     }
@@ -410,6 +418,7 @@ dnni_status dnni_host_free(void* p) {
 
 void dnni_free_all(dnni_ctx* c) {
     DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc, &c->seeds,
+                      &c->bmask, &c->smask,
                       &c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
@@ -521,6 +530,8 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     }
     plan_bins(hsc.bbox, n, 2.0, t);
     int* start = nullptr;
+    uint64_t* bmask = nullptr;
+    uint64_t* smask = nullptr;
     if (n > 0) {
         const int64_t m = t.bg.nbins + 1;
         const int nb = (int)((m + kScanTile - 1) / kScanTile);
@@ -535,10 +546,16 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
         k_scan_bsum<<<1, 1024, 0, st>>>(bsum, nb);
         k_scan_final<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum, start);
         k_bin_scatter<<<g, 256, 0, st>>>(d_xyz, d_gid, n, t.ox, t.oy, t.bg, start, rank, sorted);
+        const int64_t nblk = t.bg.nbins / kBinsPerBlock, nsup = t.bg.nbins / kBinsPerSuper;
+        bmask = (uint64_t*)(base + a.take(sizeof(uint64_t) * nblk));
+        smask = (uint64_t*)(base + a.take(sizeof(uint64_t) * nsup));
+        if (!a.fits()) return DNNI_E_SCRATCH;
+        k_block_masks<<<(int)((nblk * 32 + 255) / 256), 256, 0, st>>>(start, nblk, bmask);
+        k_super_masks<<<(int)((nsup * 32 + 255) / 256), 256, 0, st>>>(bmask, nsup, smask);
     }
     {
         dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        k_nearest<<<grd, blk, 0, st>>>(t, sorted, start, nullptr, pix, d_site, sc);
+        k_nearest<<<grd, blk, 0, st>>>(t, sorted, start, bmask, smask, nullptr, pix, d_site, sc);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         if (cudaMemsetAsync(D, 0, sizeof(unsigned long long) * cells, st) != cudaSuccess ||
             cudaMemsetAsync(Dc, 0, sizeof(int) * cells, st) != cudaSuccess)

@@ -227,37 +227,88 @@ DNNI_HD bool search_bins(const BinGrid& g, const int4* __restrict__ pts, const i
     return false;
 }
 
-// Any site at all, for a pixel whose bound is still infinite: the first point
-// of the nearest non-empty superblock in ring order.  Needs n > 0.
+// Occupancy masks: bit l of bmask[block] is set when bin l of that block
+// (row-major 8x8) holds points; bit m of smask[superblock] when block m of it
+// does.  They let the search skip empty cells without touching their ranges.
+DNNI_HD int ffs64(uint64_t v) {
+#ifdef __CUDA_ARCH__
+    return __ffsll((long long)v) - 1;
+#else
+    return __builtin_ctzll(v);
+#endif
+}
+
+DNNI_HD unsigned bits_between(int lo, int hi) { return (0xFFu << lo) & (0xFFu >> (7 - hi)) & 0xFFu; }
+
+DNNI_HD int clz32(unsigned v) {
+#ifdef __CUDA_ARCH__
+    return __clz((int)v);
+#else
+    return __builtin_clz(v);
+#endif
+}
+
+// A first bound for a pixel whose bound is still infinite: the nearest
+// non-empty superblock ring is found, and in each of its non-empty
+// superblocks the closest non-empty block and, in it, the closest non-empty
+// bin contribute their points.  Needs n > 0.
 DNNI_HD void seed_from_superblocks(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                                   const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
                                    int px, int py, Best& b) {
-    const long long u2 = (long long)g.bs * kBinsPerSuperEdge;
-    int cx = (int)(((long long)px - g.gx0) / u2), cy = (int)(((long long)py - g.gy0) / u2);
+    const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
+    int cx = (int)(((long long)px - gx0) / u2), cy = (int)(((long long)py - gy0) / u2);
     cx = cx < g.n2x - 1 ? cx : g.n2x - 1;
     cy = cy < g.n2y - 1 ? cy : g.n2y - 1;
     const int kmax = (g.n2x > g.n2y ? g.n2x : g.n2y);
     for (int k = 0; k <= kmax; ++k) {
+        bool found = false;
         const int ne = ring_size(k);
         for (int e = 0; e < ne; ++e) {
             int x, y;
             ring_cell(cx, cy, k, e, x, y);
             if (x < 0 || y < 0 || x >= g.n2x || y >= g.n2y) continue;
-            const int64_t sfirst = (int64_t)(y * g.n2x + x) << 12;
-            const int s = DNNI_LDG(&start[sfirst]);
-            if (s != DNNI_LDG(&start[sfirst + kBinsPerSuper])) {
-                consider(b, DNNI_LDG(&pts[s]), s, px, py);
-                return;
+            const int sidx = y * g.n2x + x;
+            uint64_t sm = DNNI_LDG(&smask[sidx]);
+            if (!sm) continue;
+            found = true;
+            const long long SX0 = gx0 + (long long)x * u2, SY0 = gy0 + (long long)y * u2;
+            long long blb = LLONG_MAX;
+            int bm_idx = 0;
+            while (sm) {
+                const int m = ffs64(sm);
+                sm &= sm - 1;
+                const long long BX0 = SX0 + (long long)(m & 7) * u1, BY0 = SY0 + (long long)(m >> 3) * u1;
+                const long long lb = box_lb(px, py, BX0, BX0 + u1 - 1, BY0, BY0 + u1 - 1);
+                if (lb < blb) { blb = lb; bm_idx = m; }
             }
+            const int64_t blk = ((int64_t)sidx << 6) + bm_idx;
+            uint64_t bm = DNNI_LDG(&bmask[blk]);
+            const long long BX0 = SX0 + (long long)(bm_idx & 7) * u1, BY0 = SY0 + (long long)(bm_idx >> 3) * u1;
+            long long qlb = LLONG_MAX;
+            int q_idx = 0;
+            while (bm) {
+                const int l = ffs64(bm);
+                bm &= bm - 1;
+                const long long QX0 = BX0 + (long long)(l & 7) * bs, QY0 = BY0 + (long long)(l >> 3) * bs;
+                const long long lb = box_lb(px, py, QX0, QX0 + bs - 1, QY0, QY0 + bs - 1);
+                if (lb < qlb) { qlb = lb; q_idx = l; }
+            }
+            const int64_t id = (blk << 6) + q_idx;
+            scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
         }
+        if (found) return;
     }
 }
 
-// Exact search inside the disc of the current bound: every superblock, block
-// and bin the disc touches is visited (rows in order of distance from the
-// pixel, columns narrowed per row to the disc's chord), and nothing else.  The
-// bound only shrinks, so cells left out when their row was reached can never
-// hold a closer site.  Complete whenever b holds a real site on entry.
+// Exact search inside the disc of the current bound: every non-empty
+// superblock, block and bin the disc touches is visited (superblock rows in
+// order of distance from the pixel, columns narrowed per row to the disc's
+// chord, empty cells skipped through the occupancy masks), and nothing else.
+// The bound only shrinks, so a cell left out when its row was reached can
+// never hold a closer site.  Complete whenever b holds a real site on entry.
 DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                         const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
                          int px, int py, Best& b) {
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
     const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
@@ -277,31 +328,44 @@ DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const i
         int sx0, sx1;
         cell_range(px, reach_of(b.d2 - gy * gy), gx0, u2, g.n2x, sx0, sx1);
         for (int sx = sx0; sx <= sx1; ++sx) {
+            const int sidx = sy * g.n2x + sx;
+            const uint64_t sm = DNNI_LDG(&smask[sidx]);
+            if (!sm) continue;
             const long long SX0 = gx0 + (long long)sx * u2;
             if (box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) > b.d2) continue;
-            const int64_t sfirst = (int64_t)(sy * g.n2x + sx) << 12;
-            if (DNNI_LDG(&start[sfirst]) == DNNI_LDG(&start[sfirst + kBinsPerSuper])) continue;
-            // blocks of this superblock inside the disc
+            // non-empty blocks of this superblock inside the disc
             for (int ly = 0; ly < kBinsPerBlockEdge; ++ly) {
+                unsigned row = (unsigned)(sm >> (ly * 8)) & 0xFFu;
+                if (!row) continue;
                 const long long BY0 = SY0 + (long long)ly * u1;
                 const long long gyb = axis_gap(py, BY0, BY0 + u1 - 1);
                 if (gyb * gyb > b.d2) continue;
                 int bx0, bx1;
                 cell_range(px - SX0, reach_of(b.d2 - gyb * gyb), 0, u1, kBinsPerBlockEdge, bx0, bx1);
-                for (int lx = bx0; lx <= bx1; ++lx) {
-                    const int64_t bfirst = sfirst + ((int64_t)(ly * 8 + lx) << 6);
-                    if (DNNI_LDG(&start[bfirst]) == DNNI_LDG(&start[bfirst + kBinsPerBlock])) continue;
+                if (bx0 > bx1) continue;
+                row &= bits_between(bx0, bx1);
+                while (row) {
+                    const int lx = ffs64(row);
+                    row &= row - 1;
+                    const int64_t blk = ((int64_t)sidx << 6) + ly * 8 + lx;
+                    const uint64_t bm = DNNI_LDG(&bmask[blk]);
                     const long long BX0 = SX0 + (long long)lx * u1;
-                    // bins of this block inside the disc
+                    // non-empty bins of this block inside the disc, one
+                    // contiguous point range per bin row
                     for (int qy = 0; qy < kBinsPerBlockEdge; ++qy) {
+                        unsigned qrow = (unsigned)(bm >> (qy * 8)) & 0xFFu;
+                        if (!qrow) continue;
                         const long long QY0 = BY0 + (long long)qy * bs;
                         const long long gq = axis_gap(py, QY0, QY0 + bs - 1);
                         if (gq * gq > b.d2) continue;
                         int qx0, qx1;
                         cell_range(px - BX0, reach_of(b.d2 - gq * gq), 0, bs, kBinsPerBlockEdge, qx0, qx1);
                         if (qx0 > qx1) continue;
-                        const int64_t id0 = bfirst + qy * 8;
-                        scan_points(b, pts, DNNI_LDG(&start[id0 + qx0]), DNNI_LDG(&start[id0 + qx1 + 1]), px, py);
+                        qrow &= bits_between(qx0, qx1);
+                        if (!qrow) continue;
+                        const int f = ffs64(qrow), l = 31 - clz32(qrow);
+                        const int64_t id0 = (blk << 6) + qy * 8;
+                        scan_points(b, pts, DNNI_LDG(&start[id0 + f]), DNNI_LDG(&start[id0 + l + 1]), px, py);
                     }
                 }
             }
@@ -327,6 +391,7 @@ DNNI_HD int seed_dim(int n) { return (n + kSeedStride - 1) / kSeedStride; }
 // grid, from the nearest non-empty superblock) and the disc of that bound is
 // searched exhaustively.
 DNNI_HD void nearest_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                            const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
                             int px, int py, Best& b, const SeedGrid* sg = nullptr, int i = 0, int j = 0) {
     if (search_bins(g, pts, start, px, py, b)) return;
     if (sg) {
@@ -340,8 +405,8 @@ DNNI_HD void nearest_search(const BinGrid& g, const int4* __restrict__ pts, cons
             if (q >= 0) consider(b, DNNI_LDG(&pts[q]), q, px, py);
         }
     }
-    if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, px, py, b);
-    search_disc(g, pts, start, px, py, b);
+    if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, bmask, smask, px, py, b);
+    search_disc(g, pts, start, bmask, smask, px, py, b);
 }
 
 // ---------------------------------------------------------------------------
@@ -415,6 +480,30 @@ __global__ void k_bin_scatter(const int32_t* __restrict__ xyz, const uint32_t* _
         const int pos = start[point_bin(g, xr, yr)] + rank[i];
         sorted[pos] = make_int4(xr, yr, xyz[3 * i + 2], (int)(gid ? gid[i] : (uint32_t)i));
     }
+}
+
+// Occupancy masks from the bin starts: one warp per block (bit l = bin l of
+// the block is non-empty), then one warp per superblock (bit m = block m is).
+__global__ void __launch_bounds__(256) k_block_masks(const int* __restrict__ start, int64_t nblocks,
+                                                     uint64_t* __restrict__ bmask) {
+    const int64_t blk = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (blk >= nblocks) return;
+    const int* s = start + (blk << 6);
+    const bool lo = s[lane + 1] != s[lane];
+    const bool hi = s[lane + 33] != s[lane + 32];
+    const unsigned mlo = __ballot_sync(0xffffffffu, lo), mhi = __ballot_sync(0xffffffffu, hi);
+    if (lane == 0) bmask[blk] = (uint64_t)mlo | ((uint64_t)mhi << 32);
+}
+
+__global__ void __launch_bounds__(256) k_super_masks(const uint64_t* __restrict__ bmask, int64_t nsuper,
+                                                     uint64_t* __restrict__ smask) {
+    const int64_t sidx = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (sidx >= nsuper) return;
+    const uint64_t* b = bmask + (sidx << 6);
+    const unsigned mlo = __ballot_sync(0xffffffffu, b[lane] != 0), mhi = __ballot_sync(0xffffffffu, b[lane + 32] != 0);
+    if (lane == 0) smask[sidx] = (uint64_t)mlo | ((uint64_t)mhi << 32);
 }
 
 // ---- exclusive scan of the bin counts (three passes, 4096 items per block) ----
@@ -519,8 +608,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restri
 // ---- nearest site per raster pixel ----
 
 // Exact sites of the seed lattice (no seeds of its own).
-__global__ void __launch_bounds__(128) k_seeds(TileParams t, const int4* __restrict__ pts,
-                                               const int* __restrict__ start, int* __restrict__ seed) {
+__global__ void __launch_bounds__(128, 4) k_seeds(TileParams t, const int4* __restrict__ pts,
+                                               const int* __restrict__ start, const uint64_t* __restrict__ bmask,
+                                               const uint64_t* __restrict__ smask, int* __restrict__ seed) {
     const int nx = seed_dim(t.rw), ny = seed_dim(t.rh);
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= nx * ny) return;
@@ -529,13 +619,14 @@ __global__ void __launch_bounds__(128) k_seeds(TileParams t, const int4* __restr
     i = i < t.rw - 1 ? i : t.rw - 1;
     j = j < t.rh - 1 ? j : t.rh - 1;
     Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-    nearest_search(t.bg, pts, start, (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b);
+    nearest_search(t.bg, pts, start, bmask, smask, (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b);
     seed[a] = b.idx;
 }
 
 // Block 32x8: each warp is 32 consecutive pixels of one raster row.
 __global__ void __launch_bounds__(256) k_nearest(TileParams t, const int4* __restrict__ pts,
-                                                 const int* __restrict__ start, const int* __restrict__ seed,
+                                                 const int* __restrict__ start, const uint64_t* __restrict__ bmask,
+                                                 const uint64_t* __restrict__ smask, const int* __restrict__ seed,
                                                  int2* __restrict__ pix, uint32_t* __restrict__ site,
                                                  Scalars* __restrict__ sc) {
     const int i = blockIdx.x * 32 + threadIdx.x;
@@ -548,7 +639,7 @@ __global__ void __launch_bounds__(256) k_nearest(TileParams t, const int4* __res
         const int py = (t.ry0 + j) * t.cs;
         Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
         const SeedGrid sg{seed, seed_dim(t.rw), seed_dim(t.rh)};
-        nearest_search(t.bg, pts, start, px, py, b, seed ? &sg : nullptr, i, j);
+        nearest_search(t.bg, pts, start, bmask, smask, px, py, b, seed ? &sg : nullptr, i, j);
         const long long q = b.d2 / ((long long)t.cs * t.cs);
         R2 = (int)(q < t.r2cap ? q : t.r2cap);
         z = b.z;

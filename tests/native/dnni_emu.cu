@@ -55,6 +55,14 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
     for (int64_t i = 0; i < n; ++i)
         sorted[fill[pb[i]]++] = make_int4(rel_coord(xyz[3 * i], t.ox), rel_coord(xyz[3 * i + 1], t.oy), xyz[3 * i + 2],
                                           (int)(gid ? gid[i] : (uint32_t)i));
+    const int64_t nblk = g.nbins / kBinsPerBlock, nsup = g.nbins / kBinsPerSuper;
+    std::vector<uint64_t> bmask(nblk, 0), smask(nsup, 0);
+    for (int64_t k = 0; k < nblk; ++k)
+        for (int l = 0; l < 64; ++l)
+            if (start[k * 64 + l + 1] != start[k * 64 + l]) bmask[k] |= 1ull << l;
+    for (int64_t k = 0; k < nsup; ++k)
+        for (int m = 0; m < 64; ++m)
+            if (bmask[k * 64 + m]) smask[k] |= 1ull << m;
     const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
     std::vector<int2> pix(npix);
     int max_r2 = -1;
@@ -66,7 +74,8 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
             i = std::min(i, t.rw - 1);
             j = std::min(j, t.rh - 1);
             Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-            nearest_search(g, sorted.data(), start.data(), (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b);
+            nearest_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), (t.rx0 + i) * t.cs,
+                           (t.ry0 + j) * t.cs, b);
             seeds[a] = b.idx;
         }
     const SeedGrid seedg{seeds.data(), snx, sny};
@@ -76,8 +85,8 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
             uint32_t sg = 0xFFFFFFFFu;
             if (n > 0) {
                 Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-                nearest_search(g, sorted.data(), start.data(), (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b,
-                               seeded ? &seedg : nullptr, i, j);
+                nearest_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), (t.rx0 + i) * t.cs,
+                               (t.ry0 + j) * t.cs, b, seeded ? &seedg : nullptr, i, j);
                 const long long q = b.d2 / ((long long)t.cs * t.cs);
                 R2 = (int)(q < t.r2cap ? q : t.r2cap);
                 z = b.z;
