@@ -81,6 +81,7 @@ struct Scalars {
     int32_t err;
     int32_t packed;              // decided after the nearest-site pass
     int32_t kbits;
+    int32_t nfar[2];             // far worklist lengths (lattice pixels, others)
     int32_t pad;
     long long zbase;
     int32_t max_r2[kStatSlots];
@@ -225,6 +226,60 @@ DNNI_HD bool search_bins(const BinGrid& g, const int4* __restrict__ pts, const i
         if (ring_done(b.d2, px, py, gx0, gy0, bs, bx - k, bx + k, by - k, by + k, g.nbx, g.nby)) return true;
     }
     return false;
+}
+
+// A tile's staged bin window: the bins [wx0, wx0+wnx) x [wy0, wy0+wny) with
+// their points copied (to shared memory) in window row-major bin order.
+struct BinWindow {
+    int wx0, wy0, wnx, wny;
+    const int* lstart;   // wnx*wny+1 starts into lpts
+    const int* gstart;   // sorted-array position of each window bin's first point
+    const int4* lpts;
+};
+
+// search_bins on a staged window; identical results.  Every bin within
+// kRingsBins rings of the pixel's bin (inside the grid) must lie in the window.
+DNNI_HD bool search_bins_window(const BinGrid& g, const BinWindow& w, int px, int py, Best& b) {
+    const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    int bx = (int)(((long long)px - gx0) / bs);
+    int by = (int)(((long long)py - gy0) / bs);
+    bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
+    by = by < g.nby - 1 ? by : g.nby - 1;
+    for (int k = 0; k <= kRingsBins; ++k) {
+        const int ne = ring_size(k);
+        for (int e = 0; e < ne; ++e) {
+            int x, y;
+            ring_cell(bx, by, k, e, x, y);
+            if (x < 0 || y < 0 || x >= g.nbx || y >= g.nby) continue;
+            const long long X0 = gx0 + (long long)x * bs, Y0 = gy0 + (long long)y * bs;
+            if (k > 0 && box_lb(px, py, X0, X0 + bs - 1, Y0, Y0 + bs - 1) > b.d2) continue;
+            const int lk = (y - w.wy0) * w.wnx + (x - w.wx0);
+            const int s0 = w.lstart[lk], e0 = w.lstart[lk + 1], g0 = w.gstart[lk];
+            for (int q = s0; q < e0; ++q) consider(b, w.lpts[q], g0 + (q - s0), px, py);
+        }
+        if (ring_done(b.d2, px, py, gx0, gy0, bs, bx - k, bx + k, by - k, by + k, g.nbx, g.nby)) return true;
+    }
+    return false;
+}
+
+// Window of the 32 x 8 pixel tile whose first pixel is raster (i0, j0).
+constexpr int kTileX = 32, kTileY = 8;
+DNNI_HD void tile_window(const TileParams& t, int i0, int j0, int& wx0, int& wy0, int& wnx, int& wny) {
+    const BinGrid& g = t.bg;
+    const int i1 = (i0 + kTileX - 1 < t.rw - 1) ? i0 + kTileX - 1 : t.rw - 1;
+    const int j1 = (j0 + kTileY - 1 < t.rh - 1) ? j0 + kTileY - 1 : t.rh - 1;
+    long long bxa = ((long long)(t.rx0 + i0) * t.cs - g.gx0) / g.bs, bxb = ((long long)(t.rx0 + i1) * t.cs - g.gx0) / g.bs;
+    long long bya = ((long long)(t.ry0 + j0) * t.cs - g.gy0) / g.bs, byb = ((long long)(t.ry0 + j1) * t.cs - g.gy0) / g.bs;
+    bxa = bxa < g.nbx - 1 ? bxa : g.nbx - 1;
+    bxb = bxb < g.nbx - 1 ? bxb : g.nbx - 1;
+    bya = bya < g.nby - 1 ? bya : g.nby - 1;
+    byb = byb < g.nby - 1 ? byb : g.nby - 1;
+    const long long x0 = bxa - kRingsBins > 0 ? bxa - kRingsBins : 0, x1 = bxb + kRingsBins < g.nbx - 1 ? bxb + kRingsBins : g.nbx - 1;
+    const long long y0 = bya - kRingsBins > 0 ? bya - kRingsBins : 0, y1 = byb + kRingsBins < g.nby - 1 ? byb + kRingsBins : g.nby - 1;
+    wx0 = (int)x0;
+    wy0 = (int)y0;
+    wnx = (int)(x1 - x0 + 1);
+    wny = (int)(y1 - y0 + 1);
 }
 
 // Occupancy masks: bit l of bmask[block] is set when bin l of that block
@@ -373,9 +428,9 @@ DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const i
     }
 }
 
-// Sites of a coarse lattice of raster pixels (every kSeedStride-th pixel in
-// each direction, offset by half a stride), solved exactly first; their sites
-// bound the nearest-site distance of the pixels around them.
+// Seed lattice: raster pixels (i,j) with i % kSeedStride == j % kSeedStride
+// == kSeedStride/2.  Their sites are found first (without seeds); they bound
+// the nearest-site distance of the pixels around them.
 constexpr int kSeedStride = 16;
 
 struct SeedGrid {
@@ -383,30 +438,46 @@ struct SeedGrid {
     int nx, ny;
 };
 
-DNNI_HD int seed_dim(int n) { return (n + kSeedStride - 1) / kSeedStride; }
+DNNI_HD int seed_dim(int n) { return (n + kSeedStride / 2 - 1) / kSeedStride; }
+DNNI_HD bool is_seed_pixel(int i, int j) {
+    return (i % kSeedStride) == kSeedStride / 2 && (j % kSeedStride) == kSeedStride / 2;
+}
+
+// The sites of the (up to) four lattice pixels around raster pixel (i,j).
+DNNI_HD void consider_seeds(const SeedGrid& sg, const int4* __restrict__ pts, int i, int j, int px, int py,
+                            Best& b) {
+    if (sg.nx <= 0 || sg.ny <= 0) return;
+    int a = i < kSeedStride / 2 ? 0 : (i - kSeedStride / 2) / kSeedStride;
+    int c = j < kSeedStride / 2 ? 0 : (j - kSeedStride / 2) / kSeedStride;
+    a = a > sg.nx - 1 ? sg.nx - 1 : a;
+    c = c > sg.ny - 1 ? sg.ny - 1 : c;
+    const int a1 = a + 1 < sg.nx ? a + 1 : a, c1 = c + 1 < sg.ny ? c + 1 : c;
+    const int cand[4] = {c * sg.nx + a, c * sg.nx + a1, c1 * sg.nx + a, c1 * sg.nx + a1};
+    for (int k = 0; k < 4; ++k) {
+        const int q = DNNI_LDG(&sg.idx[cand[k]]);
+        if (q >= 0) consider(b, DNNI_LDG(&pts[q]), q, px, py);
+    }
+}
+
+// Completes the search of a pixel that the bin rings did not settle: the
+// bound so far (b), the lattice sites around it (when sg is given) or else
+// the nearest non-empty superblock give a real site, and the disc of that
+// bound is searched exhaustively.
+DNNI_HD void finish_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                           const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
+                           int px, int py, Best& b, const SeedGrid* sg, int i, int j) {
+    if (sg) consider_seeds(*sg, pts, i, j, px, py, b);
+    if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, bmask, smask, px, py, b);
+    search_disc(g, pts, start, bmask, smask, px, py, b);
+}
 
 // Exact nearest site of raster pixel (i,j) at (px,py) (LAS units relative to
-// the WP origin).  Bin rings settle pixels among dense points; otherwise the
-// bound is seeded from the four surrounding lattice sites (or, without a seed
-// grid, from the nearest non-empty superblock) and the disc of that bound is
-// searched exhaustively.
+// the WP origin), all levels in one call.
 DNNI_HD void nearest_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                             const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
                             int px, int py, Best& b, const SeedGrid* sg = nullptr, int i = 0, int j = 0) {
     if (search_bins(g, pts, start, px, py, b)) return;
-    if (sg) {
-        int a = (i - kSeedStride / 2) / kSeedStride, c = (j - kSeedStride / 2) / kSeedStride;
-        a = a < 0 ? 0 : (a > sg->nx - 1 ? sg->nx - 1 : a);
-        c = c < 0 ? 0 : (c > sg->ny - 1 ? sg->ny - 1 : c);
-        const int a1 = a + 1 < sg->nx ? a + 1 : a, c1 = c + 1 < sg->ny ? c + 1 : c;
-        const int cand[4] = {c * sg->nx + a, c * sg->nx + a1, c1 * sg->nx + a, c1 * sg->nx + a1};
-        for (int k = 0; k < 4; ++k) {
-            const int q = DNNI_LDG(&sg->idx[cand[k]]);
-            if (q >= 0) consider(b, DNNI_LDG(&pts[q]), q, px, py);
-        }
-    }
-    if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, bmask, smask, px, py, b);
-    search_disc(g, pts, start, bmask, smask, px, py, b);
+    finish_search(g, pts, start, bmask, smask, px, py, b, sg, i, j);
 }
 
 // ---------------------------------------------------------------------------
@@ -420,6 +491,7 @@ __global__ void k_init_scalars(Scalars* sc) {
         sc->bbox[2] = INT_MAX; sc->bbox[3] = INT_MIN;
         sc->bbox[4] = INT_MAX; sc->bbox[5] = INT_MIN;
         sc->err = 0; sc->packed = 0; sc->kbits = 0; sc->zbase = 0;
+        sc->nfar[0] = 0; sc->nfar[1] = 0;
     }
     if (l < kStatSlots) {
         sc->max_r2[l] = -1; sc->big_pixels[l] = 0; sc->spans[l] = 0; sc->nodata[l] = 0;
@@ -607,59 +679,178 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restri
 
 // ---- nearest site per raster pixel ----
 
-// Exact sites of the seed lattice (no seeds of its own).
-__global__ void __launch_bounds__(128, 4) k_seeds(TileParams t, const int4* __restrict__ pts,
-                                               const int* __restrict__ start, const uint64_t* __restrict__ bmask,
-                                               const uint64_t* __restrict__ smask, int* __restrict__ seed) {
-    const int nx = seed_dim(t.rw), ny = seed_dim(t.rh);
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= nx * ny) return;
-    const int sx = a % nx, sy = a / nx;
-    int i = sx * kSeedStride + kSeedStride / 2, j = sy * kSeedStride + kSeedStride / 2;
-    i = i < t.rw - 1 ? i : t.rw - 1;
-    j = j < t.rh - 1 ? j : t.rh - 1;
-    Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-    nearest_search(t.bg, pts, start, bmask, smask, (t.rx0 + i) * t.cs, (t.ry0 + j) * t.cs, b);
-    seed[a] = b.idx;
+constexpr int kWinMaxBins = 2048;
+constexpr int kWinMaxPts = 3072;
+constexpr size_t kDenseSmem = sizeof(int4) * kWinMaxPts + sizeof(int) * (2 * kWinMaxBins + 1);
+
+// Records a settled pixel: its record, site, lattice seed and work figures.
+__device__ __forceinline__ void settle_pixel(const TileParams& t, int i, int j, const Best& b, int2* __restrict__ pix,
+                                             uint32_t* __restrict__ site, int* __restrict__ seed) {
+    const long long q = b.d2 / ((long long)t.cs * t.cs);
+    const int R2 = (int)(q < t.r2cap ? q : t.r2cap);
+    const int64_t o = (int64_t)j * t.rw + i;
+    pix[o] = make_int2(b.z, R2);
+    if (site) site[o] = b.gid;
+    if (seed && is_seed_pixel(i, j)) seed[(j / kSeedStride) * seed_dim(t.rw) + i / kSeedStride] = b.idx;
 }
 
-// Block 32x8: each warp is 32 consecutive pixels of one raster row.
-__global__ void __launch_bounds__(256) k_nearest(TileParams t, const int4* __restrict__ pts,
-                                                 const int* __restrict__ start, const uint64_t* __restrict__ bmask,
-                                                 const uint64_t* __restrict__ smask, const int* __restrict__ seed,
-                                                 int2* __restrict__ pix, uint32_t* __restrict__ site,
-                                                 Scalars* __restrict__ sc) {
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
-    const bool valid = i < t.rw && j < t.rh;
-    int R2 = -1, z = 0;
-    uint32_t gid = 0xFFFFFFFFu;
-    if (valid && t.npts > 0) {
-        const int px = (t.rx0 + i) * t.cs;
-        const int py = (t.ry0 + j) * t.cs;
-        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-        const SeedGrid sg{seed, seed_dim(t.rw), seed_dim(t.rh)};
-        nearest_search(t.bg, pts, start, bmask, smask, px, py, b, seed ? &sg : nullptr, i, j);
-        const long long q = b.d2 / ((long long)t.cs * t.cs);
-        R2 = (int)(q < t.r2cap ? q : t.r2cap);
-        z = b.z;
-        gid = b.gid;
-    }
-    if (valid) {
-        const int64_t o = (int64_t)j * t.rw + i;
-        pix[o] = make_int2(z, R2);
-        if (site) site[o] = gid;
-    }
+__device__ __forceinline__ void warp_stats(const TileParams& t, int R2, Scalars* __restrict__ sc, int slot) {
     const int rs2 = t.rs * t.rs;
     const unsigned big = (R2 > rs2) ? 1u : 0u;
     const unsigned sp = big ? 2u * (unsigned)isqrt_i32(R2) + 1u : 0u;
     const unsigned nbig = __reduce_add_sync(0xffffffffu, big);
     const unsigned nsp = __reduce_add_sync(0xffffffffu, sp);
     const int mx = __reduce_max_sync(0xffffffffu, R2);
-    if (threadIdx.x == 0) {
-        const int slot = (blockIdx.x + blockIdx.y * 7 + threadIdx.y) & (kStatSlots - 1);
-        if (nbig) { atomicAdd(&sc->big_pixels[slot], (unsigned long long)nbig); atomicAdd(&sc->spans[slot], (unsigned long long)nsp); }
+    if ((threadIdx.x & 31) == 0) {
+        slot &= kStatSlots - 1;
+        if (nbig) {
+            atomicAdd(&sc->big_pixels[slot], (unsigned long long)nbig);
+            atomicAdd(&sc->spans[slot], (unsigned long long)nsp);
+        }
         if (mx >= 0) atomicMax(&sc->max_r2[slot], mx);
+    }
+}
+
+// Dense pass.  One CTA per 32 x 8 pixel tile (blockDim 256, warp = one
+// pixel row of the tile): the tile's bin window (bin rings of every pixel)
+// is staged in shared memory and the rings are searched there; windows too
+// large for shared memory use the global arrays.  Pixels the rings do not
+// settle go to the far worklist: lattice pixels from the front (count
+// sc->nfar[0]), the others from the back (count sc->nfar[1]), each with its
+// best site so far.  With no points every pixel is settled as "no site".
+__global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __restrict__ pts,
+                                                    const int* __restrict__ start, int* __restrict__ seed,
+                                                    int2* __restrict__ pix, uint32_t* __restrict__ site,
+                                                    int2* __restrict__ far, Scalars* __restrict__ sc) {
+    extern __shared__ int4 smem[];
+    int4* s_pts = smem;
+    int* s_lstart = (int*)(smem + kWinMaxPts);
+    int* s_gstart = s_lstart + kWinMaxBins + 1;
+    __shared__ int wsum[8];
+    __shared__ int s_total;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int i0 = blockIdx.x * kTileX, j0 = blockIdx.y * kTileY;
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    const bool valid = i < t.rw && j < t.rh;
+    const BinGrid& g = t.bg;
+    int wx0 = 0, wy0 = 0, wnx = 0, wny = 0;
+    bool staged = false;
+    if (t.npts > 0) {
+        tile_window(t, i0, j0, wx0, wy0, wnx, wny);
+        const int nwb = wnx * wny;
+        if (nwb <= kWinMaxBins) {
+            // per-bin counts -> local starts (8 consecutive bins per thread)
+            int c[8], sum = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int lk = tid * 8 + k;
+                c[k] = 0;
+                if (lk < nwb) {
+                    const int64_t id = bin_id(g, wx0 + lk % wnx, wy0 + lk / wnx);
+                    const int gs = __ldg(&start[id]);
+                    c[k] = __ldg(&start[id + 1]) - gs;
+                    s_gstart[lk] = gs;
+                }
+                sum += c[k];
+            }
+            int total;
+            int run = block_exclusive_sum(sum, wsum, total);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int lk = tid * 8 + k;
+                if (lk < nwb) s_lstart[lk] = run;
+                run += c[k];
+            }
+            if (tid == 0) { s_lstart[nwb] = total; s_total = total; }
+            __syncthreads();
+            staged = s_total <= kWinMaxPts;
+            if (staged) {
+                // copy the window's points, one point per thread per pass
+                for (int q = tid; q < s_total; q += 256) {
+                    int lo = 0, hi = nwb - 1;           // last bin with lstart <= q
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (s_lstart[mid] <= q) lo = mid; else hi = mid - 1;
+                    }
+                    s_pts[q] = __ldg(&pts[s_gstart[lo] + (q - s_lstart[lo])]);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    int R2 = -1;
+    bool far_pixel = false;
+    Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+    if (valid) {
+        if (t.npts > 0) {
+            const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
+            bool done;
+            if (staged) {
+                const BinWindow w{wx0, wy0, wnx, wny, s_lstart, s_gstart, s_pts};
+                done = search_bins_window(g, w, px, py, b);
+            } else {
+                done = search_bins(g, pts, start, px, py, b);
+            }
+            if (done) {
+                settle_pixel(t, i, j, b, pix, site, seed);
+                const long long q = b.d2 / ((long long)t.cs * t.cs);
+                R2 = (int)(q < t.r2cap ? q : t.r2cap);
+            } else {
+                far_pixel = true;
+            }
+        } else {
+            const int64_t o = (int64_t)j * t.rw + i;
+            pix[o] = make_int2(0, -1);
+            if (site) site[o] = 0xFFFFFFFFu;
+        }
+    }
+    // worklist append, warp-aggregated
+    const bool lat = far_pixel && is_seed_pixel(i, j);
+    const bool oth = far_pixel && !lat;
+    const unsigned mlat = __ballot_sync(0xffffffffu, lat), moth = __ballot_sync(0xffffffffu, oth);
+    const int lane = threadIdx.x;
+    int base_lat = 0, base_oth = 0;
+    if (lane == 0) {
+        if (mlat) base_lat = atomicAdd(&sc->nfar[0], __popc(mlat));
+        if (moth) base_oth = atomicAdd(&sc->nfar[1], __popc(moth));
+    }
+    base_lat = __shfl_sync(0xffffffffu, base_lat, 0);
+    base_oth = __shfl_sync(0xffffffffu, base_oth, 0);
+    const unsigned below = (1u << lane) - 1u;
+    const int2 item = make_int2(j * t.rw + i, b.idx);
+    if (lat) far[base_lat + __popc(mlat & below)] = item;
+    if (oth) far[(int64_t)t.rw * t.rh - 1 - (base_oth + __popc(moth & below))] = item;
+    warp_stats(t, R2, sc, blockIdx.x + blockIdx.y * 7 + threadIdx.y);
+}
+
+// Far pass over one worklist (front: lattice pixels, unseeded, writing their
+// seeds; back: the rest, seeded by the lattice).  Grid-stride over the items,
+// a warp takes 32 consecutive ones (neighbouring pixels of one tile row).
+__global__ void __launch_bounds__(256) k_near_far(TileParams t, const int4* __restrict__ pts,
+                                                  const int* __restrict__ start, const uint64_t* __restrict__ bmask,
+                                                  const uint64_t* __restrict__ smask, int* __restrict__ seed,
+                                                  int seeded, const int2* __restrict__ far, int which,
+                                                  int2* __restrict__ pix, uint32_t* __restrict__ site,
+                                                  Scalars* __restrict__ sc) {
+    const int count = sc->nfar[which];
+    const int64_t npix = (int64_t)t.rw * t.rh;
+    const int lane = threadIdx.x & 31;
+    const SeedGrid sg{seed, seed_dim(t.rw), seed_dim(t.rh)};
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += gridDim.x * blockDim.x) {
+        const int it = base + lane;
+        int R2 = -1;
+        if (it < count) {
+            const int2 item = which ? far[npix - 1 - it] : far[it];
+            const int i = item.x % t.rw, j = item.x / t.rw;
+            const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
+            Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+            if (item.y >= 0) consider(b, __ldg(&pts[item.y]), item.y, px, py);
+            finish_search(t.bg, pts, start, bmask, smask, px, py, b, seeded ? &sg : nullptr, i, j);
+            settle_pixel(t, i, j, b, pix, site, seeded ? nullptr : seed);
+            const long long q = b.d2 / ((long long)t.cs * t.cs);
+            R2 = (int)(q < t.r2cap ? q : t.r2cap);
+        }
+        warp_stats(t, R2, sc, blockIdx.x * 3 + (threadIdx.x >> 5));
     }
 }
 

@@ -67,35 +67,74 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
     std::vector<int2> pix(npix);
     int max_r2 = -1;
     const int snx = seed_dim(t.rw), sny = seed_dim(t.rh);
-    std::vector<int> seeds(n > 0 ? snx * sny : 1, -1);
-    if (n > 0)
-        for (int a = 0; a < snx * sny; ++a) {
-            int i = (a % snx) * kSeedStride + kSeedStride / 2, j = (a / snx) * kSeedStride + kSeedStride / 2;
-            i = std::min(i, t.rw - 1);
-            j = std::min(j, t.rh - 1);
-            Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-            nearest_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), (t.rx0 + i) * t.cs,
-                           (t.ry0 + j) * t.cs, b);
-            seeds[a] = b.idx;
-        }
+    std::vector<int> seeds(std::max(1, snx * sny), -1);
     const SeedGrid seedg{seeds.data(), snx, sny};
-    for (int j = 0; j < t.rh; ++j)
-        for (int i = 0; i < t.rw; ++i) {
-            int R2 = -1, z = 0;
-            uint32_t sg = 0xFFFFFFFFu;
+    std::vector<int2> farA, farB;   // (pixel, best so far)
+    auto settle = [&](int i, int j, const Best& b) {
+        const long long q = b.d2 / ((long long)t.cs * t.cs);
+        const int R2 = (int)(q < t.r2cap ? q : t.r2cap);
+        pix[(int64_t)j * t.rw + i] = make_int2(b.z, R2);
+        if (site) site[(int64_t)j * t.rw + i] = b.gid;
+        if (r2_out) r2_out[(int64_t)j * t.rw + i] = R2;
+        max_r2 = std::max(max_r2, R2);
+        if (is_seed_pixel(i, j)) seeds[(j / kSeedStride) * snx + i / kSeedStride] = b.idx;
+    };
+    // dense pass: per 32 x 8 tile, staged window (as the device kernel) or the global arrays
+    std::vector<int> lstart(kWinMaxBins + 1), gstart(kWinMaxBins);
+    std::vector<int4> lpts(kWinMaxPts);
+    for (int j0 = 0; j0 < t.rh; j0 += kTileY)
+        for (int i0 = 0; i0 < t.rw; i0 += kTileX) {
+            bool staged = false;
+            int wx0 = 0, wy0 = 0, wnx = 0, wny = 0;
             if (n > 0) {
-                Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-                nearest_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), (t.rx0 + i) * t.cs,
-                               (t.ry0 + j) * t.cs, b, seeded ? &seedg : nullptr, i, j);
-                const long long q = b.d2 / ((long long)t.cs * t.cs);
-                R2 = (int)(q < t.r2cap ? q : t.r2cap);
-                z = b.z;
-                sg = b.gid;
+                tile_window(t, i0, j0, wx0, wy0, wnx, wny);
+                const int nwb = wnx * wny;
+                if (nwb <= kWinMaxBins) {
+                    int run2 = 0;
+                    for (int lk = 0; lk < nwb; ++lk) {
+                        const int64_t id = bin_id(g, wx0 + lk % wnx, wy0 + lk / wnx);
+                        lstart[lk] = run2;
+                        gstart[lk] = start[id];
+                        run2 += start[id + 1] - start[id];
+                    }
+                    lstart[nwb] = run2;
+                    staged = run2 <= kWinMaxPts;
+                    if (staged)
+                        for (int lk = 0; lk < nwb; ++lk)
+                            for (int q = lstart[lk]; q < lstart[lk + 1]; ++q) lpts[q] = sorted[gstart[lk] + (q - lstart[lk])];
+                }
             }
-            pix[(int64_t)j * t.rw + i] = make_int2(z, R2);
-            if (site) site[(int64_t)j * t.rw + i] = sg;
-            if (r2_out) r2_out[(int64_t)j * t.rw + i] = R2;
-            max_r2 = std::max(max_r2, R2);
+            for (int j = j0; j < std::min(j0 + kTileY, t.rh); ++j)
+                for (int i = i0; i < std::min(i0 + kTileX, t.rw); ++i) {
+                    if (n == 0) {
+                        pix[(int64_t)j * t.rw + i] = make_int2(0, -1);
+                        if (site) site[(int64_t)j * t.rw + i] = 0xFFFFFFFFu;
+                        if (r2_out) r2_out[(int64_t)j * t.rw + i] = -1;
+                        continue;
+                    }
+                    const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
+                    Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+                    bool done;
+                    if (staged) {
+                        const BinWindow w{wx0, wy0, wnx, wny, lstart.data(), gstart.data(), lpts.data()};
+                        done = search_bins_window(g, w, px, py, b);
+                    } else {
+                        done = search_bins(g, sorted.data(), start.data(), px, py, b);
+                    }
+                    if (done) settle(i, j, b);
+                    else (is_seed_pixel(i, j) ? farA : farB).push_back(make_int2(j * t.rw + i, b.idx));
+                }
+        }
+    // far passes: lattice pixels unseeded, then the rest seeded
+    for (int pass = 0; pass < 2; ++pass)
+        for (const int2& it : (pass ? farB : farA)) {
+            const int i = it.x % t.rw, j = it.x / t.rw;
+            const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
+            Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+            if (it.y >= 0) consider(b, sorted[it.y], it.y, px, py);
+            finish_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), px, py, b,
+                          (pass && seeded) ? &seedg : nullptr, i, j);
+            settle(i, j, b);
         }
     int packed, K;
     long long zbase;

@@ -148,3 +148,14 @@ def test_sinusoid_512_full_size(eng, oracle):
     assert np.array_equal(site, ref["site"]) and _same(h, ref["h"])
     mx, rms = _fp64_err(oracle, ref, h, wp)
     assert mx <= TOL_M and st.nodata_cells == 0
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_engine_window_fallbacks(oracle, k):
+    from terranni_b200 import engine
+    from test_kernel_logic_host import _fallback_cases
+    xyz, side, cs, bt = _fallback_cases()[k]
+    ref = oracle.interpolate(oracle.make_wp(side, side, cs), xyz)
+    with engine.Engine(device=0, bin_target=bt) as e:
+        h, site, _ = e.interpolate(engine.make_wp(side, side, cs), xyz, site=True)
+    assert np.array_equal(site, ref["site"]) and _same(h, ref["h"])

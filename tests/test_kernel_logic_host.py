@@ -87,3 +87,24 @@ def test_host_build_span_count_matches_oracle(emu, oracle):
     big = r2 > 9
     assert r["info"]["big_pixels"] == int(big.sum())
     assert r["info"]["spans"] == int((2 * np.floor(np.sqrt(r2[big].astype(np.float64))) + 1).sum())
+
+
+def _fallback_cases():
+    rng = np.random.default_rng(77)
+    # a dense cluster: a tile's bin window holds more points than shared memory
+    dense = np.concatenate([
+        np.stack([rng.integers(2000, 2600, 60000), rng.integers(3000, 3400, 60000), rng.integers(0, 9000, 60000)], 1),
+        np.stack([rng.integers(0, 6400, 3000), rng.integers(0, 6400, 3000), rng.integers(0, 9000, 3000)], 1)])
+    # cells much larger than bins: a tile's bin window has too many bins
+    coarse = np.stack([rng.integers(0, 64 * 2000, 400000), rng.integers(0, 64 * 2000, 400000),
+                       rng.integers(0, 9000, 400000)], 1)
+    return [(dense.astype(np.int32), 64, 100, 0), (coarse.astype(np.int32), 64, 2000, 1)]
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_host_build_window_fallbacks(emu, oracle, k):
+    xyz, side, cs, bt = _fallback_cases()[k]
+    wp = oracle.make_wp(side, side, cs)
+    ref = oracle.interpolate(wp, xyz)
+    rc, r = emu(wp, xyz, bin_target=bt)
+    assert rc == 0 and np.array_equal(r["site"], ref["site"]) and _same(r["h"], ref["h"])
