@@ -262,6 +262,63 @@ DNNI_HD bool search_bins_window(const BinGrid& g, const BinWindow& w, int px, in
     return false;
 }
 
+// The bin rings of search_bins_window with contiguous ranges: in the staged
+// window's row-major order each row of a pixel's 3 x 3 (then 5 x 5) bin
+// neighbourhood is one run of points, so rings 0-1 are three loops and ring 2
+// is two rows plus two columns.  b.idx holds a window-local point index on
+// return (window_global_index converts it).  Same result as search_bins.
+DNNI_HD void scan_local(Best& b, const int4* lpts, int s, int e, int px, int py) {
+    for (int q = s; q < e; ++q) consider(b, lpts[q], q, px, py);
+}
+
+DNNI_HD bool search_window_fast(const BinGrid& g, const BinWindow& w, int px, int py, Best& b) {
+    const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    int bx = (int)(((long long)px - gx0) / bs);
+    int by = (int)(((long long)py - gy0) / bs);
+    bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
+    by = by < g.nby - 1 ? by : g.nby - 1;
+    const int lx = bx - w.wx0, ly = by - w.wy0;
+    {
+        const int x0 = lx - 1 > 0 ? lx - 1 : 0, x1 = lx + 1 < w.wnx - 1 ? lx + 1 : w.wnx - 1;
+        const int y0 = ly - 1 > 0 ? ly - 1 : 0, y1 = ly + 1 < w.wny - 1 ? ly + 1 : w.wny - 1;
+        for (int r = y0; r <= y1; ++r) scan_local(b, w.lpts, w.lstart[r * w.wnx + x0], w.lstart[r * w.wnx + x1 + 1], px, py);
+    }
+    if (ring_done(b.d2, px, py, gx0, gy0, bs, bx - 1, bx + 1, by - 1, by + 1, g.nbx, g.nby)) return true;
+    {
+        const int x0 = lx - 2 > 0 ? lx - 2 : 0, x1 = lx + 2 < w.wnx - 1 ? lx + 2 : w.wnx - 1;
+        const long long X0 = gx0 + (long long)(w.wx0 + x0) * bs, X1 = gx0 + (long long)(w.wx0 + x1 + 1) * bs - 1;
+        for (int d = -2; d <= 2; d += 4) {
+            const int r = ly + d;
+            if (r < 0 || r >= w.wny) continue;
+            const long long Y0 = gy0 + (long long)(w.wy0 + r) * bs;
+            if (box_lb(px, py, X0, X1, Y0, Y0 + bs - 1) > b.d2) continue;
+            scan_local(b, w.lpts, w.lstart[r * w.wnx + x0], w.lstart[r * w.wnx + x1 + 1], px, py);
+        }
+        const int ya = ly - 1 > 0 ? ly - 1 : 0, yb = ly + 1 < w.wny - 1 ? ly + 1 : w.wny - 1;
+        const long long Y0 = gy0 + (long long)(w.wy0 + ya) * bs, Y1 = gy0 + (long long)(w.wy0 + yb + 1) * bs - 1;
+        for (int d = -2; d <= 2; d += 4) {
+            const int c = lx + d;
+            if (c < 0 || c >= w.wnx) continue;
+            const long long CX0 = gx0 + (long long)(w.wx0 + c) * bs;
+            if (box_lb(px, py, CX0, CX0 + bs - 1, Y0, Y1) > b.d2) continue;
+            for (int r = ya; r <= yb; ++r)
+                scan_local(b, w.lpts, w.lstart[r * w.wnx + c], w.lstart[r * w.wnx + c + 1], px, py);
+        }
+    }
+    return ring_done(b.d2, px, py, gx0, gy0, bs, bx - 2, bx + 2, by - 2, by + 2, g.nbx, g.nby);
+}
+
+// Sorted-array position of window-local point q (-1 stays -1).
+DNNI_HD int window_global_index(const BinWindow& w, int q) {
+    if (q < 0) return -1;
+    int lo = 0, hi = w.wnx * w.wny - 1;     // last bin with lstart <= q
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (w.lstart[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    return w.gstart[lo] + (q - w.lstart[lo]);
+}
+
 // Window of the 32 x 8 pixel tile whose first pixel is raster (i0, j0).
 constexpr int kTileX = 32, kTileY = 8;
 DNNI_HD void tile_window(const TileParams& t, int i0, int j0, int& wx0, int& wy0, int& wnx, int& wny) {
@@ -584,10 +641,12 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
+// Exclusive block-wide sum over 256 threads (8 warps).  tid is the thread's
+// linear index in the block (warps are formed from linear indices), so the
+// helper works for any block shape with 256 threads.
 template <typename T>
-__device__ __forceinline__ T block_exclusive_sum(T v, T* wsum, T& total) {
-    // blockDim.x == kScanThreads (8 warps)
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ __forceinline__ T block_exclusive_sum(T v, T* wsum, T& total, int tid) {
+    const int lane = tid & 31, warp = tid >> 5;
     T x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -622,7 +681,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_partial(const int* __rest
         if (idx < m) s += cnt[idx];
     }
     int total;
-    block_exclusive_sum(s, wsum, total);
+    block_exclusive_sum(s, wsum, total, (int)threadIdx.x);
     if (threadIdx.x == 0) bsum[blockIdx.x] = total;
 }
 
@@ -665,7 +724,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restri
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) { v[k] = tile[threadIdx.x * kScanItems + k]; s += v[k]; }
     int total;
-    int run = block_exclusive_sum(s, wsum, total) + bsum[blockIdx.x];
+    int run = block_exclusive_sum(s, wsum, total, (int)threadIdx.x) + bsum[blockIdx.x];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) { tile[threadIdx.x * kScanItems + k] = run; run += v[k]; }
     __syncthreads();
@@ -754,7 +813,7 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
                 sum += c[k];
             }
             int total;
-            int run = block_exclusive_sum(sum, wsum, total);
+            int run = block_exclusive_sum(sum, wsum, total, tid);
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const int lk = tid * 8 + k;
@@ -787,7 +846,8 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
             bool done;
             if (staged) {
                 const BinWindow w{wx0, wy0, wnx, wny, s_lstart, s_gstart, s_pts};
-                done = search_bins_window(g, w, px, py, b);
+                done = search_window_fast(g, w, px, py, b);
+                b.idx = window_global_index(w, b.idx);
             } else {
                 done = search_bins(g, pts, start, px, py, b);
             }
@@ -974,7 +1034,7 @@ __global__ void __launch_bounds__(kScanThreads) k_rowscan(T* __restrict__ D, int
         for (int k = 0; k < 4; ++k) v[k] = (idx + k < ncols) ? row[idx + k] : T(0);
         v[1] += v[0]; v[2] += v[1]; v[3] += v[2];
         T total;
-        const T excl = block_exclusive_sum(v[3], wsum, total) + carry;
+        const T excl = block_exclusive_sum(v[3], wsum, total, (int)threadIdx.x) + carry;
 #pragma unroll
         for (int k = 0; k < 4; ++k) if (idx + k < ncols) row[idx + k] = v[k] + excl;
         carry += total;

@@ -117,7 +117,8 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
                     bool done;
                     if (staged) {
                         const BinWindow w{wx0, wy0, wnx, wny, lstart.data(), gstart.data(), lpts.data()};
-                        done = search_bins_window(g, w, px, py, b);
+                        done = search_window_fast(g, w, px, py, b);
+                        b.idx = window_global_index(w, b.idx);
                     } else {
                         done = search_bins(g, sorted.data(), start.data(), px, py, b);
                     }
