@@ -102,6 +102,21 @@ DNNI_HD int isqrt_i32(int v) {
     return s;
 }
 
+// a / b for 0 <= a < 2^32, 0 < b < 2^32 (32-bit unsigned divide; a 64-bit
+// divide costs several times more on the GPU)
+DNNI_HD int udiv32(long long a, long long b) { return (int)((uint32_t)a / (uint32_t)b); }
+
+// min(floor(d2 / cs2), cap) exactly: the quotient estimate from doubles is
+// within one of the truth for quotients below 2^31, and is then corrected
+// with exact products.
+DNNI_HD int r2_of(long long d2, long long cs2, int cap) {
+    if (d2 >= ((long long)cap + 1) * cs2) return cap;
+    long long q = (long long)((double)d2 / (double)cs2);
+    while (q > 0 && q * cs2 > d2) --q;
+    while ((q + 1) * cs2 <= d2) ++q;
+    return (int)(q < cap ? q : cap);
+}
+
 DNNI_HD int64_t bin_id(const BinGrid& g, int bx, int by) {
     const int sx = bx >> 6, sy = by >> 6;
     const int bkx = (bx >> 3) & 7, bky = (by >> 3) & 7;
@@ -199,8 +214,8 @@ DNNI_HD void cell_range(long long c, long long w, long long o, long long u, int 
     if (b < o || a > end) { lo = 1; hi = 0; return; }
     if (a < o) a = o;
     if (b > end) b = end;
-    lo = (int)((a - o) / u);
-    hi = (int)((b - o) / u);
+    lo = udiv32(a - o, u);
+    hi = udiv32(b - o, u);
 }
 
 // Level 0 of the search: bin rings 0..kRingsBins around the pixel's bin.
@@ -208,8 +223,8 @@ DNNI_HD void cell_range(long long c, long long w, long long o, long long u, int 
 DNNI_HD bool search_bins(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                          int px, int py, Best& b) {
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
-    int bx = (int)(((long long)px - gx0) / bs);
-    int by = (int)(((long long)py - gy0) / bs);
+    int bx = udiv32((long long)px - gx0, bs);
+    int by = udiv32((long long)py - gy0, bs);
     bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
     by = by < g.nby - 1 ? by : g.nby - 1;
     for (int k = 0; k <= kRingsBins; ++k) {
@@ -241,8 +256,8 @@ struct BinWindow {
 // kRingsBins rings of the pixel's bin (inside the grid) must lie in the window.
 DNNI_HD bool search_bins_window(const BinGrid& g, const BinWindow& w, int px, int py, Best& b) {
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
-    int bx = (int)(((long long)px - gx0) / bs);
-    int by = (int)(((long long)py - gy0) / bs);
+    int bx = udiv32((long long)px - gx0, bs);
+    int by = udiv32((long long)py - gy0, bs);
     bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
     by = by < g.nby - 1 ? by : g.nby - 1;
     for (int k = 0; k <= kRingsBins; ++k) {
@@ -273,8 +288,8 @@ DNNI_HD void scan_local(Best& b, const int4* lpts, int s, int e, int px, int py)
 
 DNNI_HD bool search_window_fast(const BinGrid& g, const BinWindow& w, int px, int py, Best& b) {
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
-    int bx = (int)(((long long)px - gx0) / bs);
-    int by = (int)(((long long)py - gy0) / bs);
+    int bx = udiv32((long long)px - gx0, bs);
+    int by = udiv32((long long)py - gy0, bs);
     bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
     by = by < g.nby - 1 ? by : g.nby - 1;
     const int lx = bx - w.wx0, ly = by - w.wy0;
@@ -325,8 +340,8 @@ DNNI_HD void tile_window(const TileParams& t, int i0, int j0, int& wx0, int& wy0
     const BinGrid& g = t.bg;
     const int i1 = (i0 + kTileX - 1 < t.rw - 1) ? i0 + kTileX - 1 : t.rw - 1;
     const int j1 = (j0 + kTileY - 1 < t.rh - 1) ? j0 + kTileY - 1 : t.rh - 1;
-    long long bxa = ((long long)(t.rx0 + i0) * t.cs - g.gx0) / g.bs, bxb = ((long long)(t.rx0 + i1) * t.cs - g.gx0) / g.bs;
-    long long bya = ((long long)(t.ry0 + j0) * t.cs - g.gy0) / g.bs, byb = ((long long)(t.ry0 + j1) * t.cs - g.gy0) / g.bs;
+    long long bxa = udiv32((long long)(t.rx0 + i0) * t.cs - g.gx0, g.bs), bxb = udiv32((long long)(t.rx0 + i1) * t.cs - g.gx0, g.bs);
+    long long bya = udiv32((long long)(t.ry0 + j0) * t.cs - g.gy0, g.bs), byb = udiv32((long long)(t.ry0 + j1) * t.cs - g.gy0, g.bs);
     bxa = bxa < g.nbx - 1 ? bxa : g.nbx - 1;
     bxb = bxb < g.nbx - 1 ? bxb : g.nbx - 1;
     bya = bya < g.nby - 1 ? bya : g.nby - 1;
@@ -369,7 +384,7 @@ DNNI_HD void seed_from_superblocks(const BinGrid& g, const int4* __restrict__ pt
                                    int px, int py, Best& b) {
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
     const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
-    int cx = (int)(((long long)px - gx0) / u2), cy = (int)(((long long)py - gy0) / u2);
+    int cx = udiv32((long long)px - gx0, u2), cy = udiv32((long long)py - gy0, u2);
     cx = cx < g.n2x - 1 ? cx : g.n2x - 1;
     cy = cy < g.n2y - 1 ? cy : g.n2y - 1;
     const int kmax = (g.n2x > g.n2y ? g.n2x : g.n2y);
@@ -427,7 +442,7 @@ DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const i
     int sy0, sy1;
     cell_range(py, reach_of(b.d2), gy0, u2, g.n2y, sy0, sy1);
     if (sy0 > sy1) return;
-    int csy = (int)(((long long)py - gy0) / u2);
+    int csy = udiv32((long long)py - gy0, u2);
     csy = csy < sy0 ? sy0 : (csy > sy1 ? sy1 : csy);
     const int span = (csy - sy0) > (sy1 - csy) ? (csy - sy0) : (sy1 - csy);
     for (int r = 0; r <= 2 * span; ++r) {
@@ -745,8 +760,7 @@ constexpr size_t kDenseSmem = sizeof(int4) * kWinMaxPts + sizeof(int) * (2 * kWi
 // Records a settled pixel: its record, site, lattice seed and work figures.
 __device__ __forceinline__ void settle_pixel(const TileParams& t, int i, int j, const Best& b, int2* __restrict__ pix,
                                              uint32_t* __restrict__ site, int* __restrict__ seed) {
-    const long long q = b.d2 / ((long long)t.cs * t.cs);
-    const int R2 = (int)(q < t.r2cap ? q : t.r2cap);
+    const int R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
     const int64_t o = (int64_t)j * t.rw + i;
     pix[o] = make_int2(b.z, R2);
     if (site) site[o] = b.gid;
@@ -853,8 +867,7 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
             }
             if (done) {
                 settle_pixel(t, i, j, b, pix, site, seed);
-                const long long q = b.d2 / ((long long)t.cs * t.cs);
-                R2 = (int)(q < t.r2cap ? q : t.r2cap);
+                R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
             } else {
                 far_pixel = true;
             }
@@ -886,7 +899,7 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
 // Far pass over one worklist (front: lattice pixels, unseeded, writing their
 // seeds; back: the rest, seeded by the lattice).  Grid-stride over the items,
 // a warp takes 32 consecutive ones (neighbouring pixels of one tile row).
-__global__ void __launch_bounds__(256) k_near_far(TileParams t, const int4* __restrict__ pts,
+__global__ void __launch_bounds__(256, 2) k_near_far(TileParams t, const int4* __restrict__ pts,
                                                   const int* __restrict__ start, const uint64_t* __restrict__ bmask,
                                                   const uint64_t* __restrict__ smask, int* __restrict__ seed,
                                                   int seeded, const int2* __restrict__ far, int which,
@@ -907,8 +920,7 @@ __global__ void __launch_bounds__(256) k_near_far(TileParams t, const int4* __re
             if (item.y >= 0) consider(b, __ldg(&pts[item.y]), item.y, px, py);
             finish_search(t.bg, pts, start, bmask, smask, px, py, b, seeded ? &sg : nullptr, i, j);
             settle_pixel(t, i, j, b, pix, site, seeded ? nullptr : seed);
-            const long long q = b.d2 / ((long long)t.cs * t.cs);
-            R2 = (int)(q < t.r2cap ? q : t.r2cap);
+            R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
         }
         warp_stats(t, R2, sc, blockIdx.x * 3 + (threadIdx.x >> 5));
     }

@@ -71,8 +71,7 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
     const SeedGrid seedg{seeds.data(), snx, sny};
     std::vector<int2> farA, farB;   // (pixel, best so far)
     auto settle = [&](int i, int j, const Best& b) {
-        const long long q = b.d2 / ((long long)t.cs * t.cs);
-        const int R2 = (int)(q < t.r2cap ? q : t.r2cap);
+        const int R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
         pix[(int64_t)j * t.rw + i] = make_int2(b.z, R2);
         if (site) site[(int64_t)j * t.rw + i] = b.gid;
         if (r2_out) r2_out[(int64_t)j * t.rw + i] = R2;
@@ -217,3 +216,6 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
     }
     return 0;
 }
+
+// exposes the device helpers r2_of and udiv32 for direct tests
+extern "C" int emu_r2_of(long long d2, long long cs2, int cap) { return r2_of(d2, cs2, cap); }

@@ -108,3 +108,20 @@ def test_host_build_window_fallbacks(emu, oracle, k):
     ref = oracle.interpolate(wp, xyz)
     rc, r = emu(wp, xyz, bin_target=bt)
     assert rc == 0 and np.array_equal(r["site"], ref["site"]) and _same(r["h"], ref["h"])
+
+
+def test_r2_of_is_exact_floor_division():
+    import ctypes, os
+    L = ctypes.CDLL(os.path.join(os.path.dirname(__file__), "native", "libdnni_emu.so"))
+    L.emu_r2_of.argtypes = [ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int]
+    L.emu_r2_of.restype = ctypes.c_int
+    rng = np.random.default_rng(5)
+    cap = 2 * 32767 * 32767
+    for cs in (1, 7, 50, 100, 2000, 32767):
+        cs2 = cs * cs
+        for _ in range(2000):
+            q = int(rng.integers(0, cap + 5))
+            for d2 in (q * cs2 - 1, q * cs2, q * cs2 + cs2 - 1, int(rng.integers(0, 2 ** 62))):
+                if d2 < 0:
+                    continue
+                assert L.emu_r2_of(d2, cs2, cap) == min(d2 // cs2, cap)
