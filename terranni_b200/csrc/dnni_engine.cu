@@ -107,11 +107,10 @@ void dnni_bin_grid(const dnni_ctx* c, const int32_t bbox[6], int64_t n, TilePara
     plan_bins(bbox, n, (double)c->s.bin_target, t);
 }
 
-// Nearest-site passes: dense tiles, then the far worklist's lattice pixels
-// (unseeded), then its other pixels (seeded by the lattice).
+// Nearest-site passes: dense tiles, then the far worklist.
 static void launch_nearest(const TileParams& t, const int4* sorted, const int* start, const uint64_t* bmask,
-                           const uint64_t* smask, int* seeds, int2* pix, uint32_t* site, int2* far, Scalars* sc,
-                           int sms, cudaStream_t st) {
+                           const uint64_t* smask, int2* pix, uint32_t* site, int2* far, Scalars* sc, int sms,
+                           cudaStream_t st) {
     static thread_local int attr_dev = -1;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -120,11 +119,8 @@ static void launch_nearest(const TileParams& t, const int4* sorted, const int* s
         attr_dev = dev;
     }
     dim3 blk(32, 8), grd((t.rw + kTileX - 1) / kTileX, (t.rh + kTileY - 1) / kTileY);
-    k_near_dense<<<grd, blk, kDenseSmem, st>>>(t, sorted, start, seeds, pix, site, far, sc);
-    if (t.npts > 0) {
-        k_near_far<<<sms * 4, 256, 0, st>>>(t, sorted, start, bmask, smask, seeds, 0, far, 0, pix, site, sc);
-        k_near_far<<<sms * 4, 256, 0, st>>>(t, sorted, start, bmask, smask, seeds, 1, far, 1, pix, site, sc);
-    }
+    k_near_dense<<<grd, blk, kDenseSmem, st>>>(t, sorted, start, pix, site, far, sc);
+    if (t.npts > 0) k_near_far<<<sms * 6, 256, 0, st>>>(t, sorted, start, bmask, smask, far, pix, site, sc);
 }
 
 static void launch_final(const TileParams& t, const int2* pix, Scalars* sc, const unsigned long long* S,
@@ -199,12 +195,9 @@ dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32
     }
     if (timing) CK(cudaEventRecord(c->ev[1], st));
     {
-        const int ns = std::max(1, seed_dim(t.rw) * seed_dim(t.rh));
-        if ((rs = dnni_ensure(c, c->seeds, sizeof(int) * ns))) return rs;
         if ((rs = dnni_ensure(c, c->far, sizeof(int2) * npix))) return rs;
         launch_nearest(t, (const int4*)c->sorted.p, (const int*)c->start.p, (const uint64_t*)c->bmask.p,
-                       (const uint64_t*)c->smask.p, (int*)c->seeds.p, (int2*)c->pix.p, d_site, (int2*)c->far.p, sc,
-                       c->sm_count, st);
+                       (const uint64_t*)c->smask.p, (int2*)c->pix.p, d_site, (int2*)c->far.p, sc, c->sm_count, st);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         CK(cudaGetLastError());
     }
@@ -431,7 +424,7 @@ dnni_status dnni_host_free(void* p) {
 }  // extern "C"
 
 void dnni_free_all(dnni_ctx* c) {
-    DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc, &c->seeds,
+    DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc,
                       &c->bmask, &c->smask, &c->far,
                       &c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
     for (DevBuf* b : bufs) dnni_release(*b, c);
@@ -518,7 +511,6 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     const size_t o_Dc = a.take(sizeof(int) * cells);
     const size_t o_rank = n > 0 ? a.take(sizeof(int) * n) : 0;
     const size_t o_sorted = n > 0 ? a.take(sizeof(int4) * n) : 0;
-    const size_t o_seed = a.take(sizeof(int) * std::max(1, seed_dim(t.rw) * seed_dim(t.rh)));
     const size_t o_far = a.take(sizeof(int2) * npix);
     if (!a.fits()) return DNNI_E_SCRATCH;
     int sms = 148;
@@ -571,8 +563,7 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     }
     {
         dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        launch_nearest(t, sorted, start, bmask, smask, (int*)(base + o_seed), pix, d_site, (int2*)(base + o_far), sc,
-                       sms, st);
+        launch_nearest(t, sorted, start, bmask, smask, pix, d_site, (int2*)(base + o_far), sc, sms, st);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         if (cudaMemsetAsync(D, 0, sizeof(unsigned long long) * cells, st) != cudaSuccess ||
             cudaMemsetAsync(Dc, 0, sizeof(int) * cells, st) != cudaSuccess)

@@ -81,7 +81,8 @@ struct Scalars {
     int32_t err;
     int32_t packed;              // decided after the nearest-site pass
     int32_t kbits;
-    int32_t nfar[2];             // far worklist lengths (lattice pixels, others)
+    int32_t nfar;                // far worklist length
+    int32_t pad2;
     int32_t pad;
     long long zbase;
     int32_t max_r2[kStatSlots];
@@ -323,6 +324,81 @@ DNNI_HD bool search_window_fast(const BinGrid& g, const BinWindow& w, int px, in
     return ring_done(b.d2, px, py, gx0, gy0, bs, bx - 2, bx + 2, by - 2, by + 2, g.nbx, g.nby);
 }
 
+// The same search with 32-bit distances, for windows that span less than
+// 2^15 LAS units in each direction (squared distances then fit in 31 bits).
+// The (d^2, gid) part of the (d^2, gid, z) order is one 64-bit key.
+struct Best32 {
+    unsigned long long key;   // d2 << 32 | gid; ~0 = none
+    int z;
+    int idx;
+};
+
+DNNI_HD void consider32(Best32& b, const int4 p, int q, int px, int py) {
+    const int dx = p.x - px, dy = p.y - py;
+    const unsigned d2 = (unsigned)(dx * dx) + (unsigned)(dy * dy);
+    const unsigned long long key = ((unsigned long long)d2 << 32) | (unsigned)p.w;
+    if (key < b.key || (key == b.key && p.z < b.z)) {
+        b.key = key;
+        b.z = p.z;
+        b.idx = q;
+    }
+}
+
+DNNI_HD long long best32_d2(const Best32& b) { return b.key == ~0ull ? LLONG_MAX : (long long)(b.key >> 32); }
+
+DNNI_HD void scan_local32(Best32& b, const int4* lpts, int s, int e, int px, int py) {
+    for (int q = s; q < e; ++q) consider32(b, lpts[q], q, px, py);
+}
+
+DNNI_HD bool window_fits32(const BinGrid& g, const BinWindow& w) {
+    return (long long)(w.wnx + 1) * g.bs < 32768 && (long long)(w.wny + 1) * g.bs < 32768;
+}
+
+DNNI_HD bool search_window_fast32(const BinGrid& g, const BinWindow& w, int px, int py, Best& out) {
+    const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    int bx = udiv32((long long)px - gx0, bs);
+    int by = udiv32((long long)py - gy0, bs);
+    bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
+    by = by < g.nby - 1 ? by : g.nby - 1;
+    const int lx = bx - w.wx0, ly = by - w.wy0;
+    Best32 b{~0ull, INT_MAX, -1};
+    bool done;
+    {
+        const int x0 = lx - 1 > 0 ? lx - 1 : 0, x1 = lx + 1 < w.wnx - 1 ? lx + 1 : w.wnx - 1;
+        const int y0 = ly - 1 > 0 ? ly - 1 : 0, y1 = ly + 1 < w.wny - 1 ? ly + 1 : w.wny - 1;
+        for (int r = y0; r <= y1; ++r)
+            scan_local32(b, w.lpts, w.lstart[r * w.wnx + x0], w.lstart[r * w.wnx + x1 + 1], px, py);
+    }
+    done = ring_done(best32_d2(b), px, py, gx0, gy0, bs, bx - 1, bx + 1, by - 1, by + 1, g.nbx, g.nby);
+    if (!done) {
+        const int x0 = lx - 2 > 0 ? lx - 2 : 0, x1 = lx + 2 < w.wnx - 1 ? lx + 2 : w.wnx - 1;
+        const long long X0 = gx0 + (long long)(w.wx0 + x0) * bs, X1 = gx0 + (long long)(w.wx0 + x1 + 1) * bs - 1;
+        for (int d = -2; d <= 2; d += 4) {
+            const int r = ly + d;
+            if (r < 0 || r >= w.wny) continue;
+            const long long Y0 = gy0 + (long long)(w.wy0 + r) * bs;
+            if (box_lb(px, py, X0, X1, Y0, Y0 + bs - 1) > best32_d2(b)) continue;
+            scan_local32(b, w.lpts, w.lstart[r * w.wnx + x0], w.lstart[r * w.wnx + x1 + 1], px, py);
+        }
+        const int ya = ly - 1 > 0 ? ly - 1 : 0, yb = ly + 1 < w.wny - 1 ? ly + 1 : w.wny - 1;
+        const long long Y0 = gy0 + (long long)(w.wy0 + ya) * bs, Y1 = gy0 + (long long)(w.wy0 + yb + 1) * bs - 1;
+        for (int d = -2; d <= 2; d += 4) {
+            const int c = lx + d;
+            if (c < 0 || c >= w.wnx) continue;
+            const long long CX0 = gx0 + (long long)(w.wx0 + c) * bs;
+            if (box_lb(px, py, CX0, CX0 + bs - 1, Y0, Y1) > best32_d2(b)) continue;
+            for (int r = ya; r <= yb; ++r)
+                scan_local32(b, w.lpts, w.lstart[r * w.wnx + c], w.lstart[r * w.wnx + c + 1], px, py);
+        }
+        done = ring_done(best32_d2(b), px, py, gx0, gy0, bs, bx - 2, bx + 2, by - 2, by + 2, g.nbx, g.nby);
+    }
+    out.d2 = best32_d2(b);
+    out.gid = b.key == ~0ull ? 0xFFFFFFFFu : (uint32_t)(b.key & 0xFFFFFFFFull);
+    out.z = b.z;
+    out.idx = b.idx;
+    return done;
+}
+
 // Sorted-array position of window-local point q (-1 stays -1).
 DNNI_HD int window_global_index(const BinWindow& w, int q) {
     if (q < 0) return -1;
@@ -362,16 +438,6 @@ DNNI_HD int ffs64(uint64_t v) {
     return __ffsll((long long)v) - 1;
 #else
     return __builtin_ctzll(v);
-#endif
-}
-
-DNNI_HD unsigned bits_between(int lo, int hi) { return (0xFFu << lo) & (0xFFu >> (7 - hi)) & 0xFFu; }
-
-DNNI_HD int clz32(unsigned v) {
-#ifdef __CUDA_ARCH__
-    return __clz((int)v);
-#else
-    return __builtin_clz(v);
 #endif
 }
 
@@ -460,39 +526,39 @@ DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const i
             if (!sm) continue;
             const long long SX0 = gx0 + (long long)sx * u2;
             if (box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) > b.d2) continue;
-            // non-empty blocks of this superblock inside the disc
+            // non-empty blocks of this superblock within the bound
             for (int ly = 0; ly < kBinsPerBlockEdge; ++ly) {
                 unsigned row = (unsigned)(sm >> (ly * 8)) & 0xFFu;
                 if (!row) continue;
                 const long long BY0 = SY0 + (long long)ly * u1;
                 const long long gyb = axis_gap(py, BY0, BY0 + u1 - 1);
-                if (gyb * gyb > b.d2) continue;
-                int bx0, bx1;
-                cell_range(px - SX0, reach_of(b.d2 - gyb * gyb), 0, u1, kBinsPerBlockEdge, bx0, bx1);
-                if (bx0 > bx1) continue;
-                row &= bits_between(bx0, bx1);
+                const long long gyb2 = gyb * gyb;
+                if (gyb2 > b.d2) continue;
                 while (row) {
                     const int lx = ffs64(row);
                     row &= row - 1;
+                    const long long BX0 = SX0 + (long long)lx * u1;
+                    const long long gxb = axis_gap(px, BX0, BX0 + u1 - 1);
+                    if (gxb * gxb + gyb2 > b.d2) continue;
                     const int64_t blk = ((int64_t)sidx << 6) + ly * 8 + lx;
                     const uint64_t bm = DNNI_LDG(&bmask[blk]);
-                    const long long BX0 = SX0 + (long long)lx * u1;
-                    // non-empty bins of this block inside the disc, one
-                    // contiguous point range per bin row
+                    // non-empty bins of this block within the bound
                     for (int qy = 0; qy < kBinsPerBlockEdge; ++qy) {
                         unsigned qrow = (unsigned)(bm >> (qy * 8)) & 0xFFu;
                         if (!qrow) continue;
                         const long long QY0 = BY0 + (long long)qy * bs;
                         const long long gq = axis_gap(py, QY0, QY0 + bs - 1);
-                        if (gq * gq > b.d2) continue;
-                        int qx0, qx1;
-                        cell_range(px - BX0, reach_of(b.d2 - gq * gq), 0, bs, kBinsPerBlockEdge, qx0, qx1);
-                        if (qx0 > qx1) continue;
-                        qrow &= bits_between(qx0, qx1);
-                        if (!qrow) continue;
-                        const int f = ffs64(qrow), l = 31 - clz32(qrow);
+                        const long long gq2 = gq * gq;
+                        if (gq2 > b.d2) continue;
                         const int64_t id0 = (blk << 6) + qy * 8;
-                        scan_points(b, pts, DNNI_LDG(&start[id0 + f]), DNNI_LDG(&start[id0 + l + 1]), px, py);
+                        while (qrow) {
+                            const int qx = ffs64(qrow);
+                            qrow &= qrow - 1;
+                            const long long QX0 = BX0 + (long long)qx * bs;
+                            const long long gx = axis_gap(px, QX0, QX0 + bs - 1);
+                            if (gx * gx + gq2 > b.d2) continue;
+                            scan_points(b, pts, DNNI_LDG(&start[id0 + qx]), DNNI_LDG(&start[id0 + qx + 1]), px, py);
+                        }
                     }
                 }
             }
@@ -500,56 +566,23 @@ DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const i
     }
 }
 
-// Seed lattice: raster pixels (i,j) with i % kSeedStride == j % kSeedStride
-// == kSeedStride/2.  Their sites are found first (without seeds); they bound
-// the nearest-site distance of the pixels around them.
-constexpr int kSeedStride = 16;
-
-struct SeedGrid {
-    const int* idx;     // sorted-array position of each lattice pixel's site
-    int nx, ny;
-};
-
-DNNI_HD int seed_dim(int n) { return (n + kSeedStride / 2 - 1) / kSeedStride; }
-DNNI_HD bool is_seed_pixel(int i, int j) {
-    return (i % kSeedStride) == kSeedStride / 2 && (j % kSeedStride) == kSeedStride / 2;
-}
-
-// The sites of the (up to) four lattice pixels around raster pixel (i,j).
-DNNI_HD void consider_seeds(const SeedGrid& sg, const int4* __restrict__ pts, int i, int j, int px, int py,
-                            Best& b) {
-    if (sg.nx <= 0 || sg.ny <= 0) return;
-    int a = i < kSeedStride / 2 ? 0 : (i - kSeedStride / 2) / kSeedStride;
-    int c = j < kSeedStride / 2 ? 0 : (j - kSeedStride / 2) / kSeedStride;
-    a = a > sg.nx - 1 ? sg.nx - 1 : a;
-    c = c > sg.ny - 1 ? sg.ny - 1 : c;
-    const int a1 = a + 1 < sg.nx ? a + 1 : a, c1 = c + 1 < sg.ny ? c + 1 : c;
-    const int cand[4] = {c * sg.nx + a, c * sg.nx + a1, c1 * sg.nx + a, c1 * sg.nx + a1};
-    for (int k = 0; k < 4; ++k) {
-        const int q = DNNI_LDG(&sg.idx[cand[k]]);
-        if (q >= 0) consider(b, DNNI_LDG(&pts[q]), q, px, py);
-    }
-}
-
 // Completes the search of a pixel that the bin rings did not settle: the
-// bound so far (b), the lattice sites around it (when sg is given) or else
-// the nearest non-empty superblock give a real site, and the disc of that
-// bound is searched exhaustively.
+// bound so far (b) or else the nearest non-empty superblock gives a real
+// site, and the disc of that bound is searched exhaustively.
 DNNI_HD void finish_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                            const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
-                           int px, int py, Best& b, const SeedGrid* sg, int i, int j) {
-    if (sg) consider_seeds(*sg, pts, i, j, px, py, b);
+                           int px, int py, Best& b) {
     if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, bmask, smask, px, py, b);
     search_disc(g, pts, start, bmask, smask, px, py, b);
 }
 
-// Exact nearest site of raster pixel (i,j) at (px,py) (LAS units relative to
-// the WP origin), all levels in one call.
+// Exact nearest site of the pixel at (px,py) (LAS units relative to the WP
+// origin), all levels in one call.
 DNNI_HD void nearest_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                             const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
-                            int px, int py, Best& b, const SeedGrid* sg = nullptr, int i = 0, int j = 0) {
+                            int px, int py, Best& b) {
     if (search_bins(g, pts, start, px, py, b)) return;
-    finish_search(g, pts, start, bmask, smask, px, py, b, sg, i, j);
+    finish_search(g, pts, start, bmask, smask, px, py, b);
 }
 
 // ---------------------------------------------------------------------------
@@ -563,7 +596,7 @@ __global__ void k_init_scalars(Scalars* sc) {
         sc->bbox[2] = INT_MAX; sc->bbox[3] = INT_MIN;
         sc->bbox[4] = INT_MAX; sc->bbox[5] = INT_MIN;
         sc->err = 0; sc->packed = 0; sc->kbits = 0; sc->zbase = 0;
-        sc->nfar[0] = 0; sc->nfar[1] = 0;
+        sc->nfar = 0;
     }
     if (l < kStatSlots) {
         sc->max_r2[l] = -1; sc->big_pixels[l] = 0; sc->spans[l] = 0; sc->nodata[l] = 0;
@@ -757,14 +790,13 @@ constexpr int kWinMaxBins = 2048;
 constexpr int kWinMaxPts = 3072;
 constexpr size_t kDenseSmem = sizeof(int4) * kWinMaxPts + sizeof(int) * (2 * kWinMaxBins + 1);
 
-// Records a settled pixel: its record, site, lattice seed and work figures.
+// Records a settled pixel: its record and site.
 __device__ __forceinline__ void settle_pixel(const TileParams& t, int i, int j, const Best& b, int2* __restrict__ pix,
-                                             uint32_t* __restrict__ site, int* __restrict__ seed) {
+                                             uint32_t* __restrict__ site) {
     const int R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
     const int64_t o = (int64_t)j * t.rw + i;
     pix[o] = make_int2(b.z, R2);
     if (site) site[o] = b.gid;
-    if (seed && is_seed_pixel(i, j)) seed[(j / kSeedStride) * seed_dim(t.rw) + i / kSeedStride] = b.idx;
 }
 
 __device__ __forceinline__ void warp_stats(const TileParams& t, int R2, Scalars* __restrict__ sc, int slot) {
@@ -788,13 +820,12 @@ __device__ __forceinline__ void warp_stats(const TileParams& t, int R2, Scalars*
 // pixel row of the tile): the tile's bin window (bin rings of every pixel)
 // is staged in shared memory and the rings are searched there; windows too
 // large for shared memory use the global arrays.  Pixels the rings do not
-// settle go to the far worklist: lattice pixels from the front (count
-// sc->nfar[0]), the others from the back (count sc->nfar[1]), each with its
-// best site so far.  With no points every pixel is settled as "no site".
+// settle go to the far worklist (count sc->nfar), each with its best site so
+// far.  With no points every pixel is settled as "no site".
 __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __restrict__ pts,
-                                                    const int* __restrict__ start, int* __restrict__ seed,
-                                                    int2* __restrict__ pix, uint32_t* __restrict__ site,
-                                                    int2* __restrict__ far, Scalars* __restrict__ sc) {
+                                                    const int* __restrict__ start, int2* __restrict__ pix,
+                                                    uint32_t* __restrict__ site, int2* __restrict__ far,
+                                                    Scalars* __restrict__ sc) {
     extern __shared__ int4 smem[];
     int4* s_pts = smem;
     int* s_lstart = (int*)(smem + kWinMaxPts);
@@ -838,14 +869,19 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
             __syncthreads();
             staged = s_total <= kWinMaxPts;
             if (staged) {
-                // copy the window's points, one point per thread per pass
-                for (int q = tid; q < s_total; q += 256) {
-                    int lo = 0, hi = nwb - 1;           // last bin with lstart <= q
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (s_lstart[mid] <= q) lo = mid; else hi = mid - 1;
-                    }
-                    s_pts[q] = __ldg(&pts[s_gstart[lo] + (q - s_lstart[lo])]);
+                // copy the window's points run by run: the bins of one window
+                // row inside one block are consecutive in both layouts; one
+                // warp per run, lanes striding over its points
+                const int cb0 = wx0 >> 3, cb1 = (wx0 + wnx - 1) >> 3;
+                const int nseg = cb1 - cb0 + 1, nrun = nseg * wny;
+                const int warp = tid >> 5, lane = tid & 31;
+                for (int run = warp; run < nrun; run += 8) {
+                    const int r = run / nseg, sg = run - r * nseg;
+                    const int xa = (cb0 + sg) * 8 > wx0 ? (cb0 + sg) * 8 : wx0;
+                    const int xb = (cb0 + sg) * 8 + 7 < wx0 + wnx - 1 ? (cb0 + sg) * 8 + 7 : wx0 + wnx - 1;
+                    const int lk0 = r * wnx + (xa - wx0), lk1 = r * wnx + (xb - wx0);
+                    const int l0 = s_lstart[lk0], cntp = s_lstart[lk1 + 1] - l0, g0 = s_gstart[lk0];
+                    for (int q = lane; q < cntp; q += 32) s_pts[l0 + q] = __ldg(&pts[g0 + q]);
                 }
             }
             __syncthreads();
@@ -860,13 +896,13 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
             bool done;
             if (staged) {
                 const BinWindow w{wx0, wy0, wnx, wny, s_lstart, s_gstart, s_pts};
-                done = search_window_fast(g, w, px, py, b);
+                done = window_fits32(g, w) ? search_window_fast32(g, w, px, py, b) : search_window_fast(g, w, px, py, b);
                 b.idx = window_global_index(w, b.idx);
             } else {
                 done = search_bins(g, pts, start, px, py, b);
             }
             if (done) {
-                settle_pixel(t, i, j, b, pix, site, seed);
+                settle_pixel(t, i, j, b, pix, site);
                 R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
             } else {
                 far_pixel = true;
@@ -878,48 +914,35 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
         }
     }
     // worklist append, warp-aggregated
-    const bool lat = far_pixel && is_seed_pixel(i, j);
-    const bool oth = far_pixel && !lat;
-    const unsigned mlat = __ballot_sync(0xffffffffu, lat), moth = __ballot_sync(0xffffffffu, oth);
+    const unsigned mfar = __ballot_sync(0xffffffffu, far_pixel);
     const int lane = threadIdx.x;
-    int base_lat = 0, base_oth = 0;
-    if (lane == 0) {
-        if (mlat) base_lat = atomicAdd(&sc->nfar[0], __popc(mlat));
-        if (moth) base_oth = atomicAdd(&sc->nfar[1], __popc(moth));
-    }
-    base_lat = __shfl_sync(0xffffffffu, base_lat, 0);
-    base_oth = __shfl_sync(0xffffffffu, base_oth, 0);
-    const unsigned below = (1u << lane) - 1u;
-    const int2 item = make_int2(j * t.rw + i, b.idx);
-    if (lat) far[base_lat + __popc(mlat & below)] = item;
-    if (oth) far[(int64_t)t.rw * t.rh - 1 - (base_oth + __popc(moth & below))] = item;
+    int base = 0;
+    if (lane == 0 && mfar) base = atomicAdd(&sc->nfar, __popc(mfar));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (far_pixel) far[base + __popc(mfar & ((1u << lane) - 1u))] = make_int2(j * t.rw + i, b.idx);
     warp_stats(t, R2, sc, blockIdx.x + blockIdx.y * 7 + threadIdx.y);
 }
 
-// Far pass over one worklist (front: lattice pixels, unseeded, writing their
-// seeds; back: the rest, seeded by the lattice).  Grid-stride over the items,
-// a warp takes 32 consecutive ones (neighbouring pixels of one tile row).
-__global__ void __launch_bounds__(256, 2) k_near_far(TileParams t, const int4* __restrict__ pts,
-                                                  const int* __restrict__ start, const uint64_t* __restrict__ bmask,
-                                                  const uint64_t* __restrict__ smask, int* __restrict__ seed,
-                                                  int seeded, const int2* __restrict__ far, int which,
-                                                  int2* __restrict__ pix, uint32_t* __restrict__ site,
-                                                  Scalars* __restrict__ sc) {
-    const int count = sc->nfar[which];
-    const int64_t npix = (int64_t)t.rw * t.rh;
+// Far pass over the worklist: grid-stride over the items, a warp takes 32
+// consecutive ones (neighbouring pixels of one tile row).
+__global__ void __launch_bounds__(256, 3) k_near_far(TileParams t, const int4* __restrict__ pts,
+                                                     const int* __restrict__ start, const uint64_t* __restrict__ bmask,
+                                                     const uint64_t* __restrict__ smask, const int2* __restrict__ far,
+                                                     int2* __restrict__ pix, uint32_t* __restrict__ site,
+                                                     Scalars* __restrict__ sc) {
+    const int count = sc->nfar;
     const int lane = threadIdx.x & 31;
-    const SeedGrid sg{seed, seed_dim(t.rw), seed_dim(t.rh)};
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += gridDim.x * blockDim.x) {
         const int it = base + lane;
         int R2 = -1;
         if (it < count) {
-            const int2 item = which ? far[npix - 1 - it] : far[it];
+            const int2 item = far[it];
             const int i = item.x % t.rw, j = item.x / t.rw;
             const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
             Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
             if (item.y >= 0) consider(b, __ldg(&pts[item.y]), item.y, px, py);
-            finish_search(t.bg, pts, start, bmask, smask, px, py, b, seeded ? &sg : nullptr, i, j);
-            settle_pixel(t, i, j, b, pix, site, seeded ? nullptr : seed);
+            finish_search(t.bg, pts, start, bmask, smask, px, py, b);
+            settle_pixel(t, i, j, b, pix, site);
             R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
         }
         warp_stats(t, R2, sc, blockIdx.x * 3 + (threadIdx.x >> 5));

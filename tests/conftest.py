@@ -54,10 +54,10 @@ def emu():
     L = ctypes.CDLL(EMU_SO)
     L.emu_interpolate.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                  ctypes.c_void_p, ctypes.c_int]
+                                  ctypes.c_void_p]
     L.emu_interpolate.restype = ctypes.c_int
 
-    def run(wp, xyz, gid=None, small_radius=0, bin_target=0, seeded=True):
+    def run(wp, xyz, gid=None, small_radius=0, bin_target=0):
         from oracle.oracle import raster_box
         xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
         if gid is not None:
@@ -69,7 +69,7 @@ def emu():
         info = np.zeros(8, np.int64)
         p = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
         rc = L.emu_interpolate(ctypes.addressof(wp), p(xyz), p(gid), xyz.shape[0], small_radius, bin_target,
-                               p(h), p(site), p(r2), p(info), 1 if seeded else 0)
+                               p(h), p(site), p(r2), p(info))
         return rc, {"h": h, "site": site, "r2": r2,
                     "info": dict(zip(["packed", "K", "zbase", "bin_size", "big_pixels", "spans", "nodata",
                                       "max_r2"], info.tolist()))}

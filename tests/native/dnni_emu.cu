@@ -24,7 +24,7 @@ static float host_height(long long Z, long long C, double zs, double zo, float n
 
 extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, const uint32_t* gid, int64_t n,
                                int small_radius, int bin_target, float* h, uint32_t* site, int32_t* r2_out,
-                               int64_t* info, int seeded) {
+                               int64_t* info) {
     TileParams t;
     const char* msg;
     int rs = small_radius ? small_radius : 3;
@@ -66,17 +66,13 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
     const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
     std::vector<int2> pix(npix);
     int max_r2 = -1;
-    const int snx = seed_dim(t.rw), sny = seed_dim(t.rh);
-    std::vector<int> seeds(std::max(1, snx * sny), -1);
-    const SeedGrid seedg{seeds.data(), snx, sny};
-    std::vector<int2> farA, farB;   // (pixel, best so far)
+    std::vector<int2> farl;   // (pixel, best so far)
     auto settle = [&](int i, int j, const Best& b) {
         const int R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
         pix[(int64_t)j * t.rw + i] = make_int2(b.z, R2);
         if (site) site[(int64_t)j * t.rw + i] = b.gid;
         if (r2_out) r2_out[(int64_t)j * t.rw + i] = R2;
         max_r2 = std::max(max_r2, R2);
-        if (is_seed_pixel(i, j)) seeds[(j / kSeedStride) * snx + i / kSeedStride] = b.idx;
     };
     // dense pass: per 32 x 8 tile, staged window (as the device kernel) or the global arrays
     std::vector<int> lstart(kWinMaxBins + 1), gstart(kWinMaxBins);
@@ -116,26 +112,25 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
                     bool done;
                     if (staged) {
                         const BinWindow w{wx0, wy0, wnx, wny, lstart.data(), gstart.data(), lpts.data()};
-                        done = search_window_fast(g, w, px, py, b);
+                        done = window_fits32(g, w) ? search_window_fast32(g, w, px, py, b)
+                                                   : search_window_fast(g, w, px, py, b);
                         b.idx = window_global_index(w, b.idx);
                     } else {
                         done = search_bins(g, sorted.data(), start.data(), px, py, b);
                     }
                     if (done) settle(i, j, b);
-                    else (is_seed_pixel(i, j) ? farA : farB).push_back(make_int2(j * t.rw + i, b.idx));
+                    else farl.push_back(make_int2(j * t.rw + i, b.idx));
                 }
         }
-    // far passes: lattice pixels unseeded, then the rest seeded
-    for (int pass = 0; pass < 2; ++pass)
-        for (const int2& it : (pass ? farB : farA)) {
-            const int i = it.x % t.rw, j = it.x / t.rw;
-            const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
-            Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
-            if (it.y >= 0) consider(b, sorted[it.y], it.y, px, py);
-            finish_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), px, py, b,
-                          (pass && seeded) ? &seedg : nullptr, i, j);
-            settle(i, j, b);
-        }
+    // far pass
+    for (const int2& it : farl) {
+        const int i = it.x % t.rw, j = it.x / t.rw;
+        const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
+        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+        if (it.y >= 0) consider(b, sorted[it.y], it.y, px, py);
+        finish_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), px, py, b);
+        settle(i, j, b);
+    }
     int packed, K;
     long long zbase;
     decide_packing(max_r2, npix, bbox[4], bbox[5], packed, K, zbase);

@@ -37,11 +37,10 @@ def test_host_build_matches_oracle(emu, oracle, seed, side, n, lakes, rs, bt):
     xyz = terrain_case(seed, side, n, lakes=lakes, lake_r=(8.0, 30.0))
     wp = oracle.make_wp(side, side, 100)
     ref = oracle.interpolate(wp, xyz)
-    for seeded in (True, False):    # lattice-seeded search (k_nearest) and unseeded (no-alloc path)
-        rc, r = emu(wp, xyz, small_radius=rs, bin_target=bt, seeded=seeded)
-        assert rc == 0
-        assert np.array_equal(r["site"], ref["site"])
-        assert _same(r["h"], ref["h"])
+    rc, r = emu(wp, xyz, small_radius=rs, bin_target=bt)
+    assert rc == 0
+    assert np.array_equal(r["site"], ref["site"])
+    assert _same(r["h"], ref["h"])
 
 
 def test_host_build_raster_halo_and_origin(emu, oracle):
