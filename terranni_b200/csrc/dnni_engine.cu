@@ -109,8 +109,8 @@ void dnni_bin_grid(const dnni_ctx* c, const int32_t bbox[6], int64_t n, TilePara
 
 // Nearest-site passes: dense tiles, then the far worklist.
 static void launch_nearest(const TileParams& t, const int4* sorted, const int* start, const uint64_t* bmask,
-                           const uint64_t* smask, int2* pix, uint32_t* site, int2* far, Scalars* sc, int sms,
-                           cudaStream_t st) {
+                           const uint64_t* smask, int* rownear, int64_t* near, int2* pix, uint32_t* site, int2* far,
+                           Scalars* sc, int sms, cudaStream_t st) {
     static thread_local int attr_dev = -1;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -120,7 +120,12 @@ static void launch_nearest(const TileParams& t, const int4* sorted, const int* s
     }
     dim3 blk(32, 8), grd((t.rw + kTileX - 1) / kTileX, (t.rh + kTileY - 1) / kTileY);
     k_near_dense<<<grd, blk, kDenseSmem, st>>>(t, sorted, start, pix, site, far, sc);
-    if (t.npts > 0) k_near_far<<<sms * 6, 256, 0, st>>>(t, sorted, start, bmask, smask, far, pix, site, sc);
+    if (t.npts > 0) {
+        const int n1x = t.bg.nbx >> 3, n1y = t.bg.nby >> 3;
+        k_block_rows<<<(n1y + 127) / 128, 128, 0, st>>>(t.bg, bmask, rownear);
+        k_block_near<<<(int)(((int64_t)n1x * n1y + 255) / 256), 256, 0, st>>>(t.bg, rownear, near);
+        k_near_far<<<sms * 6, 256, 0, st>>>(t, sorted, start, bmask, smask, near, far, pix, site, sc);
+    }
 }
 
 static void launch_final(const TileParams& t, const int2* pix, Scalars* sc, const unsigned long long* S,
@@ -196,8 +201,12 @@ dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32
     if (timing) CK(cudaEventRecord(c->ev[1], st));
     {
         if ((rs = dnni_ensure(c, c->far, sizeof(int2) * npix))) return rs;
+        const int64_t nblk = n > 0 ? t.bg.nbins / kBinsPerBlock : 1;
+        if ((rs = dnni_ensure(c, c->rownear, sizeof(int) * nblk))) return rs;
+        if ((rs = dnni_ensure(c, c->near, sizeof(int64_t) * nblk))) return rs;
         launch_nearest(t, (const int4*)c->sorted.p, (const int*)c->start.p, (const uint64_t*)c->bmask.p,
-                       (const uint64_t*)c->smask.p, (int2*)c->pix.p, d_site, (int2*)c->far.p, sc, c->sm_count, st);
+                       (const uint64_t*)c->smask.p, (int*)c->rownear.p, (int64_t*)c->near.p, (int2*)c->pix.p, d_site,
+                       (int2*)c->far.p, sc, c->sm_count, st);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         CK(cudaGetLastError());
     }
@@ -425,7 +434,7 @@ dnni_status dnni_host_free(void* p) {
 
 void dnni_free_all(dnni_ctx* c) {
     DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc,
-                      &c->bmask, &c->smask, &c->far,
+                      &c->bmask, &c->smask, &c->far, &c->rownear, &c->near,
                       &c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
@@ -540,6 +549,8 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     int* start = nullptr;
     uint64_t* bmask = nullptr;
     uint64_t* smask = nullptr;
+    int* rownear = nullptr;
+    int64_t* nearb = nullptr;
     if (n > 0) {
         const int64_t m = t.bg.nbins + 1;
         const int nb = (int)((m + kScanTile - 1) / kScanTile);
@@ -560,10 +571,13 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
         if (!a.fits()) return DNNI_E_SCRATCH;
         k_block_masks<<<(int)((nblk * 32 + 255) / 256), 256, 0, st>>>(start, nblk, bmask);
         k_super_masks<<<(int)((nsup * 32 + 255) / 256), 256, 0, st>>>(bmask, nsup, smask);
+        rownear = (int*)(base + a.take(sizeof(int) * nblk));
+        nearb = (int64_t*)(base + a.take(sizeof(int64_t) * nblk));
+        if (!a.fits()) return DNNI_E_SCRATCH;
     }
     {
         dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        launch_nearest(t, sorted, start, bmask, smask, pix, d_site, (int2*)(base + o_far), sc, sms, st);
+        launch_nearest(t, sorted, start, bmask, smask, rownear, nearb, pix, d_site, (int2*)(base + o_far), sc, sms, st);
         k_decide<<<1, 32, 0, st>>>(sc, npix);
         if (cudaMemsetAsync(D, 0, sizeof(unsigned long long) * cells, st) != cudaSuccess ||
             cudaMemsetAsync(Dc, 0, sizeof(int) * cells, st) != cudaSuccess)

@@ -22,7 +22,7 @@ struct dnni_ctx {
     cudaStream_t stream = nullptr;
     dnni_settings s{};
     // per-work-package scratch (grow-only until dnni_clear)
-    DevBuf rank, sorted, cnt, start, bsum, pix, D, Dc, bmask, smask, far;
+    DevBuf rank, sorted, cnt, start, bsum, pix, D, Dc, bmask, smask, far, rownear, near;
     // staging for the host-buffer entry point
     DevBuf in_xyz, in_gid, out_h, out_site;
     dnni::Scalars* d_sc = nullptr;

@@ -112,6 +112,7 @@ DNNI_HD int udiv32(long long a, long long b) { return (int)((uint32_t)a / (uint3
 // with exact products.
 DNNI_HD int r2_of(long long d2, long long cs2, int cap) {
     if (d2 >= ((long long)cap + 1) * cs2) return cap;
+    if (d2 < (1LL << 32) && cs2 < (1LL << 32)) return (int)((uint32_t)d2 / (uint32_t)cs2);
     long long q = (long long)((double)d2 / (double)cs2);
     while (q > 0 && q * cs2 > d2) --q;
     while ((q + 1) * cs2 <= d2) ++q;
@@ -566,12 +567,49 @@ DNNI_HD void search_disc(const BinGrid& g, const int4* __restrict__ pts, const i
     }
 }
 
+// Block index (in bmask order) of block (cx, cy) of the block grid.
+DNNI_HD int64_t block_index(const BinGrid& g, int cx, int cy) {
+    return ((int64_t)((cy >> 3) * g.n2x + (cx >> 3)) << 6) + (((cy & 7) << 3) | (cx & 7));
+}
+
+// A first bound from the nearest non-empty block map: the points of the bin
+// of block `nb` (in bmask order) whose box is closest to the pixel.
+DNNI_HD void seed_from_block(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                             const uint64_t* __restrict__ bmask, int64_t nb, int px, int py, Best& b) {
+    const long long bs = g.bs, u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
+    const int64_t sidx = nb >> 6;
+    const int m = (int)(nb & 63);
+    const long long BX0 = g.gx0 + (long long)(sidx % g.n2x) * u2 + (long long)(m & 7) * u1;
+    const long long BY0 = g.gy0 + (long long)(sidx / g.n2x) * u2 + (long long)(m >> 3) * u1;
+    uint64_t bm = DNNI_LDG(&bmask[nb]);
+    long long qlb = LLONG_MAX;
+    int q_idx = 0;
+    while (bm) {
+        const int l = ffs64(bm);
+        bm &= bm - 1;
+        const long long QX0 = BX0 + (long long)(l & 7) * bs, QY0 = BY0 + (long long)(l >> 3) * bs;
+        const long long lb = box_lb(px, py, QX0, QX0 + bs - 1, QY0, QY0 + bs - 1);
+        if (lb < qlb) { qlb = lb; q_idx = l; }
+    }
+    const int64_t id = (nb << 6) + q_idx;
+    scan_points(b, pts, DNNI_LDG(&start[id]), DNNI_LDG(&start[id + 1]), px, py);
+}
+
 // Completes the search of a pixel that the bin rings did not settle: the
 // bound so far (b) or else the nearest non-empty superblock gives a real
 // site, and the disc of that bound is searched exhaustively.
 DNNI_HD void finish_search(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                            const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask,
-                           int px, int py, Best& b) {
+                           int px, int py, Best& b, const int64_t* __restrict__ near = nullptr) {
+    if (near) {
+        // the nearest non-empty block of the pixel's block
+        const int n1x = g.nbx >> 3;
+        int bx = udiv32((long long)px - g.gx0, g.bs), by = udiv32((long long)py - g.gy0, g.bs);
+        bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
+        by = by < g.nby - 1 ? by : g.nby - 1;
+        const int64_t nb = DNNI_LDG(&near[(int64_t)(by >> 3) * n1x + (bx >> 3)]);
+        if (nb >= 0) seed_from_block(g, pts, start, bmask, nb, px, py, b);
+    }
     if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, bmask, smask, px, py, b);
     search_disc(g, pts, start, bmask, smask, px, py, b);
 }
@@ -681,6 +719,51 @@ __global__ void __launch_bounds__(256) k_super_masks(const uint64_t* __restrict_
     const uint64_t* b = bmask + (sidx << 6);
     const unsigned mlo = __ballot_sync(0xffffffffu, b[lane] != 0), mhi = __ballot_sync(0xffffffffu, b[lane + 32] != 0);
     if (lane == 0) smask[sidx] = (uint64_t)mlo | ((uint64_t)mhi << 32);
+}
+
+// Nearest non-empty block map, exact in block-centre distance: per block
+// row the nearest non-empty column (forward and backward sweep), then per
+// block the best row found by walking rows outward until the row offset
+// alone exceeds the best distance.  near[cy * n1x + cx] = bmask index of the
+// chosen block, -1 when the grid has no points.
+__global__ void k_block_rows(BinGrid g, const uint64_t* __restrict__ bmask, int* __restrict__ rownear) {
+    const int n1x = g.nbx >> 3, n1y = g.nby >> 3;
+    const int cy = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cy >= n1y) return;
+    int* row = rownear + (int64_t)cy * n1x;
+    int last = -1;
+    for (int cx = 0; cx < n1x; ++cx) {
+        if (bmask[block_index(g, cx, cy)]) last = cx;
+        row[cx] = last;
+    }
+    last = -1;
+    for (int cx = n1x - 1; cx >= 0; --cx) {
+        if (bmask[block_index(g, cx, cy)]) last = cx;
+        const int l = row[cx];
+        if (last >= 0 && (l < 0 || last - cx < cx - l)) row[cx] = last;
+    }
+}
+
+__global__ void k_block_near(BinGrid g, const int* __restrict__ rownear, int64_t* __restrict__ near) {
+    const int n1x = g.nbx >> 3, n1y = g.nby >> 3;
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= (int64_t)n1x * n1y) return;
+    const int cx = (int)(k % n1x), cy = (int)(k / n1x);
+    long long best = LLONG_MAX;
+    int bxn = -1, byn = -1;
+    for (int d = 0; d < n1y; ++d) {
+        if ((long long)d * d > best) break;
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            if (d == 0 && sgn > 0) continue;
+            const int y = cy + sgn * d;
+            if (y < 0 || y >= n1y) continue;
+            const int x = rownear[(int64_t)y * n1x + cx];
+            if (x < 0) continue;
+            const long long v = (long long)(x - cx) * (x - cx) + (long long)d * d;
+            if (v < best) { best = v; bxn = x; byn = y; }
+        }
+    }
+    near[k] = bxn >= 0 ? block_index(g, bxn, byn) : -1;
 }
 
 // ---- exclusive scan of the bin counts (three passes, 4096 items per block) ----
@@ -897,7 +980,7 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
             if (staged) {
                 const BinWindow w{wx0, wy0, wnx, wny, s_lstart, s_gstart, s_pts};
                 done = window_fits32(g, w) ? search_window_fast32(g, w, px, py, b) : search_window_fast(g, w, px, py, b);
-                b.idx = window_global_index(w, b.idx);
+                if (!done) b.idx = window_global_index(w, b.idx);
             } else {
                 done = search_bins(g, pts, start, px, py, b);
             }
@@ -927,7 +1010,8 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
 // consecutive ones (neighbouring pixels of one tile row).
 __global__ void __launch_bounds__(256, 3) k_near_far(TileParams t, const int4* __restrict__ pts,
                                                      const int* __restrict__ start, const uint64_t* __restrict__ bmask,
-                                                     const uint64_t* __restrict__ smask, const int2* __restrict__ far,
+                                                     const uint64_t* __restrict__ smask,
+                                                     const int64_t* __restrict__ near, const int2* __restrict__ far,
                                                      int2* __restrict__ pix, uint32_t* __restrict__ site,
                                                      Scalars* __restrict__ sc) {
     const int count = sc->nfar;
@@ -941,7 +1025,7 @@ __global__ void __launch_bounds__(256, 3) k_near_far(TileParams t, const int4* _
             const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
             Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
             if (item.y >= 0) consider(b, __ldg(&pts[item.y]), item.y, px, py);
-            finish_search(t.bg, pts, start, bmask, smask, px, py, b);
+            finish_search(t.bg, pts, start, bmask, smask, px, py, b, near);
             settle_pixel(t, i, j, b, pix, site);
             R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
         }

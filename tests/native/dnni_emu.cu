@@ -63,6 +63,41 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
     for (int64_t k = 0; k < nsup; ++k)
         for (int m = 0; m < 64; ++m)
             if (bmask[k * 64 + m]) smask[k] |= 1ull << m;
+    // nearest non-empty block map (the k_block_rows / k_block_near rule)
+    const int n1x = g.nbx >> 3, n1y = g.nby >> 3;
+    std::vector<int> rownear((size_t)n1x * n1y, -1);
+    std::vector<int64_t> nearmap((size_t)n1x * n1y, -1);
+    for (int cy = 0; cy < n1y; ++cy) {
+        int last = -1;
+        for (int cx = 0; cx < n1x; ++cx) {
+            if (bmask[block_index(g, cx, cy)]) last = cx;
+            rownear[(size_t)cy * n1x + cx] = last;
+        }
+        last = -1;
+        for (int cx = n1x - 1; cx >= 0; --cx) {
+            if (bmask[block_index(g, cx, cy)]) last = cx;
+            const int l = rownear[(size_t)cy * n1x + cx];
+            if (last >= 0 && (l < 0 || last - cx < cx - l)) rownear[(size_t)cy * n1x + cx] = last;
+        }
+    }
+    for (int cy = 0; cy < n1y; ++cy)
+        for (int cx = 0; cx < n1x; ++cx) {
+            long long best = LLONG_MAX;
+            int bxn = -1, byn = -1;
+            for (int d = 0; d < n1y; ++d) {
+                if ((long long)d * d > best) break;
+                for (int sgn = -1; sgn <= 1; sgn += 2) {
+                    if (d == 0 && sgn > 0) continue;
+                    const int y = cy + sgn * d;
+                    if (y < 0 || y >= n1y) continue;
+                    const int x = rownear[(size_t)y * n1x + cx];
+                    if (x < 0) continue;
+                    const long long v = (long long)(x - cx) * (x - cx) + (long long)d * d;
+                    if (v < best) { best = v; bxn = x; byn = y; }
+                }
+            }
+            nearmap[(size_t)cy * n1x + cx] = bxn >= 0 ? block_index(g, bxn, byn) : -1;
+        }
     const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
     std::vector<int2> pix(npix);
     int max_r2 = -1;
@@ -114,7 +149,7 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
                         const BinWindow w{wx0, wy0, wnx, wny, lstart.data(), gstart.data(), lpts.data()};
                         done = window_fits32(g, w) ? search_window_fast32(g, w, px, py, b)
                                                    : search_window_fast(g, w, px, py, b);
-                        b.idx = window_global_index(w, b.idx);
+                        if (!done) b.idx = window_global_index(w, b.idx);
                     } else {
                         done = search_bins(g, sorted.data(), start.data(), px, py, b);
                     }
@@ -128,7 +163,7 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
         const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
         Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
         if (it.y >= 0) consider(b, sorted[it.y], it.y, px, py);
-        finish_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), px, py, b);
+        finish_search(g, sorted.data(), start.data(), bmask.data(), smask.data(), px, py, b, nearmap.data());
         settle(i, j, b);
     }
     int packed, K;
