@@ -107,6 +107,12 @@ void dnni_bin_grid(const dnni_ctx* c, const int32_t bbox[6], int64_t n, TilePara
     plan_bins(bbox, n, (double)c->s.bin_target, t);
 }
 
+// Worklist capacity: every dense warp (32 pixels of a tile row, the raster
+// padded to whole tiles) may append one group of 32 slots.
+static int64_t far_slots(const TileParams& t) {
+    return (int64_t)((t.rw + kTileX - 1) / kTileX * kTileX) * ((t.rh + kTileY - 1) / kTileY * kTileY);
+}
+
 // Nearest-site passes: dense tiles, then the far worklist.
 static void launch_nearest(const TileParams& t, const int4* sorted, const int* start, const uint64_t* bmask,
                            const uint64_t* smask, int* rownear, int64_t* near, int2* pix, uint32_t* site, int2* far,
@@ -200,7 +206,7 @@ dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32
     }
     if (timing) CK(cudaEventRecord(c->ev[1], st));
     {
-        if ((rs = dnni_ensure(c, c->far, sizeof(int2) * npix))) return rs;
+        if ((rs = dnni_ensure(c, c->far, sizeof(int2) * far_slots(t)))) return rs;
         const int64_t nblk = n > 0 ? t.bg.nbins / kBinsPerBlock : 1;
         if ((rs = dnni_ensure(c, c->rownear, sizeof(int) * nblk))) return rs;
         if ((rs = dnni_ensure(c, c->near, sizeof(int64_t) * nblk))) return rs;
@@ -520,7 +526,7 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     const size_t o_Dc = a.take(sizeof(int) * cells);
     const size_t o_rank = n > 0 ? a.take(sizeof(int) * n) : 0;
     const size_t o_sorted = n > 0 ? a.take(sizeof(int4) * n) : 0;
-    const size_t o_far = a.take(sizeof(int2) * npix);
+    const size_t o_far = a.take(sizeof(int2) * far_slots(t));
     if (!a.fits()) return DNNI_E_SCRATCH;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

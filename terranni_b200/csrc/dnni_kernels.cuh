@@ -903,8 +903,8 @@ __device__ __forceinline__ void warp_stats(const TileParams& t, int R2, Scalars*
 // pixel row of the tile): the tile's bin window (bin rings of every pixel)
 // is staged in shared memory and the rings are searched there; windows too
 // large for shared memory use the global arrays.  Pixels the rings do not
-// settle go to the far worklist (count sc->nfar), each with its best site so
-// far.  With no points every pixel is settled as "no site".
+// settle go to the far worklist (sc->nfar slots, in groups of 32), each with
+// its best site so far.  With no points every pixel is settled as "no site".
 __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __restrict__ pts,
                                                     const int* __restrict__ start, int2* __restrict__ pix,
                                                     uint32_t* __restrict__ site, int2* __restrict__ far,
@@ -996,18 +996,97 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
             if (site) site[o] = 0xFFFFFFFFu;
         }
     }
-    // worklist append, warp-aggregated
+    // worklist: a warp with any unsettled pixel appends its whole row of 32
+    // slots as one group (settled or absent pixels as x = -1), so that a far
+    // warp later takes 32 neighbouring pixels
     const unsigned mfar = __ballot_sync(0xffffffffu, far_pixel);
     const int lane = threadIdx.x;
-    int base = 0;
-    if (lane == 0 && mfar) base = atomicAdd(&sc->nfar, __popc(mfar));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (far_pixel) far[base + __popc(mfar & ((1u << lane) - 1u))] = make_int2(j * t.rw + i, b.idx);
+    if (mfar) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&sc->nfar, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        far[base + lane] = far_pixel ? make_int2(j * t.rw + i, b.idx) : make_int2(-1, -1);
+    }
     warp_stats(t, R2, sc, blockIdx.x + blockIdx.y * 7 + threadIdx.y);
 }
 
-// Far pass over the worklist: grid-stride over the items, a warp takes 32
-// consecutive ones (neighbouring pixels of one tile row).
+__device__ __forceinline__ long long warp_min64(long long v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) { const long long w = __shfl_xor_sync(0xffffffffu, v, o); v = w < v ? w : v; }
+    return v;
+}
+__device__ __forceinline__ long long warp_max64(long long v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) { const long long w = __shfl_xor_sync(0xffffffffu, v, o); v = w > v ? w : v; }
+    return v;
+}
+
+// Warp-cooperative exact search for the 32 pixels of one worklist group
+// (neighbouring pixels of one tile row; inactive lanes have act = false).
+// The warp walks the superblocks of the union of the lanes' bound boxes
+// (rows outward from the group's centre) and, uniformly, the set bits of
+// the occupancy masks; each lane tests every cell's box bound against its
+// own best, a cell is entered when any lane needs it, and every point of an
+// entered bin is loaded once and considered by the lanes that need the bin.
+// Complete for each active lane whose b holds a real site on entry, by the
+// same argument as search_disc.
+__device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
+                                 const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask, bool act,
+                                 int px, int py, Best& b) {
+    const unsigned full = 0xffffffffu;
+    const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
+    const long long reach = act ? reach_of(b.d2) : 0;
+    const long long xlo = warp_min64(act ? px - reach : LLONG_MAX), xhi = warp_max64(act ? px + reach : LLONG_MIN);
+    const long long ylo = warp_min64(act ? py - reach : LLONG_MAX), yhi = warp_max64(act ? py + reach : LLONG_MIN);
+    if (xlo > xhi) return;   // no active lane
+    int sx0, sx1, sy0, sy1;
+    cell_range((xlo + xhi) / 2, (xhi - xlo) / 2 + 1, gx0, u2, g.n2x, sx0, sx1);
+    cell_range((ylo + yhi) / 2, (yhi - ylo) / 2 + 1, gy0, u2, g.n2y, sy0, sy1);
+    if (sx0 > sx1 || sy0 > sy1) return;
+    const long long cyy = warp_min64(act ? py : LLONG_MAX);
+    int csy = udiv32((cyy < gy0 ? gy0 : cyy) - gy0, u2);
+    csy = csy < sy0 ? sy0 : (csy > sy1 ? sy1 : csy);
+    const int span = (csy - sy0) > (sy1 - csy) ? (csy - sy0) : (sy1 - csy);
+    for (int r = 0; r <= 2 * span; ++r) {
+        const int sy = csy + ((r & 1) ? -((r + 1) >> 1) : (r >> 1));
+        if (sy < sy0 || sy > sy1) continue;
+        const long long SY0 = gy0 + (long long)sy * u2;
+        for (int sx = sx0; sx <= sx1; ++sx) {
+            const int sidx = sy * g.n2x + sx;
+            uint64_t sm = __ldg(&smask[sidx]);
+            if (!sm) continue;
+            const long long SX0 = gx0 + (long long)sx * u2;
+            if (!__any_sync(full, act && box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) <= b.d2)) continue;
+            while (sm) {
+                const int m = ffs64(sm);
+                sm &= sm - 1;
+                const long long BX0 = SX0 + (long long)(m & 7) * u1, BY0 = SY0 + (long long)(m >> 3) * u1;
+                if (!__any_sync(full, act && box_lb(px, py, BX0, BX0 + u1 - 1, BY0, BY0 + u1 - 1) <= b.d2)) continue;
+                const int64_t blk = ((int64_t)sidx << 6) + m;
+                uint64_t bm = __ldg(&bmask[blk]);
+                while (bm) {
+                    const int l = ffs64(bm);
+                    bm &= bm - 1;
+                    const long long QX0 = BX0 + (long long)(l & 7) * bs, QY0 = BY0 + (long long)(l >> 3) * bs;
+                    const bool need = act && box_lb(px, py, QX0, QX0 + bs - 1, QY0, QY0 + bs - 1) <= b.d2;
+                    if (!__any_sync(full, need)) continue;
+                    const int64_t id = (blk << 6) + l;
+                    const int s0 = __ldg(&start[id]), e0 = __ldg(&start[id + 1]);
+                    for (int q = s0; q < e0; ++q) {
+                        const int4 p = __ldg(&pts[q]);
+                        if (need) consider(b, p, q, px, py);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Far pass over the worklist: one warp per group of 32 slots (grid-stride).
+// Each lane seeds its bound (its best site so far, else the nearest
+// non-empty block's closest bin, else the nearest non-empty superblock) and
+// the warp searches the union of the bound discs cooperatively.
 __global__ void __launch_bounds__(256, 3) k_near_far(TileParams t, const int4* __restrict__ pts,
                                                      const int* __restrict__ start, const uint64_t* __restrict__ bmask,
                                                      const uint64_t* __restrict__ smask,
@@ -1016,16 +1095,28 @@ __global__ void __launch_bounds__(256, 3) k_near_far(TileParams t, const int4* _
                                                      Scalars* __restrict__ sc) {
     const int count = sc->nfar;
     const int lane = threadIdx.x & 31;
+    const int n1x = t.bg.nbx >> 3;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += gridDim.x * blockDim.x) {
-        const int it = base + lane;
-        int R2 = -1;
-        if (it < count) {
-            const int2 item = far[it];
-            const int i = item.x % t.rw, j = item.x / t.rw;
-            const int px = (t.rx0 + i) * t.cs, py = (t.ry0 + j) * t.cs;
-            Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+        const int2 item = far[base + lane];
+        const bool act = item.x >= 0;
+        int i = 0, j = 0, px = 0, py = 0;
+        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+        if (act) {
+            i = item.x % t.rw;
+            j = item.x / t.rw;
+            px = (t.rx0 + i) * t.cs;
+            py = (t.ry0 + j) * t.cs;
             if (item.y >= 0) consider(b, __ldg(&pts[item.y]), item.y, px, py);
-            finish_search(t.bg, pts, start, bmask, smask, px, py, b, near);
+            int bx = udiv32((long long)px - t.bg.gx0, t.bg.bs), by = udiv32((long long)py - t.bg.gy0, t.bg.bs);
+            bx = bx < t.bg.nbx - 1 ? bx : t.bg.nbx - 1;
+            by = by < t.bg.nby - 1 ? by : t.bg.nby - 1;
+            const int64_t nb = __ldg(&near[(int64_t)(by >> 3) * n1x + (bx >> 3)]);
+            if (nb >= 0) seed_from_block(t.bg, pts, start, bmask, nb, px, py, b);
+            if (b.d2 == LLONG_MAX) seed_from_superblocks(t.bg, pts, start, bmask, smask, px, py, b);
+        }
+        search_disc_warp(t.bg, pts, start, bmask, smask, act, px, py, b);
+        int R2 = -1;
+        if (act) {
             settle_pixel(t, i, j, b, pix, site);
             R2 = r2_of(b.d2, (long long)t.cs * t.cs, t.r2cap);
         }
