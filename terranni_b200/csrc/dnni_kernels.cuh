@@ -352,7 +352,25 @@ DNNI_HD void scan_local32(Best32& b, const int4* lpts, int s, int e, int px, int
 }
 
 DNNI_HD bool window_fits32(const BinGrid& g, const BinWindow& w) {
-    return (long long)(w.wnx + 1) * g.bs < 32768 && (long long)(w.wny + 1) * g.bs < 32768;
+    const long long ax = g.gx0 < 0 ? -(long long)g.gx0 : g.gx0, ay = g.gy0 < 0 ? -(long long)g.gy0 : g.gy0;
+    return (long long)(w.wnx + 1) * g.bs < 32768 && (long long)(w.wny + 1) * g.bs < 32768 &&
+           ax + (long long)(g.nbx + 1) * g.bs < (1LL << 31) && ay + (long long)(g.nby + 1) * g.bs < (1LL << 31);
+}
+
+// ring_done for the 32-bit window path: every coordinate involved lies
+// within the window (less than 2^15 LAS units from the pixel), so the margins
+// and their squares fit in 32 bits; a missing best (none found) never stops.
+DNNI_HD bool ring_done32(long long best, int px, int py, const BinGrid& g, int x0, int x1, int y0, int y1) {
+    if (best == LLONG_MAX) return false;
+    int m = INT_MAX;
+    bool open = false;
+    const int gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
+    if (x0 > 0) { const int v = px - (gx0 + x0 * bs) + 1; m = v < m ? v : m; open = true; }
+    if (x1 < g.nbx - 1) { const int v = gx0 + (x1 + 1) * bs - px; m = v < m ? v : m; open = true; }
+    if (y0 > 0) { const int v = py - (gy0 + y0 * bs) + 1; m = v < m ? v : m; open = true; }
+    if (y1 < g.nby - 1) { const int v = gy0 + (y1 + 1) * bs - py; m = v < m ? v : m; open = true; }
+    if (!open) return true;
+    return best < (long long)m * m;
 }
 
 DNNI_HD bool search_window_fast32(const BinGrid& g, const BinWindow& w, int px, int py, Best& out) {
@@ -370,7 +388,7 @@ DNNI_HD bool search_window_fast32(const BinGrid& g, const BinWindow& w, int px, 
         for (int r = y0; r <= y1; ++r)
             scan_local32(b, w.lpts, w.lstart[r * w.wnx + x0], w.lstart[r * w.wnx + x1 + 1], px, py);
     }
-    done = ring_done(best32_d2(b), px, py, gx0, gy0, bs, bx - 1, bx + 1, by - 1, by + 1, g.nbx, g.nby);
+    done = ring_done32(best32_d2(b), px, py, g, bx - 1, bx + 1, by - 1, by + 1);
     if (!done) {
         const int x0 = lx - 2 > 0 ? lx - 2 : 0, x1 = lx + 2 < w.wnx - 1 ? lx + 2 : w.wnx - 1;
         const long long X0 = gx0 + (long long)(w.wx0 + x0) * bs, X1 = gx0 + (long long)(w.wx0 + x1 + 1) * bs - 1;
@@ -391,7 +409,7 @@ DNNI_HD bool search_window_fast32(const BinGrid& g, const BinWindow& w, int px, 
             for (int r = ya; r <= yb; ++r)
                 scan_local32(b, w.lpts, w.lstart[r * w.wnx + c], w.lstart[r * w.wnx + c + 1], px, py);
         }
-        done = ring_done(best32_d2(b), px, py, gx0, gy0, bs, bx - 2, bx + 2, by - 2, by + 2, g.nbx, g.nby);
+        done = ring_done32(best32_d2(b), px, py, g, bx - 2, bx + 2, by - 2, by + 2);
     }
     out.d2 = best32_d2(b);
     out.gid = b.key == ~0ull ? 0xFFFFFFFFu : (uint32_t)(b.key & 0xFFFFFFFFull);
@@ -870,6 +888,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restri
 // ---- nearest site per raster pixel ----
 
 constexpr int kWinMaxBins = 2048;
+constexpr int kWinMaxRows = 256;
 constexpr int kWinMaxPts = 3072;
 constexpr size_t kDenseSmem = sizeof(int4) * kWinMaxPts + sizeof(int) * (2 * kWinMaxBins + 1);
 
@@ -905,7 +924,7 @@ __device__ __forceinline__ void warp_stats(const TileParams& t, int R2, Scalars*
 // large for shared memory use the global arrays.  Pixels the rings do not
 // settle go to the far worklist (sc->nfar slots, in groups of 32), each with
 // its best site so far.  With no points every pixel is settled as "no site".
-__global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __restrict__ pts,
+__global__ void __launch_bounds__(256, 3) k_near_dense(TileParams t, const int4* __restrict__ pts,
                                                     const int* __restrict__ start, int2* __restrict__ pix,
                                                     uint32_t* __restrict__ site, int2* __restrict__ far,
                                                     Scalars* __restrict__ sc) {
@@ -913,7 +932,7 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
     int4* s_pts = smem;
     int* s_lstart = (int*)(smem + kWinMaxPts);
     int* s_gstart = s_lstart + kWinMaxBins + 1;
-    __shared__ int wsum[8];
+    __shared__ int s_rowbase[kWinMaxRows];
     __shared__ int s_total;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int i0 = blockIdx.x * kTileX, j0 = blockIdx.y * kTileY;
@@ -925,30 +944,52 @@ __global__ void __launch_bounds__(256) k_near_dense(TileParams t, const int4* __
     if (t.npts > 0) {
         tile_window(t, i0, j0, wx0, wy0, wnx, wny);
         const int nwb = wnx * wny;
-        if (nwb <= kWinMaxBins) {
-            // per-bin counts -> local starts (8 consecutive bins per thread)
-            int c[8], sum = 0;
+        if (nwb <= kWinMaxBins && wny <= kWinMaxRows) {
+            // per-bin counts -> local starts: warp w takes window rows w, w+8,
+            // ...; lanes take columns, with a warp scan along the row
+            const int warp = tid >> 5, lane = tid & 31;
+            for (int r = warp; r < wny; r += 8) {
+                int rowsum = 0;
+                for (int c0 = 0; c0 < wnx; c0 += 32) {
+                    const int c = c0 + lane;
+                    int cnt = 0;
+                    if (c < wnx) {
+                        const int64_t id = bin_id(g, wx0 + c, wy0 + r);
+                        const int gs = __ldg(&start[id]);
+                        cnt = __ldg(&start[id + 1]) - gs;
+                        s_gstart[r * wnx + c] = gs;
+                    }
+                    int x = cnt;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int lk = tid * 8 + k;
-                c[k] = 0;
-                if (lk < nwb) {
-                    const int64_t id = bin_id(g, wx0 + lk % wnx, wy0 + lk / wnx);
-                    const int gs = __ldg(&start[id]);
-                    c[k] = __ldg(&start[id + 1]) - gs;
-                    s_gstart[lk] = gs;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    if (c < wnx) s_lstart[r * wnx + c] = rowsum + x - cnt;
+                    rowsum += __shfl_sync(0xffffffffu, x, 31);
                 }
-                sum += c[k];
+                if (lane == 0) s_rowbase[r] = rowsum;
             }
-            int total;
-            int run = block_exclusive_sum(sum, wsum, total, tid);
+            __syncthreads();
+            if (warp == 0) {
+                int run = 0;
+                for (int r0 = 0; r0 < wny; r0 += 32) {
+                    const int r = r0 + lane;
+                    const int v = r < wny ? s_rowbase[r] : 0;
+                    int x = v;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int lk = tid * 8 + k;
-                if (lk < nwb) s_lstart[lk] = run;
-                run += c[k];
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    if (r < wny) s_rowbase[r] = run + x - v;
+                    run += __shfl_sync(0xffffffffu, x, 31);
+                }
+                if (lane == 0) { s_lstart[nwb] = run; s_total = run; }
             }
-            if (tid == 0) { s_lstart[nwb] = total; s_total = total; }
+            __syncthreads();
+            for (int r = warp; r < wny; r += 8)
+                for (int c = lane; c < wnx; c += 32) s_lstart[r * wnx + c] += s_rowbase[r];
             __syncthreads();
             staged = s_total <= kWinMaxPts;
             if (staged) {
@@ -1030,13 +1071,61 @@ __device__ __forceinline__ long long warp_max64(long long v) {
 // entered bin is loaded once and considered by the lanes that need the bin.
 // Complete for each active lane whose b holds a real site on entry, by the
 // same argument as search_disc.
+__device__ __forceinline__ uint64_t warp_or64(uint64_t v) {
+    const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)v), hi = __reduce_or_sync(0xffffffffu, (unsigned)(v >> 32));
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// 8 x 8 cell mask of the cells [a0,a1] x [b0,b1] (x = bit & 7, y = bit >> 3);
+// 0 when the range is empty.
+__device__ __forceinline__ uint64_t box_mask8(int a0, int a1, int b0, int b1) {
+    a0 = a0 < 0 ? 0 : a0;
+    b0 = b0 < 0 ? 0 : b0;
+    a1 = a1 > 7 ? 7 : a1;
+    b1 = b1 > 7 ? 7 : b1;
+    if (a0 > a1 || b0 > b1) return 0;
+    const uint64_t row = (uint64_t)((0xFFu << a0) & (0xFFu >> (7 - a1)) & 0xFFu);
+    uint64_t m = 0;
+    for (int y = b0; y <= b1; ++y) m |= row << (8 * y);
+    return m;
+}
+
+// Cells (u wide, 8 per side, origin o) that the box [c - r, c + r] may touch,
+// widened by one cell on each side so float rounding can only add cells.
+__device__ __forceinline__ void cell_span8(long long c, long long r, long long o, float inv_u, int& lo, int& hi) {
+    const float a = (float)(c - r - o) * inv_u, b = (float)(c + r - o) * inv_u;
+    lo = a < -2.0f ? -2 : (a > 9.0f ? 9 : (int)floorf(a)) - 1;
+    hi = b < -2.0f ? -2 : (b > 9.0f ? 9 : (int)floorf(b)) + 1;
+}
+
+// Squared box bound in 32-bit arithmetic, for gaps below 46341 (larger
+// gaps are clamped there, which still exceeds any bound below 2^31).
+__device__ __forceinline__ unsigned box_lb32(int rx, int ry, int x0, int x1, int y0, int y1) {
+    int dx = rx < x0 ? x0 - rx : (rx > x1 ? rx - x1 : 0);
+    int dy = ry < y0 ? y0 - ry : (ry > y1 ? ry - y1 : 0);
+    dx = dx < 46340 ? dx : 46340;
+    dy = dy < 46340 ? dy : 46340;
+    return (unsigned)(dx * dx) + (unsigned)(dy * dy);
+}
+
+// Warp-cooperative exact search for the 32 pixels of one worklist group
+// (neighbouring pixels of one tile row; inactive lanes have act = false).
+// The warp walks the superblocks of the union of the lanes' bound boxes
+// (rows outward from the group's centre).  Inside a superblock, candidate
+// blocks are the non-empty ones inside some lane's bound box (an OR of the
+// lanes' box masks); each candidate gets every lane's exact box test and is
+// entered when any lane needs it; bins likewise; every point of an entered
+// bin is loaded once and considered by the lanes that need the bin.  All
+// control flow is uniform across the warp.  Complete for each active lane
+// whose b holds a real site on entry, by the same argument as search_disc.
 __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                                  const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask, bool act,
                                  int px, int py, Best& b) {
     const unsigned full = 0xffffffffu;
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
     const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
-    const long long reach = act ? reach_of(b.d2) : 0;
+    const float inv_u1 = 1.0f / (float)u1, inv_bs = 1.0f / (float)bs;
+    long long reach = act ? reach_of(b.d2) : 0;
     const long long xlo = warp_min64(act ? px - reach : LLONG_MAX), xhi = warp_max64(act ? px + reach : LLONG_MIN);
     const long long ylo = warp_min64(act ? py - reach : LLONG_MAX), yhi = warp_max64(act ? py + reach : LLONG_MIN);
     if (xlo > xhi) return;   // no active lane
@@ -1044,6 +1133,8 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
     cell_range((xlo + xhi) / 2, (xhi - xlo) / 2 + 1, gx0, u2, g.n2x, sx0, sx1);
     cell_range((ylo + yhi) / 2, (yhi - ylo) / 2 + 1, gy0, u2, g.n2y, sy0, sy1);
     if (sx0 > sx1 || sy0 > sy1) return;
+    // 32-bit tests are exact while every active lane's bound is below 2^31
+    const bool small = __all_sync(full, !act || b.d2 < (1LL << 31));
     const long long cyy = warp_min64(act ? py : LLONG_MAX);
     int csy = udiv32((cyy < gy0 ? gy0 : cyy) - gy0, u2);
     csy = csy < sy0 ? sy0 : (csy > sy1 ? sy1 : csy);
@@ -1054,22 +1145,51 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
         const long long SY0 = gy0 + (long long)sy * u2;
         for (int sx = sx0; sx <= sx1; ++sx) {
             const int sidx = sy * g.n2x + sx;
-            uint64_t sm = __ldg(&smask[sidx]);
+            const uint64_t sm = __ldg(&smask[sidx]);
             if (!sm) continue;
             const long long SX0 = gx0 + (long long)sx * u2;
-            if (!__any_sync(full, act && box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) <= b.d2)) continue;
-            while (sm) {
-                const int m = ffs64(sm);
-                sm &= sm - 1;
-                const long long BX0 = SX0 + (long long)(m & 7) * u1, BY0 = SY0 + (long long)(m >> 3) * u1;
-                if (!__any_sync(full, act && box_lb(px, py, BX0, BX0 + u1 - 1, BY0, BY0 + u1 - 1) <= b.d2)) continue;
+            const bool need_s = act && box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) <= b.d2;
+            if (!__any_sync(full, need_s)) continue;
+            // candidate blocks: inside some needing lane's bound box
+            reach = act ? reach_of(b.d2) : 0;
+            uint64_t lm = 0;
+            if (need_s) {
+                int a0, a1, b0, b1;
+                cell_span8(px, reach, SX0, inv_u1, a0, a1);
+                cell_span8(py, reach, SY0, inv_u1, b0, b1);
+                lm = box_mask8(a0, a1, b0, b1);
+            }
+            uint64_t cand = sm & warp_or64(lm);
+            // pixel relative to the superblock (in range whenever the lane needs it)
+            const long long rxl = px - SX0, ryl = py - SY0;
+            const int rx = (int)(rxl < -(1LL << 30) ? -(1LL << 30) : (rxl > (1LL << 30) ? (1LL << 30) : rxl));
+            const int ry = (int)(ryl < -(1LL << 30) ? -(1LL << 30) : (ryl > (1LL << 30) ? (1LL << 30) : ryl));
+            while (cand) {
+                const int m = ffs64(cand);
+                cand &= cand - 1;
+                const int bx0 = (m & 7) * (int)u1, by0 = (m >> 3) * (int)u1;
+                bool need_b;
+                if (small) need_b = act && (long long)box_lb32(rx, ry, bx0, bx0 + (int)u1 - 1, by0, by0 + (int)u1 - 1) <= b.d2;
+                else need_b = act && box_lb(px, py, SX0 + bx0, SX0 + bx0 + u1 - 1, SY0 + by0, SY0 + by0 + u1 - 1) <= b.d2;
+                if (!__any_sync(full, need_b)) continue;
                 const int64_t blk = ((int64_t)sidx << 6) + m;
-                uint64_t bm = __ldg(&bmask[blk]);
-                while (bm) {
-                    const int l = ffs64(bm);
-                    bm &= bm - 1;
-                    const long long QX0 = BX0 + (long long)(l & 7) * bs, QY0 = BY0 + (long long)(l >> 3) * bs;
-                    const bool need = act && box_lb(px, py, QX0, QX0 + bs - 1, QY0, QY0 + bs - 1) <= b.d2;
+                const uint64_t bm = __ldg(&bmask[blk]);
+                uint64_t lq = 0;
+                if (need_b) {
+                    int a0, a1, b0, b1;
+                    const long long rr = reach_of(b.d2);
+                    cell_span8(px, rr, SX0 + bx0, inv_bs, a0, a1);
+                    cell_span8(py, rr, SY0 + by0, inv_bs, b0, b1);
+                    lq = box_mask8(a0, a1, b0, b1);
+                }
+                uint64_t qc = bm & warp_or64(lq);
+                while (qc) {
+                    const int l = ffs64(qc);
+                    qc &= qc - 1;
+                    const int qx0 = bx0 + (l & 7) * (int)bs, qy0 = by0 + (l >> 3) * (int)bs;
+                    bool need;
+                    if (small) need = act && (long long)box_lb32(rx, ry, qx0, qx0 + (int)bs - 1, qy0, qy0 + (int)bs - 1) <= b.d2;
+                    else need = act && box_lb(px, py, SX0 + qx0, SX0 + qx0 + bs - 1, SY0 + qy0, SY0 + qy0 + bs - 1) <= b.d2;
                     if (!__any_sync(full, need)) continue;
                     const int64_t id = (blk << 6) + l;
                     const int s0 = __ldg(&start[id]), e0 = __ldg(&start[id + 1]);

@@ -119,7 +119,7 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
             if (n > 0) {
                 tile_window(t, i0, j0, wx0, wy0, wnx, wny);
                 const int nwb = wnx * wny;
-                if (nwb <= kWinMaxBins) {
+                if (nwb <= kWinMaxBins && wny <= kWinMaxRows) {
                     int run2 = 0;
                     for (int lk = 0; lk < nwb; ++lk) {
                         const int64_t id = bin_id(g, wx0 + lk % wnx, wy0 + lk / wnx);
