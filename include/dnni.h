@@ -65,7 +65,7 @@ typedef struct dnni_settings {
     int32_t small_radius;   /* pixels with floor(d^2/cell^2) <= r^2 use the
                                per-tile stencil, others the span scatter;
                                1..6, 0 = default (3) */
-    int32_t bin_target;     /* mean points per search bin; 0 = default (2) */
+    int32_t bin_target;     /* mean points per search bin; 0 = default (4) */
     int32_t flags;          /* DNNI_F_* */
     uint64_t mem_budget;    /* bytes of device scratch a context may hold;
                                0 = no limit */

@@ -551,7 +551,7 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
         }
         if (hsc.err & kErrRange) return DNNI_E_RANGE;
     }
-    plan_bins(hsc.bbox, n, 2.0, t);
+    plan_bins(hsc.bbox, n, 0.0, t);
     int* start = nullptr;
     uint64_t* bmask = nullptr;
     uint64_t* smask = nullptr;

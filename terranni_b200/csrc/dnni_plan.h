@@ -79,7 +79,7 @@ inline void plan_bins(const int32_t bbox[6], int64_t n, double bin_target, TileP
         yhi = std::max<int64_t>(yhi, bbox[3]);
     }
     const int64_t W = xhi - xlo + 1, Hh = yhi - ylo + 1;
-    const double target = bin_target > 0 ? bin_target : 2.0;
+    const double target = bin_target > 0 ? bin_target : 4.0;
     const double bsd = std::sqrt(target * (double)W * (double)Hh / (double)std::max<int64_t>(n, 1));
     int64_t bs = (int64_t)std::ceil(bsd);
     if (bs < 1) bs = 1;
