@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "DEM cells/s batched vs plain GPU NNI at ≤1e-4 m err vs FP64; p50/p99 tile latency"
 UNIT = "cells/s"
-KERNELS_PER_CALL = 13      # own kernel launches per interpolate call with points
+KERNELS_PER_CALL = 18      # own kernel launches per interpolate call with points (2 + 16)
 FALLBACK_HBM_GBS = 6650.0
 
 

@@ -166,6 +166,54 @@ dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpackage *wp, 
                                                     const uint32_t *d_gid, int64_t n, float *d_h,
                                                     uint32_t *d_site, void *stream);
 
+/* ---- batches: the loop of binRun (terranni.cpp:394-426) as one launch ----
+ *
+ * Many work packages ("tiles") of uneven size run through one launch sequence
+ * whose kernels cover every tile; with use_graph the sequence is captured in a
+ * CUDA graph on the first run and replayed afterwards.  Planning happens once,
+ * at creation, from each tile's geometry and its declared point extent, so a
+ * run never waits on the host. */
+typedef struct dnni_tile {
+    dnni_workpackage wp;
+    int64_t pt_offset, pt_count;   /* the tile's points: rows [pt_offset,
+                                      pt_offset + pt_count) of the xyz (and gid)
+                                      arrays given to the run */
+    int32_t ext_x0, ext_y0, ext_x1, ext_y1;  /* absolute LAS box (inclusive)
+                                      holding every point of the tile; all zero
+                                      = the raster; a point outside fails the
+                                      run with DNNI_E_RANGE */
+    int64_t out_offset;            /* first float of the tile's grid in the
+                                      output array */
+    int64_t site_offset;           /* first uint32 of its site map in the site
+                                      array, -1 = none */
+} dnni_tile;
+
+typedef struct dnni_batch dnni_batch;
+
+typedef struct dnni_batch_options {
+    int32_t small_radius;          /* 0 = the context's setting */
+    int32_t bin_target;            /* 0 = the context's setting */
+    int32_t use_graph;             /* capture the launch sequence in a CUDA graph */
+    int32_t order_by_cost;         /* schedule the largest tiles first */
+} dnni_batch_options;
+
+/* Plans the tiles and allocates the batch's device scratch (allocates). */
+dnni_status dnni_batch_create(dnni_ctx *ctx, const dnni_tile *tiles, int32_t ntiles,
+                              const dnni_batch_options *options, dnni_batch **out);
+/* Runs every tile on device buffers, queued on `stream` (NULL = the
+ * context's stream).  Returns with the work queued unless stats is non-NULL,
+ * in which case it waits, reports totals over the tiles (ms_total is the
+ * device time of the run) and checks the points against the declared
+ * extents (DNNI_E_RANGE); without stats that check is not read back. */
+dnni_status dnni_batch_run_device(dnni_batch *batch, const int32_t *d_xyz, const uint32_t *d_gid,
+                                  float *d_h, uint32_t *d_site, void *stream, dnni_stats *stats);
+/* The same from host buffers: n_rows point rows are copied in, the output
+ * (the largest out_offset + cells of the tiles) and site maps copied out;
+ * always waits and checks the extents. */
+dnni_status dnni_batch_run(dnni_batch *batch, const int32_t *xyz, const uint32_t *gid, int64_t n_rows,
+                           float *out_h, uint32_t *out_site, dnni_stats *stats);
+dnni_status dnni_batch_destroy(dnni_batch *batch);
+
 /* ---- nni::clearRenderbuffers / nni::printTimes (nni.h:87-97) ---- */
 
 /* Free the context's scratch (it is re-created on demand). */

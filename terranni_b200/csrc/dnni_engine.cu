@@ -1,5 +1,5 @@
-// dnni_engine.cu -- context, device scratch and the per-work-package pipeline
-// behind the C ABI in include/dnni.h.
+// dnni_engine.cu -- context, device scratch, batch planning and the launch
+// sequence behind the C ABI in include/dnni.h.
 //
 // Reference counterparts:
 //   nni::init / cuda_nni::init          nni.cpp:569-598, cuda_nni.cu:641-669
@@ -7,18 +7,18 @@
 //   nni::performNNI                     nni.cpp:870-944
 //   nni::clearRenderbuffers / cleanup   nni.cpp:362-379, 563-566
 //   nni::printTimes                     nni.cpp:554-560
+//   binRun's loop over work packages    terranni.cpp:394-426 (the batch API)
 // The GL context, framebuffers, renderbuffers and GL/CUDA interop of the
 // reference have no counterpart: the engine works on plain device buffers.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <numeric>
 #include <string>
 
 #include "../../include/dnni.h"
 #include "dnni_internal.h"
-#include "dnni_kernels.cuh"
-#include "dnni_plan.h"
 
 using namespace dnni;
 
@@ -52,10 +52,181 @@ struct DeviceGuard {
     }
 };
 
-int grid_for(int64_t n, int threads, int cap) {
-    int64_t b = (n + threads - 1) / threads;
-    if (b < 1) b = 1;
-    return (int)(b < cap ? b : cap);
+// Every scratch array a batch needs, in bytes.
+struct ScratchSizes {
+    size_t sorted, rank, cnt, bsum, bmask, smask, rownear, near, pix, far, D, Dc, sc, ctr, tables;
+};
+
+ScratchSizes scratch_sizes(const HostBatch& hb) {
+    const int n = (int)hb.tiles.size();
+    ScratchSizes z;
+    z.sorted = sizeof(int4) * std::max<int64_t>(hb.n_pts, 1);
+    z.rank = sizeof(int) * std::max<int64_t>(hb.n_pts, 1);
+    z.cnt = sizeof(int) * std::max<int64_t>(hb.n_bins, 1);
+    z.bsum = sizeof(int) * std::max<int64_t>(hb.scan_base.back(), 1);
+    z.bmask = sizeof(uint64_t) * std::max<int64_t>(hb.blk_base.back(), 1);
+    z.smask = sizeof(uint64_t) * std::max<int64_t>(hb.sup_base.back(), 1);
+    z.rownear = sizeof(int) * std::max<int64_t>(hb.blk_base.back(), 1);
+    z.near = sizeof(int64_t) * std::max<int64_t>(hb.blk_base.back(), 1);
+    z.pix = sizeof(int2) * std::max<int64_t>(hb.n_pix, 1);
+    z.far = sizeof(FarSlot) * std::max<int64_t>(hb.n_far, 1);
+    z.D = sizeof(unsigned long long) * std::max<int64_t>(hb.n_cells, 1);
+    z.Dc = sizeof(int) * std::max<int64_t>(hb.n_cells, 1);
+    z.sc = sizeof(Scalars) * n;
+    z.ctr = sizeof(BatchCounters);
+    z.tables = TableLayout(n).total;
+    return z;
+}
+
+dnni_status ensure_scratch(dnni_ctx* c, Scratch& s, const ScratchSizes& z, DevArrays& a) {
+    dnni_status rs;
+    if ((rs = dnni_ensure(c, s.sorted, z.sorted)) || (rs = dnni_ensure(c, s.rank, z.rank)) ||
+        (rs = dnni_ensure(c, s.cnt, z.cnt)) || (rs = dnni_ensure(c, s.start, z.cnt)) ||
+        (rs = dnni_ensure(c, s.bsum, z.bsum)) || (rs = dnni_ensure(c, s.bmask, z.bmask)) ||
+        (rs = dnni_ensure(c, s.smask, z.smask)) || (rs = dnni_ensure(c, s.rownear, z.rownear)) ||
+        (rs = dnni_ensure(c, s.near, z.near)) || (rs = dnni_ensure(c, s.pix, z.pix)) ||
+        (rs = dnni_ensure(c, s.far, z.far)) || (rs = dnni_ensure(c, s.D, z.D)) || (rs = dnni_ensure(c, s.Dc, z.Dc)) ||
+        (rs = dnni_ensure(c, s.sc, z.sc)) || (rs = dnni_ensure(c, s.ctr, z.ctr)) ||
+        (rs = dnni_ensure(c, s.tables, z.tables)))
+        return rs;
+    a.sorted = (int4*)s.sorted.p;
+    a.rank = (int*)s.rank.p;
+    a.cnt = (int*)s.cnt.p;
+    a.start = (int*)s.start.p;
+    a.bsum = (int*)s.bsum.p;
+    a.bmask = (uint64_t*)s.bmask.p;
+    a.smask = (uint64_t*)s.smask.p;
+    a.rownear = (int*)s.rownear.p;
+    a.near = (int64_t*)s.near.p;
+    a.pix = (int2*)s.pix.p;
+    a.far = (FarSlot*)s.far.p;
+    a.D = (unsigned long long*)s.D.p;
+    a.Dc = (int*)s.Dc.p;
+    a.sc = (Scalars*)s.sc.p;
+    a.ctr = (BatchCounters*)s.ctr.p;
+    a.tables = (unsigned char*)s.tables.p;
+    return DNNI_OK;
+}
+
+void release_scratch(dnni_ctx* c, Scratch& s) {
+    DevBuf* bufs[] = {&s.sorted, &s.rank, &s.cnt, &s.start, &s.bsum, &s.bmask, &s.smask, &s.rownear,
+                      &s.near, &s.pix, &s.far, &s.D, &s.Dc, &s.sc, &s.ctr, &s.tables};
+    for (DevBuf* b : bufs) dnni_release(*b, c);
+}
+
+// Stencil + finalize, for the batch's stencil radius.
+void launch_final(const BatchTables& bt, int ncta, int rs, const int2* pix, Scalars* sc,
+                  const unsigned long long* S, const int* Sc, float* h, cudaStream_t st) {
+    dim3 blk(32, 16);
+    switch (rs) {
+        case 1: k_final<1><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 2: k_final<2><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 4: k_final<4><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 5: k_final<5><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 6: k_final<6><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        default: k_final<3><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+    }
+}
+
+void set_dense_smem_attr() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(k_near_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmem);
+        done[dev] = true;
+    }
+}
+
+// Launch sequence, part 1: per-tile scalars and the point bounding boxes.
+void launch_prologue(const HostBatch& hb, const BatchTables& bt, const DevArrays& a, const int32_t* d_xyz,
+                     cudaStream_t st) {
+    const int n = (int)hb.tiles.size();
+    k_init_scalars<<<n, 32, 0, st>>>(bt, a.sc, a.ctr);
+    const int nchunk = hb.chunk_base.back();
+    if (nchunk > 0) k_bbox<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.sc, a.ctr);
+}
+
+// Launch sequence, part 2: binning, nearest sites, spans, stencil, finalize.
+// Needs no host synchronisation (a batch's whole sequence can be captured).
+// ev[0..2] (optional) mark the ends of binning, nearest sites and spans.
+void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a, const int32_t* d_xyz,
+                 const uint32_t* d_gid, float* d_h, uint32_t* d_site, int sms, cudaStream_t st,
+                 const cudaEvent_t* ev) {
+    const int nchunk = hb.chunk_base.back();
+    const int64_t nblk = hb.blk_base.back(), nsup = hb.sup_base.back();
+    if (nchunk > 0) {
+        cudaMemsetAsync(a.cnt, 0, sizeof(int) * hb.n_bins, st);
+        k_bin_count<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.cnt, a.rank, a.ctr);
+        const int nscan = hb.scan_base.back();
+        k_scan_partial<<<nscan, kScanThreads, 0, st>>>(bt, a.cnt, a.bsum);
+        k_scan_bsum<<<(int)hb.tiles.size(), 1024, 0, st>>>(bt, a.bsum);
+        k_scan_final<<<nscan, kScanThreads, 0, st>>>(bt, a.cnt, a.bsum, a.start);
+        k_bin_scatter<<<nchunk, 256, 0, st>>>(bt, d_xyz, d_gid, a.start, a.rank, a.sorted);
+        if (nblk > 0) k_block_masks<<<(int)((nblk * 32 + 255) / 256), 256, 0, st>>>(bt, a.start, a.bmask);
+        if (nsup > 0) k_super_masks<<<(int)((nsup * 32 + 255) / 256), 256, 0, st>>>(bt, a.bmask, a.smask);
+        const int nrow1 = hb.row1_base.back();
+        if (nrow1 > 0) k_block_rows<<<(nrow1 + 127) / 128, 128, 0, st>>>(bt, a.bmask, a.rownear);
+        if (nblk > 0) k_block_near<<<(int)((nblk + 255) / 256), 256, 0, st>>>(bt, a.rownear, a.near);
+    }
+    if (ev) cudaEventRecord(ev[0], st);
+    const int nrt = hb.rt_base.back();
+    k_near_dense<<<nrt, dim3(32, 8), kDenseSmem, st>>>(bt, a.sorted, a.start, a.pix, d_site, a.far, a.sc, a.ctr);
+    if (nchunk > 0)
+        k_near_far<<<sms * 6, 256, 0, st>>>(bt, a.sorted, a.start, a.bmask, a.smask, a.near, a.far, a.pix, d_site,
+                                            a.sc, a.ctr);
+    k_decide<<<(int)hb.tiles.size(), 32, 0, st>>>(bt, a.sc);
+    if (ev) cudaEventRecord(ev[1], st);
+    cudaMemsetAsync(a.D, 0, sizeof(unsigned long long) * hb.n_cells, st);
+    cudaMemsetAsync(a.Dc, 0, sizeof(int) * hb.n_cells, st);
+    k_scatter_spans<<<nrt, dim3(32, 8), 0, st>>>(bt, a.pix, a.sc, a.D, a.Dc);
+    if (ev) cudaEventRecord(ev[2], st);
+    const int ngrow = hb.grow_base.back();
+    k_rowscan<unsigned long long><<<ngrow, kScanThreads, 0, st>>>(bt, a.D, a.sc, 0);
+    k_rowscan<int><<<ngrow, kScanThreads, 0, st>>>(bt, a.Dc, a.sc, 1);
+    launch_final(bt, hb.ct_base.back(), hb.rs, a.pix, a.sc, a.D, a.Dc, d_h, st);
+}
+
+// Sums the per-tile scalars into dnni_stats.
+void fold_stats(const Scalars* s, int n, dnni_stats* st) {
+    int64_t big = 0, sp = 0, nod = 0;
+    int mx = -1, packed = 1;
+    for (int t = 0; t < n; ++t) {
+        for (int k = 0; k < kStatSlots; ++k) {
+            big += (int64_t)s[t].big_pixels[k];
+            sp += (int64_t)s[t].spans[k];
+            nod += (int64_t)s[t].nodata[k];
+            mx = std::max(mx, s[t].max_r2[k]);
+        }
+        packed &= s[t].packed;
+    }
+    st->big_pixels = big;
+    st->spans = sp;
+    st->nodata_cells = nod;
+    st->max_r2 = mx;
+    st->packed = packed;
+}
+
+// Uploads a batch's tables through the context's pinned staging buffer.
+dnni_status stage_tables(dnni_ctx* c, const HostBatch& hb, unsigned char* d_tables, cudaStream_t st) {
+    const size_t bytes = TableLayout((int)hb.tiles.size()).total;
+    // the previous upload from the staging buffer must have completed
+    CK(cudaStreamSynchronize(st));
+    if (bytes > c->h_tables_cap) {
+        if (c->h_tables) cudaFreeHost(c->h_tables);
+        c->h_tables = nullptr;
+        c->h_tables_cap = 0;
+        if (cudaMallocHost((void**)&c->h_tables, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(c, DNNI_E_NOMEM, "pinned staging for the tile tables");
+        }
+        c->h_tables_cap = bytes;
+    }
+    pack_tables(hb, c->h_tables);
+    CK(cudaMemcpyAsync(d_tables, c->h_tables, bytes, cudaMemcpyHostToDevice, st));
+    return DNNI_OK;
 }
 
 }  // namespace
@@ -96,141 +267,46 @@ void dnni_release(DevBuf& b, dnni_ctx* c) {
     b.cap = 0;
 }
 
-dnni_status dnni_tile_geometry(dnni_ctx* c, const dnni_workpackage* wp, int64_t n, TileParams& t) {
-    const char* msg = "";
-    dnni_status st = plan_geometry(wp, n, c->s.small_radius, t, &msg);
-    if (st) return set_err(c, st, msg);
-    return DNNI_OK;
-}
-
-void dnni_bin_grid(const dnni_ctx* c, const int32_t bbox[6], int64_t n, TileParams& t) {
-    plan_bins(bbox, n, (double)c->s.bin_target, t);
-}
-
-// Worklist capacity: every dense warp (32 pixels of a tile row, the raster
-// padded to whole tiles) may append one group of 32 slots.
-static int64_t far_slots(const TileParams& t) {
-    return (int64_t)((t.rw + kTileX - 1) / kTileX * kTileX) * ((t.rh + kTileY - 1) / kTileY * kTileY);
-}
-
-// Nearest-site passes: dense tiles, then the far worklist.
-static void launch_nearest(const TileParams& t, const int4* sorted, const int* start, const uint64_t* bmask,
-                           const uint64_t* smask, int* rownear, int64_t* near, int2* pix, uint32_t* site, int2* far,
-                           Scalars* sc, int sms, cudaStream_t st) {
-    static thread_local int attr_dev = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (attr_dev != dev) {
-        cudaFuncSetAttribute(k_near_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmem);
-        attr_dev = dev;
-    }
-    dim3 blk(32, 8), grd((t.rw + kTileX - 1) / kTileX, (t.rh + kTileY - 1) / kTileY);
-    k_near_dense<<<grd, blk, kDenseSmem, st>>>(t, sorted, start, pix, site, far, sc);
-    if (t.npts > 0) {
-        const int n1x = t.bg.nbx >> 3, n1y = t.bg.nby >> 3;
-        k_block_rows<<<(n1y + 127) / 128, 128, 0, st>>>(t.bg, bmask, rownear);
-        k_block_near<<<(int)(((int64_t)n1x * n1y + 255) / 256), 256, 0, st>>>(t.bg, rownear, near);
-        k_near_far<<<sms * 6, 256, 0, st>>>(t, sorted, start, bmask, smask, near, far, pix, site, sc);
-    }
-}
-
-static void launch_final(const TileParams& t, const int2* pix, Scalars* sc, const unsigned long long* S,
-                         const int* Sc, float* h, cudaStream_t st) {
-    dim3 blk(32, 16), grd((t.ncols + 31) / 32, (t.nrows + 15) / 16);
-    switch (t.rs) {
-        case 1: k_final<1><<<grd, blk, 0, st>>>(t, pix, sc, S, Sc, h); break;
-        case 2: k_final<2><<<grd, blk, 0, st>>>(t, pix, sc, S, Sc, h); break;
-        case 4: k_final<4><<<grd, blk, 0, st>>>(t, pix, sc, S, Sc, h); break;
-        case 5: k_final<5><<<grd, blk, 0, st>>>(t, pix, sc, S, Sc, h); break;
-        case 6: k_final<6><<<grd, blk, 0, st>>>(t, pix, sc, S, Sc, h); break;
-        default: k_final<3><<<grd, blk, 0, st>>>(t, pix, sc, S, Sc, h); break;
-    }
-}
-
-// The plain per-work-package pipeline on device buffers.
-dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32_t* d_xyz, const uint32_t* d_gid,
-                            int64_t n, float* d_h, uint32_t* d_site, cudaStream_t st, dnni_stats* stats) {
+// The plain per-work-package call: a batch of one.  The bin grid is planned
+// from the points' bounding box, which costs one synchronisation.
+static dnni_status run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32_t* d_xyz, const uint32_t* d_gid,
+                              int64_t n, float* d_h, uint32_t* d_site, cudaStream_t st, dnni_stats* stats) {
     TileParams t;
-    dnni_status rs = dnni_tile_geometry(c, wp, n, t);
-    if (rs) return rs;
+    const char* msg = "";
+    dnni_status rs = plan_geometry(wp, n, c->s.small_radius, t, &msg);
+    if (rs) return set_err(c, rs, msg);
     if (!d_h) return set_err(c, DNNI_E_INVAL, "output grid pointer is NULL");
     if (n > 0 && !d_xyz) return set_err(c, DNNI_E_INVAL, "point pointer is NULL");
     t.has_gid = d_gid ? 1 : 0;
-    const int64_t npix = (int64_t)t.rw * t.rh;
-    const int64_t cells = (int64_t)t.ncols * t.nrows;
     const bool timing = stats || (c->s.flags & DNNI_F_TIMING);
-
-    if ((rs = dnni_ensure(c, c->pix, sizeof(int2) * npix))) return rs;
-    if ((rs = dnni_ensure(c, c->D, sizeof(unsigned long long) * cells))) return rs;
-    if ((rs = dnni_ensure(c, c->Dc, sizeof(int) * cells))) return rs;
-    if (n > 0) {
-        if ((rs = dnni_ensure(c, c->rank, sizeof(int) * n))) return rs;
-        if ((rs = dnni_ensure(c, c->sorted, sizeof(int4) * n))) return rs;
-    }
-    Scalars* sc = c->d_sc;
+    // provisional plan (geometry only) for the bounding-box pass
+    int32_t bb[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN};
+    plan_bins(bb, 0, c->s.bin_target, t);
+    HostBatch hb;
+    hb.rs = c->s.small_radius;
+    batch_add(hb, t, 0, 0, d_site ? 0 : -1);
+    DevArrays a;
+    if ((rs = ensure_scratch(c, c->scr, scratch_sizes(hb), a))) return rs;
+    BatchTables bt = device_tables(a.tables, 1);
+    if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
     if (timing) CK(cudaEventRecord(c->ev[0], st));
-    k_init_scalars<<<1, 32, 0, st>>>(sc);
+    launch_prologue(hb, bt, a, d_xyz, st);
+    CK(cudaGetLastError());
     if (n > 0) {
-        k_bbox<<<grid_for(n, 256, c->sm_count * 8), 256, 0, st>>>(d_xyz, n, t.ox, t.oy, sc);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(c->h_sc, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(c->h_sc, a.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (c->h_sc->err & kErrRange)
             return set_err(c, DNNI_E_RANGE, "a point lies beyond +-2^30 LAS units of the work-package origin");
+        plan_bins(c->h_sc->bbox, n, c->s.bin_target, t);
+        hb = HostBatch();
+        hb.rs = c->s.small_radius;
+        batch_add(hb, t, 0, 0, d_site ? 0 : -1);
+        if ((rs = ensure_scratch(c, c->scr, scratch_sizes(hb), a))) return rs;
+        bt = device_tables(a.tables, 1);
+        if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
     }
-    dnni_bin_grid(c, c->h_sc->bbox, n, t);
-    if (n > 0) {
-        const int64_t m = t.bg.nbins + 1;
-        const int nb = (int)((m + kScanTile - 1) / kScanTile);
-        if ((rs = dnni_ensure(c, c->cnt, sizeof(int) * m))) return rs;
-        if ((rs = dnni_ensure(c, c->start, sizeof(int) * m))) return rs;
-        if ((rs = dnni_ensure(c, c->bsum, sizeof(int) * nb))) return rs;
-        int* cnt = (int*)c->cnt.p;
-        int* start = (int*)c->start.p;
-        int* bsum = (int*)c->bsum.p;
-        CK(cudaMemsetAsync(cnt, 0, sizeof(int) * m, st));
-        const int g = grid_for(n, 256, c->sm_count * 16);
-        k_bin_count<<<g, 256, 0, st>>>(d_xyz, n, t.ox, t.oy, t.bg, cnt, (int*)c->rank.p);
-        k_scan_partial<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum);
-        k_scan_bsum<<<1, 1024, 0, st>>>(bsum, nb);
-        k_scan_final<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum, start);
-        k_bin_scatter<<<g, 256, 0, st>>>(d_xyz, d_gid, n, t.ox, t.oy, t.bg, start, (int*)c->rank.p,
-                                         (int4*)c->sorted.p);
-        const int64_t nblk = t.bg.nbins / kBinsPerBlock, nsup = t.bg.nbins / kBinsPerSuper;
-        if ((rs = dnni_ensure(c, c->bmask, sizeof(uint64_t) * nblk))) return rs;
-        if ((rs = dnni_ensure(c, c->smask, sizeof(uint64_t) * nsup))) return rs;
-        k_block_masks<<<(int)((nblk * 32 + 255) / 256), 256, 0, st>>>(start, nblk, (uint64_t*)c->bmask.p);
-        k_super_masks<<<(int)((nsup * 32 + 255) / 256), 256, 0, st>>>((const uint64_t*)c->bmask.p, nsup,
-                                                                      (uint64_t*)c->smask.p);
-        CK(cudaGetLastError());
-    }
-    if (timing) CK(cudaEventRecord(c->ev[1], st));
-    {
-        if ((rs = dnni_ensure(c, c->far, sizeof(int2) * far_slots(t)))) return rs;
-        const int64_t nblk = n > 0 ? t.bg.nbins / kBinsPerBlock : 1;
-        if ((rs = dnni_ensure(c, c->rownear, sizeof(int) * nblk))) return rs;
-        if ((rs = dnni_ensure(c, c->near, sizeof(int64_t) * nblk))) return rs;
-        launch_nearest(t, (const int4*)c->sorted.p, (const int*)c->start.p, (const uint64_t*)c->bmask.p,
-                       (const uint64_t*)c->smask.p, (int*)c->rownear.p, (int64_t*)c->near.p, (int2*)c->pix.p, d_site,
-                       (int2*)c->far.p, sc, c->sm_count, st);
-        k_decide<<<1, 32, 0, st>>>(sc, npix);
-        CK(cudaGetLastError());
-    }
-    if (timing) CK(cudaEventRecord(c->ev[2], st));
-    {
-        CK(cudaMemsetAsync(c->D.p, 0, sizeof(unsigned long long) * cells, st));
-        CK(cudaMemsetAsync(c->Dc.p, 0, sizeof(int) * cells, st));
-        dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        k_scatter_spans<<<grd, blk, 0, st>>>(t, (const int2*)c->pix.p, sc, (unsigned long long*)c->D.p, (int*)c->Dc.p);
-        CK(cudaGetLastError());
-    }
-    if (timing) CK(cudaEventRecord(c->ev[3], st));
-    {
-        k_rowscan<unsigned long long><<<t.nrows, kScanThreads, 0, st>>>((unsigned long long*)c->D.p, t.ncols, sc, 0);
-        k_rowscan<int><<<t.nrows, kScanThreads, 0, st>>>((int*)c->Dc.p, t.ncols, sc, 1);
-        launch_final(t, (const int2*)c->pix.p, sc, (const unsigned long long*)c->D.p, (const int*)c->Dc.p, d_h, st);
-        CK(cudaGetLastError());
-    }
+    launch_body(hb, bt, a, d_xyz, d_gid, d_h, d_site, c->sm_count, st, timing ? &c->ev[1] : nullptr);
+    CK(cudaGetLastError());
     if (timing) CK(cudaEventRecord(c->ev[4], st));
     c->calls++;
     if (timing) {
@@ -247,25 +323,14 @@ dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32
         }
     }
     if (stats) {
-        CK(cudaMemcpyAsync(c->h_sc, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(c->h_sc, a.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(c->h_ctr, a.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        const Scalars& h = *c->h_sc;
+        if (c->h_ctr->err & kErrRange) return set_err(c, DNNI_E_RANGE, "a point lies outside the search-bin grid");
         stats->n_points = n;
-        stats->n_cells = cells;
-        stats->n_pixels = npix;
-        int64_t big = 0, sp = 0, nod = 0;
-        int mx = -1;
-        for (int k = 0; k < kStatSlots; ++k) {
-            big += (int64_t)h.big_pixels[k];
-            sp += (int64_t)h.spans[k];
-            nod += (int64_t)h.nodata[k];
-            mx = std::max(mx, h.max_r2[k]);
-        }
-        stats->big_pixels = big;
-        stats->spans = sp;
-        stats->nodata_cells = nod;
-        stats->max_r2 = mx;
-        stats->packed = h.packed;
+        stats->n_cells = (int64_t)t.ncols * t.nrows;
+        stats->n_pixels = (int64_t)t.rw * t.rh;
+        fold_stats(c->h_sc, 1, stats);
         stats->bin_size = t.bg.bs;
     }
     return DNNI_OK;
@@ -303,12 +368,14 @@ dnni_status dnni_init(const dnni_settings* settings, dnni_ctx** out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return DNNI_E_CUDA; }
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) { dnni_destroy(c); return DNNI_E_CUDA; }
-    if (cudaMalloc(&c->d_sc, sizeof(Scalars)) != cudaSuccess ||
-        cudaMallocHost(&c->h_sc, sizeof(Scalars)) != cudaSuccess) {
+    if (cudaMallocHost(&c->h_sc, sizeof(Scalars)) != cudaSuccess ||
+        cudaMallocHost(&c->h_ctr, sizeof(BatchCounters)) != cudaSuccess) {
         dnni_destroy(c);
         return DNNI_E_NOMEM;
     }
     memset(c->h_sc, 0, sizeof(Scalars));
+    memset(c->h_ctr, 0, sizeof(BatchCounters));
+    set_dense_smem_attr();
     *out = c;
     return DNNI_OK;
 }
@@ -319,8 +386,9 @@ dnni_status dnni_destroy(dnni_ctx* c) {
         DeviceGuard g(c->device);
         if (c->stream) cudaStreamSynchronize(c->stream);
         dnni_free_all(c);
-        if (c->d_sc) cudaFree(c->d_sc);
         if (c->h_sc) cudaFreeHost(c->h_sc);
+        if (c->h_ctr) cudaFreeHost(c->h_ctr);
+        if (c->h_tables) cudaFreeHost(c->h_tables);
         for (auto& e : c->ev)
             if (e) cudaEventDestroy(e);
         if (c->stream) cudaStreamDestroy(c->stream);
@@ -336,24 +404,16 @@ dnni_status dnni_setup_run(dnni_ctx* c, const dnni_workpackage* wp, int64_t max_
     c->err.clear();
     DeviceGuard g(c->device);
     TileParams t;
-    dnni_status rs = dnni_tile_geometry(c, wp, max_points, t);
-    if (rs) return rs;
-    const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
-    if ((rs = dnni_ensure(c, c->pix, sizeof(int2) * npix))) return rs;
-    if ((rs = dnni_ensure(c, c->D, sizeof(unsigned long long) * cells))) return rs;
-    if ((rs = dnni_ensure(c, c->Dc, sizeof(int) * cells))) return rs;
-    if (max_points > 0) {
-        if ((rs = dnni_ensure(c, c->rank, sizeof(int) * max_points))) return rs;
-        if ((rs = dnni_ensure(c, c->sorted, sizeof(int4) * max_points))) return rs;
-        // bins are sized from the points; reserve for the densest grid allowed
-        int32_t bb[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, 0, 0};
-        dnni_bin_grid(c, bb, max_points, t);
-        const int64_t m = t.bg.nbins + 1;
-        if ((rs = dnni_ensure(c, c->cnt, sizeof(int) * m))) return rs;
-        if ((rs = dnni_ensure(c, c->start, sizeof(int) * m))) return rs;
-        if ((rs = dnni_ensure(c, c->bsum, sizeof(int) * ((m + kScanTile - 1) / kScanTile)))) return rs;
-    }
-    return DNNI_OK;
+    const char* msg = "";
+    dnni_status rs = plan_geometry(wp, max_points, c->s.small_radius, t, &msg);
+    if (rs) return set_err(c, rs, msg);
+    // bins are sized from the points; reserve for the densest grid allowed
+    int32_t bb[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, 0, 0};
+    plan_bins(bb, max_points, c->s.bin_target, t);
+    HostBatch hb;
+    batch_add(hb, t, 0, 0, 0);
+    DevArrays a;
+    return ensure_scratch(c, c->scr, scratch_sizes(hb), a);
 }
 
 dnni_status dnni_interpolate_segment_device(dnni_ctx* c, const dnni_workpackage* wp, const int32_t* d_xyz,
@@ -364,7 +424,7 @@ dnni_status dnni_interpolate_segment_device(dnni_ctx* c, const dnni_workpackage*
     DeviceGuard g(c->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     if (stats) memset(stats, 0, sizeof(*stats));
-    return dnni_run_device(c, wp, d_xyz, d_gid, n, d_h, d_site, st, stats);
+    return run_device(c, wp, d_xyz, d_gid, n, d_h, d_site, st, stats);
 }
 
 dnni_status dnni_interpolate_segment(dnni_ctx* c, const dnni_workpackage* wp, const int32_t* xyz, const uint32_t* gid,
@@ -375,8 +435,9 @@ dnni_status dnni_interpolate_segment(dnni_ctx* c, const dnni_workpackage* wp, co
     if (n > 0 && !xyz) return set_err(c, DNNI_E_INVAL, "point pointer is NULL");
     DeviceGuard g(c->device);
     TileParams t;
-    dnni_status rs = dnni_tile_geometry(c, wp, n, t);
-    if (rs) return rs;
+    const char* msg = "";
+    dnni_status rs = plan_geometry(wp, n, c->s.small_radius, t, &msg);
+    if (rs) return set_err(c, rs, msg);
     const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
     cudaStream_t st = c->stream;
     if (stats) memset(stats, 0, sizeof(*stats));
@@ -390,8 +451,8 @@ dnni_status dnni_interpolate_segment(dnni_ctx* c, const dnni_workpackage* wp, co
     }
     if ((rs = dnni_ensure(c, c->out_h, sizeof(float) * cells))) return rs;
     if (out_site && (rs = dnni_ensure(c, c->out_site, sizeof(uint32_t) * npix))) return rs;
-    rs = dnni_run_device(c, wp, (const int32_t*)c->in_xyz.p, gid ? (const uint32_t*)c->in_gid.p : nullptr, n,
-                         (float*)c->out_h.p, out_site ? (uint32_t*)c->out_site.p : nullptr, st, stats);
+    rs = run_device(c, wp, (const int32_t*)c->in_xyz.p, gid ? (const uint32_t*)c->in_gid.p : nullptr, n,
+                    (float*)c->out_h.p, out_site ? (uint32_t*)c->out_site.p : nullptr, st, stats);
     if (rs) return rs;
     CK(cudaMemcpyAsync(out_h, c->out_h.p, sizeof(float) * cells, cudaMemcpyDeviceToHost, st));
     if (out_site) CK(cudaMemcpyAsync(out_site, c->out_site.p, sizeof(uint32_t) * npix, cudaMemcpyDeviceToHost, st));
@@ -436,12 +497,191 @@ dnni_status dnni_host_free(void* p) {
     return DNNI_OK;
 }
 
+// ---- batches ---------------------------------------------------------------
+
+dnni_status dnni_batch_create(dnni_ctx* c, const dnni_tile* tiles, int32_t ntiles, const dnni_batch_options* opt,
+                              dnni_batch** out) {
+    if (!c || !out || !tiles || ntiles <= 0) return DNNI_E_INVAL;
+    *out = nullptr;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    dnni_batch_options o{};
+    if (opt) o = *opt;
+    const int rs_ = o.small_radius ? o.small_radius : c->s.small_radius;
+    const int bt_ = o.bin_target ? o.bin_target : c->s.bin_target;
+    if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0) return set_err(c, DNNI_E_INVAL, "bad batch options");
+    // plan every tile from its geometry and declared point extent
+    std::vector<TileParams> plan(ntiles);
+    std::vector<int64_t> cost(ntiles);
+    for (int k = 0; k < ntiles; ++k) {
+        const dnni_tile& d = tiles[k];
+        const char* msg = "";
+        dnni_status rs = plan_geometry(&d.wp, d.pt_count, rs_, plan[k], &msg);
+        if (rs) return set_err(c, rs, std::string("tile ") + std::to_string(k) + ": " + msg);
+        if (d.pt_offset < 0 || d.pt_count < 0 || d.out_offset < 0)
+            return set_err(c, DNNI_E_INVAL, "negative tile offset");
+        int32_t bb[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, 0, 0};
+        if (d.ext_x0 || d.ext_y0 || d.ext_x1 || d.ext_y1) {
+            const long long ex0 = (long long)d.ext_x0 - d.wp.origin_x, ex1 = (long long)d.ext_x1 - d.wp.origin_x;
+            const long long ey0 = (long long)d.ext_y0 - d.wp.origin_y, ey1 = (long long)d.ext_y1 - d.wp.origin_y;
+            if (ex1 < ex0 || ey1 < ey0) return set_err(c, DNNI_E_INVAL, "empty point extent");
+            if (ex0 <= -kCoordLimit || ex1 >= kCoordLimit || ey0 <= -kCoordLimit || ey1 >= kCoordLimit)
+                return set_err(c, DNNI_E_RANGE, "point extent beyond +-2^30 LAS units of the origin");
+            bb[0] = (int32_t)ex0;
+            bb[1] = (int32_t)ex1;
+            bb[2] = (int32_t)ey0;
+            bb[3] = (int32_t)ey1;
+        }
+        plan_bins(bb, d.pt_count, bt_, plan[k]);
+        if (bb[0] <= bb[1]) {
+            plan[k].has_ext = 1;
+            plan[k].ex0 = bb[0];
+            plan[k].ex1 = bb[1];
+            plan[k].ey0 = bb[2];
+            plan[k].ey1 = bb[3];
+        }
+        cost[k] = (int64_t)plan[k].rw * plan[k].rh + d.pt_count;
+    }
+    dnni_batch* b = new dnni_batch();
+    b->ctx = c;
+    b->use_graph = o.use_graph;
+    b->order.resize(ntiles);
+    std::iota(b->order.begin(), b->order.end(), 0);
+    if (o.order_by_cost)
+        std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    b->hb.rs = rs_;
+    for (int k : b->order) batch_add(b->hb, plan[k], tiles[k].pt_offset, tiles[k].out_offset, tiles[k].site_offset);
+    dnni_status rs = ensure_scratch(c, b->scr, scratch_sizes(b->hb), b->arr);
+    if (!rs) {
+        b->bt = device_tables(b->arr.tables, ntiles);
+        rs = stage_tables(c, b->hb, b->arr.tables, c->stream);
+        if (!rs && cudaStreamSynchronize(c->stream) != cudaSuccess) rs = cuda_err(c, cudaGetLastError(), "upload");
+    }
+    if (rs) {
+        release_scratch(c, b->scr);
+        delete b;
+        return rs;
+    }
+    b->h_sc.resize(ntiles);
+    *out = b;
+    return DNNI_OK;
+}
+
+dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uint32_t* d_gid, float* d_h,
+                                  uint32_t* d_site, void* stream, dnni_stats* stats) {
+    if (!b) return DNNI_E_INVAL;
+    dnni_ctx* c = b->ctx;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    if (!d_h || (b->hb.n_rows > 0 && !d_xyz)) return set_err(c, DNNI_E_INVAL, "NULL buffer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (stats) CK(cudaEventRecord(c->ev[0], st));
+    if (b->use_graph) {
+        const void* key[4] = {d_xyz, d_gid, d_h, d_site};
+        if (!b->exec || memcmp(key, b->graph_key, sizeof(key)) != 0) {
+            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+            if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+            cudaStream_t cap;
+            CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                launch_prologue(b->hb, b->bt, b->arr, d_xyz, cap);
+                launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, cap, nullptr);
+                e = cudaStreamEndCapture(cap, &b->graph);
+            }
+            cudaStreamDestroy(cap);
+            if (e != cudaSuccess) return cuda_err(c, e, "graph capture");
+            CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+            memcpy(b->graph_key, key, sizeof(key));
+        }
+        CK(cudaGraphLaunch(b->exec, st));
+    } else {
+        launch_prologue(b->hb, b->bt, b->arr, d_xyz, st);
+        launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, st, nullptr);
+        CK(cudaGetLastError());
+    }
+    if (stats) {
+        CK(cudaEventRecord(c->ev[1], st));
+        const int n = (int)b->hb.tiles.size();
+        CK(cudaMemcpyAsync(b->h_sc.data(), b->arr.sc, sizeof(Scalars) * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(c->h_ctr, b->arr.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+        stats->ms_total = ms;
+        if (c->h_ctr->err & kErrRange)
+            return set_err(c, DNNI_E_RANGE, "a point lies beyond its tile's declared extent or the coordinate range");
+        fold_stats(b->h_sc.data(), n, stats);
+        for (const TileParams& t : b->hb.tiles) stats->n_points += t.npts;
+        stats->n_cells = b->hb.n_cells;
+        stats->n_pixels = b->hb.n_pix;
+    }
+    return DNNI_OK;
+}
+
+dnni_status dnni_batch_run(dnni_batch* b, const int32_t* xyz, const uint32_t* gid, int64_t n_rows, float* out_h,
+                           uint32_t* out_site, dnni_stats* stats) {
+    if (!b) return DNNI_E_INVAL;
+    dnni_ctx* c = b->ctx;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    if (n_rows < b->hb.n_rows) return set_err(c, DNNI_E_INVAL, "fewer point rows than the tiles reference");
+    if (!out_h || (n_rows > 0 && !xyz)) return set_err(c, DNNI_E_INVAL, "NULL buffer");
+    cudaStream_t st = c->stream;
+    dnni_status rs;
+    if (n_rows > 0) {
+        if ((rs = dnni_ensure(c, b->in_xyz, sizeof(int32_t) * 3 * n_rows))) return rs;
+        CK(cudaMemcpyAsync(b->in_xyz.p, xyz, sizeof(int32_t) * 3 * n_rows, cudaMemcpyHostToDevice, st));
+        if (gid) {
+            if ((rs = dnni_ensure(c, b->in_gid, sizeof(uint32_t) * n_rows))) return rs;
+            CK(cudaMemcpyAsync(b->in_gid.p, gid, sizeof(uint32_t) * n_rows, cudaMemcpyHostToDevice, st));
+        }
+    }
+    const int64_t nh = std::max<int64_t>(b->hb.out_end, 1), ns = std::max<int64_t>(b->hb.site_end, 1);
+    if ((rs = dnni_ensure(c, b->out_h, sizeof(float) * nh))) return rs;
+    if (out_site && (rs = dnni_ensure(c, b->out_site, sizeof(uint32_t) * ns))) return rs;
+    rs = dnni_batch_run_device(b, (const int32_t*)b->in_xyz.p, gid ? (const uint32_t*)b->in_gid.p : nullptr,
+                               (float*)b->out_h.p, out_site ? (uint32_t*)b->out_site.p : nullptr, st, stats);
+    if (rs) return rs;
+    CK(cudaMemcpyAsync(out_h, b->out_h.p, sizeof(float) * b->hb.out_end, cudaMemcpyDeviceToHost, st));
+    if (out_site && b->hb.site_end > 0)
+        CK(cudaMemcpyAsync(out_site, b->out_site.p, sizeof(uint32_t) * b->hb.site_end, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->h_ctr, b->arr.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (c->h_ctr->err & kErrRange)
+        return set_err(c, DNNI_E_RANGE, "a point lies beyond its tile's declared extent or the coordinate range");
+    if (stats) {
+        stats->h2d_bytes = (int64_t)(sizeof(int32_t) * 3 * n_rows + (gid ? sizeof(uint32_t) * n_rows : 0));
+        stats->d2h_bytes =
+            (int64_t)(sizeof(float) * b->hb.out_end + (out_site ? sizeof(uint32_t) * b->hb.site_end : 0));
+    }
+    return DNNI_OK;
+}
+
+dnni_status dnni_batch_destroy(dnni_batch* b) {
+    if (!b) return DNNI_E_INVAL;
+    dnni_ctx* c = b->ctx;
+    {
+        DeviceGuard g(c->device);
+        cudaDeviceSynchronize();
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        if (b->graph) cudaGraphDestroy(b->graph);
+        release_scratch(c, b->scr);
+        dnni_release(b->in_xyz, c);
+        dnni_release(b->in_gid, c);
+        dnni_release(b->out_h, c);
+        dnni_release(b->out_site, c);
+    }
+    delete b;
+    return DNNI_OK;
+}
+
 }  // extern "C"
 
 void dnni_free_all(dnni_ctx* c) {
-    DevBuf* bufs[] = {&c->rank, &c->sorted, &c->cnt, &c->start, &c->bsum, &c->pix, &c->D, &c->Dc,
-                      &c->bmask, &c->smask, &c->far, &c->rownear, &c->near,
-                      &c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
+    release_scratch(c, c->scr);
+    DevBuf* bufs[] = {&c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
 
@@ -489,15 +729,33 @@ dnni_status noalloc_base(int dev, unsigned char** out) {
     return DNNI_OK;
 }
 
-struct ArenaCursor {
+// Carves one work package's scratch out of the array; false when it does
+// not fit.
+bool carve_noalloc(unsigned char* base, const ScratchSizes& z, DevArrays& a) {
     size_t off = 0;
-    size_t take(size_t bytes) {
-        const size_t o = off;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base + off;
         off = (off + bytes + 255) & ~(size_t)255;
-        return o;
-    }
-    bool fits() const { return off <= kNoAllocScratchBytes; }
-};
+        return p;
+    };
+    a.tables = take(z.tables);
+    a.sc = (Scalars*)take(z.sc);
+    a.ctr = (BatchCounters*)take(z.ctr);
+    a.pix = (int2*)take(z.pix);
+    a.far = (FarSlot*)take(z.far);
+    a.D = (unsigned long long*)take(z.D);
+    a.Dc = (int*)take(z.Dc);
+    a.sorted = (int4*)take(z.sorted);
+    a.rank = (int*)take(z.rank);
+    a.cnt = (int*)take(z.cnt);
+    a.start = (int*)take(z.cnt);
+    a.bsum = (int*)take(z.bsum);
+    a.bmask = (uint64_t*)take(z.bmask);
+    a.smask = (uint64_t*)take(z.smask);
+    a.rownear = (int*)take(z.rownear);
+    a.near = (int64_t*)take(z.near);
+    return off <= kNoAllocScratchBytes;
+}
 
 }  // namespace
 
@@ -518,81 +776,47 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     if (rs) return rs;
     if (!d_h || (n > 0 && !d_xyz)) return DNNI_E_INVAL;
     t.has_gid = d_gid ? 1 : 0;
-    const int64_t npix = (int64_t)t.rw * t.rh, cells = (int64_t)t.ncols * t.nrows;
-    ArenaCursor a;
-    const size_t o_sc = a.take(sizeof(Scalars));
-    const size_t o_pix = a.take(sizeof(int2) * npix);
-    const size_t o_D = a.take(sizeof(unsigned long long) * cells);
-    const size_t o_Dc = a.take(sizeof(int) * cells);
-    const size_t o_rank = n > 0 ? a.take(sizeof(int) * n) : 0;
-    const size_t o_sorted = n > 0 ? a.take(sizeof(int4) * n) : 0;
-    const size_t o_far = a.take(sizeof(int2) * far_slots(t));
-    if (!a.fits()) return DNNI_E_SCRATCH;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    set_dense_smem_attr();
     cudaStream_t st = (cudaStream_t)stream;
-    Scalars* sc = (Scalars*)(base + o_sc);
-    int2* pix = (int2*)(base + o_pix);
-    unsigned long long* D = (unsigned long long*)(base + o_D);
-    int* Dc = (int*)(base + o_Dc);
-    int* rank = (int*)(base + o_rank);
-    int4* sorted = (int4*)(base + o_sorted);
-    // the array keeps the previous call's contents: every region that must
-    // start at zero (scalars, bin counts, span words) is cleared below
-    k_init_scalars<<<1, 32, 0, st>>>(sc);
-    Scalars hsc;
-    memset(&hsc, 0, sizeof(hsc));
+    // provisional one-tile plan for the bounding-box pass
+    int32_t bb[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, INT_MAX, INT_MIN};
+    plan_bins(bb, 0, 0.0, t);
+    HostBatch hb;
+    batch_add(hb, t, 0, 0, d_site ? 0 : -1);
+    DevArrays a;
+    if (!carve_noalloc(base, scratch_sizes(hb), a)) return DNNI_E_SCRATCH;
+    // the one-tile tables go up from pageable host memory: the copy has
+    // taken the bytes when cudaMemcpyAsync returns, so the buffer can be
+    // repacked at once
+    std::vector<unsigned char> tbl(TableLayout(1).total);
+    pack_tables(hb, tbl.data());
+    if (cudaMemcpyAsync(a.tables, tbl.data(), tbl.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return DNNI_E_CUDA;
+    BatchTables bt = device_tables(a.tables, 1);
+    // the array keeps the previous call's contents: the scalars, bin counts
+    // and span words are cleared by the launch sequence itself
+    launch_prologue(hb, bt, a, d_xyz, st);
     if (n > 0) {
-        k_bbox<<<grid_for(n, 256, sms * 8), 256, 0, st>>>(d_xyz, n, t.ox, t.oy, sc);
-        if (cudaMemcpyAsync(&hsc, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        Scalars hsc;
+        if (cudaMemcpyAsync(&hsc, a.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) {
             cudaGetLastError();
             return DNNI_E_CUDA;
         }
         if (hsc.err & kErrRange) return DNNI_E_RANGE;
-    }
-    plan_bins(hsc.bbox, n, 0.0, t);
-    int* start = nullptr;
-    uint64_t* bmask = nullptr;
-    uint64_t* smask = nullptr;
-    int* rownear = nullptr;
-    int64_t* nearb = nullptr;
-    if (n > 0) {
-        const int64_t m = t.bg.nbins + 1;
-        const int nb = (int)((m + kScanTile - 1) / kScanTile);
-        int* cnt = (int*)(base + a.take(sizeof(int) * m));
-        start = (int*)(base + a.take(sizeof(int) * m));
-        int* bsum = (int*)(base + a.take(sizeof(int) * nb));
-        if (!a.fits()) return DNNI_E_SCRATCH;
-        if (cudaMemsetAsync(cnt, 0, sizeof(int) * m, st) != cudaSuccess) return DNNI_E_CUDA;
-        const int g = grid_for(n, 256, sms * 16);
-        k_bin_count<<<g, 256, 0, st>>>(d_xyz, n, t.ox, t.oy, t.bg, cnt, rank);
-        k_scan_partial<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum);
-        k_scan_bsum<<<1, 1024, 0, st>>>(bsum, nb);
-        k_scan_final<<<nb, kScanThreads, 0, st>>>(cnt, m, bsum, start);
-        k_bin_scatter<<<g, 256, 0, st>>>(d_xyz, d_gid, n, t.ox, t.oy, t.bg, start, rank, sorted);
-        const int64_t nblk = t.bg.nbins / kBinsPerBlock, nsup = t.bg.nbins / kBinsPerSuper;
-        bmask = (uint64_t*)(base + a.take(sizeof(uint64_t) * nblk));
-        smask = (uint64_t*)(base + a.take(sizeof(uint64_t) * nsup));
-        if (!a.fits()) return DNNI_E_SCRATCH;
-        k_block_masks<<<(int)((nblk * 32 + 255) / 256), 256, 0, st>>>(start, nblk, bmask);
-        k_super_masks<<<(int)((nsup * 32 + 255) / 256), 256, 0, st>>>(bmask, nsup, smask);
-        rownear = (int*)(base + a.take(sizeof(int) * nblk));
-        nearb = (int64_t*)(base + a.take(sizeof(int64_t) * nblk));
-        if (!a.fits()) return DNNI_E_SCRATCH;
-    }
-    {
-        dim3 blk(32, 8), grd((t.rw + 31) / 32, (t.rh + 7) / 8);
-        launch_nearest(t, sorted, start, bmask, smask, rownear, nearb, pix, d_site, (int2*)(base + o_far), sc, sms, st);
-        k_decide<<<1, 32, 0, st>>>(sc, npix);
-        if (cudaMemsetAsync(D, 0, sizeof(unsigned long long) * cells, st) != cudaSuccess ||
-            cudaMemsetAsync(Dc, 0, sizeof(int) * cells, st) != cudaSuccess)
+        plan_bins(hsc.bbox, n, 0.0, t);
+        hb = HostBatch();
+        batch_add(hb, t, 0, 0, d_site ? 0 : -1);
+        if (!carve_noalloc(base, scratch_sizes(hb), a)) return DNNI_E_SCRATCH;
+        pack_tables(hb, tbl.data());
+        if (cudaMemcpyAsync(a.tables, tbl.data(), tbl.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
             return DNNI_E_CUDA;
-        k_scatter_spans<<<grd, blk, 0, st>>>(t, pix, sc, D, Dc);
+        bt = device_tables(a.tables, 1);
     }
-    k_rowscan<unsigned long long><<<t.nrows, kScanThreads, 0, st>>>(D, t.ncols, sc, 0);
-    k_rowscan<int><<<t.nrows, kScanThreads, 0, st>>>(Dc, t.ncols, sc, 1);
-    launch_final(t, pix, sc, D, Dc, d_h, st);
+    launch_body(hb, bt, a, d_xyz, d_gid, d_h, d_site, sms, st, nullptr);
     if (cudaGetLastError() != cudaSuccess) return DNNI_E_CUDA;
     return DNNI_OK;
 }

@@ -1,4 +1,5 @@
-// dnni_internal.h -- context layout shared by the engine's translation units.
+// dnni_internal.h -- context and batch layout shared by the engine's
+// translation units.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -7,13 +8,40 @@
 #include <climits>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/dnni.h"
 #include "dnni_kernels.cuh"
+#include "dnni_plan.h"
 
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
+};
+
+// Device scratch of one batch (or of the context's single work packages).
+struct Scratch {
+    DevBuf sorted, rank, cnt, start, bsum, bmask, smask, rownear, near, pix, far, D, Dc, sc, ctr, tables;
+};
+
+// Raw device pointers of a scratch set for one launch sequence.
+struct DevArrays {
+    int4* sorted = nullptr;
+    int* rank = nullptr;
+    int* cnt = nullptr;
+    int* start = nullptr;
+    int* bsum = nullptr;
+    uint64_t* bmask = nullptr;
+    uint64_t* smask = nullptr;
+    int* rownear = nullptr;
+    int64_t* near = nullptr;
+    int2* pix = nullptr;
+    dnni::FarSlot* far = nullptr;
+    unsigned long long* D = nullptr;
+    int* Dc = nullptr;
+    dnni::Scalars* sc = nullptr;
+    dnni::BatchCounters* ctr = nullptr;
+    unsigned char* tables = nullptr;
 };
 
 struct dnni_ctx {
@@ -21,12 +49,12 @@ struct dnni_ctx {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     dnni_settings s{};
-    // per-work-package scratch (grow-only until dnni_clear)
-    DevBuf rank, sorted, cnt, start, bsum, pix, D, Dc, bmask, smask, far, rownear, near;
-    // staging for the host-buffer entry point
-    DevBuf in_xyz, in_gid, out_h, out_site;
-    dnni::Scalars* d_sc = nullptr;
-    dnni::Scalars* h_sc = nullptr;   // pinned mirror
+    Scratch scr;                     // single work packages (grow-only until dnni_clear)
+    DevBuf in_xyz, in_gid, out_h, out_site;   // staging for the host-buffer entry point
+    unsigned char* h_tables = nullptr;        // pinned staging of the tile tables
+    size_t h_tables_cap = 0;
+    dnni::Scalars* h_sc = nullptr;            // pinned mirror of one tile's scalars
+    dnni::BatchCounters* h_ctr = nullptr;
     cudaEvent_t ev[6] = {};
     std::string err;
     size_t held = 0;
@@ -34,10 +62,22 @@ struct dnni_ctx {
     int64_t calls = 0;
 };
 
+struct dnni_batch {
+    dnni_ctx* ctx = nullptr;
+    dnni::HostBatch hb;
+    Scratch scr;
+    DevArrays arr;
+    dnni::BatchTables bt{};
+    std::vector<int> order;          // batch position -> caller's tile index
+    int use_graph = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void* graph_key[4] = {};   // pointers the captured graph was built for
+    cudaStream_t graph_stream = nullptr;
+    DevBuf in_xyz, in_gid, out_h, out_site;
+    std::vector<dnni::Scalars> h_sc;
+};
+
 dnni_status dnni_ensure(dnni_ctx* c, DevBuf& b, size_t bytes);
 void dnni_release(DevBuf& b, dnni_ctx* c);
 void dnni_free_all(dnni_ctx* c);
-dnni_status dnni_tile_geometry(dnni_ctx* c, const dnni_workpackage* wp, int64_t n, dnni::TileParams& t);
-void dnni_bin_grid(const dnni_ctx* c, const int32_t bbox[6], int64_t n, dnni::TileParams& t);
-dnni_status dnni_run_device(dnni_ctx* c, const dnni_workpackage* wp, const int32_t* d_xyz, const uint32_t* d_gid,
-                            int64_t n, float* d_h, uint32_t* d_site, cudaStream_t st, dnni_stats* stats);

@@ -9,7 +9,7 @@
 #include <cstring>
 
 #include "../../include/dnni.h"
-#include "dnni_kernels.cuh"
+#include "dnni_search.cuh"
 
 namespace dnni {
 
@@ -101,6 +101,118 @@ inline void plan_bins(const int32_t bbox[6], int64_t n, double bin_target, TileP
     t.bg.n2x = (int32_t)(nbx / kBinsPerSuperEdge);
     t.bg.n2y = (int32_t)(nby / kBinsPerSuperEdge);
     t.bg.nbins = nbx * nby;
+}
+
+}  // namespace dnni
+
+#include <vector>
+
+#include "dnni_kernels.cuh"
+
+namespace dnni {
+
+// Host-side plan of a batch: every tile's geometry, bin grid and offsets,
+// plus the prefix arrays that map launch indices to tiles.
+struct HostBatch {
+    std::vector<TileParams> tiles;
+    std::vector<int> chunk_base{0}, scan_base{0}, row1_base{0}, rt_base{0}, ct_base{0}, grow_base{0};
+    std::vector<int64_t> blk_base{0}, sup_base{0};
+    int64_t n_rows = 0;                  // input point rows the tiles reference
+    int64_t n_pts = 0, n_bins = 0, n_pix = 0, n_cells = 0, n_far = 0;
+    int64_t out_end = 0, site_end = 0;   // extent of the caller's output arrays used
+    int64_t cost = 0;
+    int rs = 3;                          // stencil radius shared by the batch
+};
+
+// Worklist capacity of a tile: every dense warp (32 pixels of a tile row, the
+// raster padded to whole 32 x 8 tiles) may append one group of 32 slots.
+inline int64_t far_slots(const TileParams& t) {
+    return (int64_t)((t.rw + kTileX - 1) / kTileX * kTileX) * ((t.rh + kTileY - 1) / kTileY * kTileY);
+}
+
+// Appends a tile whose geometry and bin grid are set; its point range starts
+// at pt_off of the batch's point arrays and its heights at out_off of the
+// caller's output (site_off: site map offset or -1).
+inline void batch_add(HostBatch& hb, TileParams t, int64_t pt_off, int64_t out_off, int64_t site_off) {
+    t.pt_off = pt_off;
+    t.srt_off = hb.n_pts;
+    t.bin_off = hb.n_bins;
+    t.blk_off = hb.blk_base.back();
+    t.sup_off = hb.sup_base.back();
+    t.pix_off = hb.n_pix;
+    t.cell_off = hb.n_cells;
+    t.out_off = out_off;
+    t.site_off = site_off;
+    const int64_t nbins = t.bg.nbins;
+    hb.n_bins += nbins + 1;
+    hb.blk_base.push_back(t.blk_off + nbins / kBinsPerBlock);
+    hb.sup_base.push_back(t.sup_off + nbins / kBinsPerSuper);
+    hb.chunk_base.push_back(hb.chunk_base.back() + (int)((t.npts + kChunk - 1) / kChunk));
+    hb.scan_base.push_back(hb.scan_base.back() + (int)((nbins + 1 + kScanTile - 1) / kScanTile));
+    hb.row1_base.push_back(hb.row1_base.back() + (t.npts > 0 ? (t.bg.nby >> 3) : 0));
+    hb.rt_base.push_back(hb.rt_base.back() + ((t.rw + kTileX - 1) / kTileX) * ((t.rh + kTileY - 1) / kTileY));
+    hb.ct_base.push_back(hb.ct_base.back() + ((t.ncols + 31) / 32) * ((t.nrows + 15) / 16));
+    hb.grow_base.push_back(hb.grow_base.back() + t.nrows);
+    hb.n_rows = std::max<int64_t>(hb.n_rows, pt_off + t.npts);
+    hb.n_pts += t.npts;
+    hb.n_pix += (int64_t)t.rw * t.rh;
+    hb.n_cells += (int64_t)t.ncols * t.nrows;
+    hb.n_far += far_slots(t);
+    hb.out_end = std::max<int64_t>(hb.out_end, out_off + (int64_t)t.ncols * t.nrows);
+    if (site_off >= 0) hb.site_end = std::max<int64_t>(hb.site_end, site_off + (int64_t)t.rw * t.rh);
+    t.tile_id = (int32_t)hb.tiles.size();
+    hb.tiles.push_back(t);
+}
+
+// Byte layout of the device copy of a batch's tables (one upload).
+struct TableLayout {
+    size_t tiles, chunk, scan, blk, sup, row1, rt, ct, grow, total;
+    explicit TableLayout(int n) {
+        size_t o = 0;
+        auto take = [&](size_t b) { const size_t r = o; o = (o + b + 15) & ~(size_t)15; return r; };
+        tiles = take(sizeof(TileParams) * n);
+        chunk = take(sizeof(int) * (n + 1));
+        scan = take(sizeof(int) * (n + 1));
+        blk = take(sizeof(int64_t) * (n + 1));
+        sup = take(sizeof(int64_t) * (n + 1));
+        row1 = take(sizeof(int) * (n + 1));
+        rt = take(sizeof(int) * (n + 1));
+        ct = take(sizeof(int) * (n + 1));
+        grow = take(sizeof(int) * (n + 1));
+        total = o;
+    }
+};
+
+// Serialises the tables into host memory laid out as TableLayout.
+inline void pack_tables(const HostBatch& hb, unsigned char* dst) {
+    const int n = (int)hb.tiles.size();
+    const TableLayout L(n);
+    memcpy(dst + L.tiles, hb.tiles.data(), sizeof(TileParams) * n);
+    memcpy(dst + L.chunk, hb.chunk_base.data(), sizeof(int) * (n + 1));
+    memcpy(dst + L.scan, hb.scan_base.data(), sizeof(int) * (n + 1));
+    memcpy(dst + L.blk, hb.blk_base.data(), sizeof(int64_t) * (n + 1));
+    memcpy(dst + L.sup, hb.sup_base.data(), sizeof(int64_t) * (n + 1));
+    memcpy(dst + L.row1, hb.row1_base.data(), sizeof(int) * (n + 1));
+    memcpy(dst + L.rt, hb.rt_base.data(), sizeof(int) * (n + 1));
+    memcpy(dst + L.ct, hb.ct_base.data(), sizeof(int) * (n + 1));
+    memcpy(dst + L.grow, hb.grow_base.data(), sizeof(int) * (n + 1));
+}
+
+// Device view of tables uploaded to `dev` (laid out as TableLayout).
+inline BatchTables device_tables(const unsigned char* dev, int n) {
+    const TableLayout L(n);
+    BatchTables bt;
+    bt.tiles = (const TileParams*)(dev + L.tiles);
+    bt.ntiles = n;
+    bt.chunk_base = (const int*)(dev + L.chunk);
+    bt.scan_base = (const int*)(dev + L.scan);
+    bt.blk_base = (const int64_t*)(dev + L.blk);
+    bt.sup_base = (const int64_t*)(dev + L.sup);
+    bt.row1_base = (const int*)(dev + L.row1);
+    bt.rt_base = (const int*)(dev + L.rt);
+    bt.ct_base = (const int*)(dev + L.ct);
+    bt.grow_base = (const int*)(dev + L.grow);
+    return bt;
 }
 
 }  // namespace dnni

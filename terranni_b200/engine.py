@@ -64,6 +64,21 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
+class Tile(ctypes.Structure):
+    _fields_ = [
+        ("wp", WorkPackage),
+        ("pt_offset", ctypes.c_int64), ("pt_count", ctypes.c_int64),
+        ("ext_x0", ctypes.c_int32), ("ext_y0", ctypes.c_int32),
+        ("ext_x1", ctypes.c_int32), ("ext_y1", ctypes.c_int32),
+        ("out_offset", ctypes.c_int64), ("site_offset", ctypes.c_int64),
+    ]
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32),
+                ("use_graph", ctypes.c_int32), ("order_by_cost", ctypes.c_int32)]
+
+
 # every symbol include/dnni.h declares, with (argtypes, restype)
 _P = ctypes.c_void_p
 _SIGS = {
@@ -82,6 +97,11 @@ _SIGS = {
     "dnni_print_times": ([_P], ctypes.c_int),
     "dnni_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(_P)], ctypes.c_int),
     "dnni_host_free": ([_P], ctypes.c_int),
+    "dnni_batch_create": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, ctypes.POINTER(BatchOptions),
+                           ctypes.POINTER(_P)], ctypes.c_int),
+    "dnni_batch_run_device": ([_P, _P, _P, _P, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
+    "dnni_batch_run": ([_P, _P, _P, ctypes.c_int64, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
+    "dnni_batch_destroy": ([_P], ctypes.c_int),
 }
 
 _lib = None
@@ -196,8 +216,69 @@ class Engine:
             stream, ctypes.byref(st) if st is not None else None))
         return st
 
+    def batch(self, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False):
+        """Plans a batch of tiles (dnni_batch_create) -> Batch."""
+        return Batch(self, tiles, small_radius, bin_target, use_graph, order_by_cost)
+
     def clear(self):
         self._check(lib().dnni_clear(self._h))
 
     def print_times(self):
         self._check(lib().dnni_print_times(self._h))
+
+
+def make_tile(wp: WorkPackage, pt_offset, pt_count, out_offset, site_offset=-1, extent=None) -> Tile:
+    """One batch entry; extent = absolute (x0, y0, x1, y1) LAS box of its
+    points, None = the raster."""
+    t = Tile()
+    t.wp = wp
+    t.pt_offset, t.pt_count = int(pt_offset), int(pt_count)
+    if extent is not None:
+        t.ext_x0, t.ext_y0, t.ext_x1, t.ext_y1 = (int(v) for v in extent)
+    t.out_offset, t.site_offset = int(out_offset), int(site_offset)
+    return t
+
+
+class Batch:
+    """A planned batch of tiles (dnni_batch); runs many times."""
+
+    def __init__(self, eng: Engine, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False):
+        self._eng = eng
+        arr = (Tile * len(tiles))(*tiles)
+        opt = BatchOptions(int(small_radius), int(bin_target), int(bool(use_graph)), int(bool(order_by_cost)))
+        h = _P()
+        eng._check(lib().dnni_batch_create(eng.handle, arr, len(tiles), ctypes.byref(opt), ctypes.byref(h)))
+        self._h = h
+        self.tiles = list(tiles)
+
+    def close(self):
+        if self._h:
+            lib().dnni_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run_device(self, d_xyz, d_h, d_gid=None, d_site=None, stream=None, stats=False):
+        st = Stats() if stats else None
+        self._eng._check(lib().dnni_batch_run_device(self._h, _ptr(d_xyz), _ptr(d_gid), _ptr(d_h), _ptr(d_site),
+                                                     stream, ctypes.byref(st) if st is not None else None))
+        return st
+
+    def run(self, xyz, out_h, gid=None, out_site=None, stats=True):
+        xyz = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1, 3)
+        if gid is not None:
+            gid = np.ascontiguousarray(gid, dtype=np.uint32)
+        st = Stats() if stats else None
+        self._eng._check(lib().dnni_batch_run(self._h, _ptr(xyz), _ptr(gid), xyz.shape[0], _ptr(out_h),
+                                              _ptr(out_site), ctypes.byref(st) if st is not None else None))
+        return st

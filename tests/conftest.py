@@ -38,7 +38,7 @@ def oracle():
 def _emu_deps():
     deps = [os.path.join(NATIVE, "dnni_emu.cu")]
     csrc = os.path.join(ROOT, "terranni_b200", "csrc")
-    deps += [os.path.join(csrc, f) for f in ("dnni_kernels.cuh", "dnni_plan.h")]
+    deps += [os.path.join(csrc, f) for f in ("dnni_search.cuh", "dnni_kernels.cuh", "dnni_plan.h")]
     deps.append(os.path.join(ROOT, "include", "dnni.h"))
     return deps
 

@@ -9,7 +9,7 @@
 #include <vector>
 
 #include "../../include/dnni.h"
-#include "../../terranni_b200/csrc/dnni_kernels.cuh"
+#include "../../terranni_b200/csrc/dnni_search.cuh"
 #include "../../terranni_b200/csrc/dnni_plan.h"
 
 using namespace dnni;
