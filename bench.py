@@ -1,22 +1,28 @@
 #!/usr/bin/env python
 """Benchmark of the discrete natural-neighbour interpolation hot path.
 
-Workload (one step = one pass of the hot path over one batch):
+Workloads (one step = one pass of the hot path over one batch):
+  "mixed" (default): 4096 independent tiles, side log-uniform in 64-1024
+  cells, cells of 0.5/1/2 m, 1e3-1e6 points per tile (density log-uniform in
+  0.05-8 points/cell), per-tile fBm terrain with 0-4 lakes, each tile at its
+  own origin.  The batched form runs all tiles in one graph-captured launch
+  sequence (dnni_batch_run_device); the plain form beside it makes one
+  blocking dnni_interpolate_segment_device call per tile.
   "tile4096": one 4096 x 4096 work package at 1 m cells, 20M points
   (70 % uniform + 30 % in 64 Gaussian clusters, 16 empty lakes of radius
-  50-400 m, fBm z 0-300 m + N(0, 0.1 m)), int32 LAS coordinates at 0.01 m.
-  Seeded synthetic data; each rank interpolates its own tile (weak scaling,
-  no collective on the data path).
+  50-400 m, fBm z 0-300 m + N(0, 0.1 m)), plain per-call form.
+Seeded synthetic data, int32 LAS coordinates at 0.01 m; each rank
+interpolates its own tiles (weak scaling, no collective on the data path).
 
-value   cells/s with the points already in HBM (device-buffer C-ABI call),
-        timed with CUDA events on the launch stream, max over ranks.
-e2e     the same metric through the host-buffer C-ABI call
-        (dnni_interpolate_segment) from pinned host memory: the 240 MB point
-        upload and the 67 MB height download are inside the timed region.
+value   cells/s with the points already in HBM, timed with CUDA events on
+        the launch stream, max over ranks.
+e2e     the same metric through the host-buffer C-ABI call (dnni_batch_run
+        or dnni_interpolate_segment) from pinned host memory: the point
+        upload and the height download are inside the timed region.
 
 ``--impl reference`` times the CPU rendition of the reference's algorithm
 (the oracle port; the reference itself cannot be built) with all host threads
-on bounded windows of the same workload.
+on a bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -34,8 +40,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "DEM cells/s batched vs plain GPU NNI at ≤1e-4 m err vs FP64; p50/p99 tile latency"
 UNIT = "cells/s"
-KERNELS_PER_CALL = 18      # own kernel launches per interpolate call with points (2 + 16)
+KERNELS_PER_CALL = 18      # own kernel launches per interpolate call or batch run with points (2 + 16)
 FALLBACK_HBM_GBS = 6650.0
+BASE_SEED = 20261203
 
 
 def parse():
@@ -44,10 +51,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", choices=["mixed", "tile4096"], default="mixed")
+    ap.add_argument("--tiles", type=int, default=4096, help="tiles of the mixed workload")
+    ap.add_argument("--plain-steps", type=int, default=2, help="timed passes of the plain per-tile form")
     ap.add_argument("--side", type=int, default=4096)
     ap.add_argument("--points", type=int, default=20_000_000)
     ap.add_argument("--cpu-window", type=int, default=2048, help="side of the CPU baseline sample window")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small-radius", type=int, default=0)
+    ap.add_argument("--bin-target", type=int, default=0)
     return ap.parse_args()
 
 
@@ -153,7 +166,7 @@ def cpu_baseline(xyz, side, window, seed_note):
                       f"single-thread C oracle (k-d tree nearest site + row-span scatter), {dt:.2f} s"}
 
 
-def run_reference(args, world, rank):
+def run_reference_tile4096(args, world, rank):
     """CPU rendition of the reference's algorithm with all host threads."""
     if rank != 0:
         return
@@ -200,7 +213,7 @@ def run_reference(args, world, rank):
     }), flush=True)
 
 
-def run_engine(args, world, rank, local):
+def run_engine_tile4096(args, world, rank, local):
     import numpy as np
     import torch
     from terranni_b200 import engine
@@ -313,13 +326,291 @@ def run_engine(args, world, rank, local):
         tdist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# mixed-tile batch
+# ---------------------------------------------------------------------------
+
+def mixed_workload(count, rank, pinned):
+    """Specs, layout, points (absolute LAS xyz rows, pinned when asked) and
+    per-tile point extents of the mixed batch of this rank."""
+    import numpy as np
+    from terranni_b200 import synth
+    specs = synth.mixed_tiles(count=count, seed=BASE_SEED + 4 + 1000 * rank)
+    lay, npt, nout = synth.mixed_layout(specs)
+    if pinned:
+        import torch
+        h = torch.empty((max(npt, 1), 3), dtype=torch.int32, pin_memory=True)
+        xyz = h.numpy()[:npt]
+    else:
+        h = None
+        xyz = np.empty((npt, 3), np.int32)
+    ext = synth.fill_mixed(specs, lay, xyz)
+    return {"specs": specs, "lay": lay, "npt": npt, "nout": nout, "xyz": xyz, "ext": ext, "host": h}
+
+
+def mixed_tiles_abi(w):
+    from terranni_b200 import engine
+    return [engine.make_tile(engine.make_wp(L["side"], L["side"], L["cell"], *L["origin"]), L["pt"], L["n"],
+                             L["out"], -1, extent=w["ext"][k]) for k, L in enumerate(w["lay"])]
+
+
+def sample_order(n):
+    """Fixed visiting order of tiles for bounded CPU samples (a stride
+    through the list, so the sample spans the size distribution)."""
+    step = 97 if n > 97 else 1
+    return [(k * step) % n for k in range(n)]
+
+
+def cpu_baseline_mixed(w, h_gpu, budget_s):
+    """Oracle port, one thread, on tiles of the same batch until the budget
+    is spent; the same tiles' GPU heights are checked against it (bit-exact
+    float32, and the error against the FP64 height)."""
+    import numpy as np
+    from oracle import oracle
+    cells = 0
+    spent = 0.0
+    ntile = 0
+    exact = True
+    errs = []
+    for k in sample_order(len(w["lay"])):
+        if spent >= budget_s:
+            break
+        L = w["lay"][k]
+        wp = oracle.make_wp(L["side"], L["side"], L["cell"], *L["origin"])
+        pts = w["xyz"][L["pt"]:L["pt"] + L["n"]]
+        t0 = time.perf_counter()
+        r = oracle.interpolate(wp, pts)
+        spent += time.perf_counter() - t0
+        cells += L["side"] * L["side"]
+        ntile += 1
+        g = h_gpu[L["out"]:L["out"] + L["side"] * L["side"]].reshape(L["side"], L["side"])
+        exact &= bool(np.array_equal(g.view(np.uint32), r["h"].view(np.uint32)))
+        ok = r["C"] > 0
+        truth = oracle.exact_height_f64(r["Z"][ok], r["C"][ok], wp.z_scale, wp.z_offset)
+        errs.append(np.abs(g[ok].astype(np.float64) - truth))
+    e = np.concatenate(errs) if errs else np.zeros(1)
+    acc = {"tiles_checked": ntile, "cells_checked": cells, "bit_exact_vs_oracle": exact,
+           "max_abs_err_m": float(e.max(initial=0.0)), "rms_err_m": float(np.sqrt(np.mean(e * e)))}
+    base = {"value": cells / spent, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{ntile} tiles ({cells} cells) of the same batch in a fixed stride order, "
+                      f"single-thread C oracle (k-d tree nearest site + row-span scatter), {spent:.1f} s"}
+    return base, acc
+
+
+def run_reference_mixed(args, world, rank):
+    """CPU rendition of the reference's algorithm, all host threads, one tile
+    per thread at a time, on a fixed sample of the batch per step."""
+    if rank != 0:
+        return
+    import concurrent.futures as cf
+    from oracle import oracle
+    nthreads = os.cpu_count() or 1
+    w = mixed_workload(args.tiles, 0, pinned=False)
+    order = sample_order(len(w["lay"]))
+    # about 1.5 s of work per step on this many threads (oracle ~0.6 M cells/s
+    # per thread on these tiles)
+    target = int(1.5 * 0.6e6 * nthreads)
+    sample, cells = [], 0
+    for k in order:
+        if cells >= target:
+            break
+        sample.append(k)
+        cells += w["lay"][k]["side"] ** 2
+
+    def job(k):
+        L = w["lay"][k]
+        wp = oracle.make_wp(L["side"], L["side"], L["cell"], *L["origin"])
+        oracle.interpolate(wp, w["xyz"][L["pt"]:L["pt"] + L["n"]])
+        return L["side"] ** 2
+
+    times = []
+    with cf.ThreadPoolExecutor(nthreads) as ex:
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            c = sum(ex.map(job, sample))
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append((c, dt))
+    tot = sum(d for _, d in times)
+    v = sum(c for c, _ in times) / tot
+    desc = (f"{len(sample)} tiles ({cells} cells) of the {args.tiles}-tile batch per step, fixed stride order, "
+            f"C oracle on {nthreads} host threads (one tile per thread at a time)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": f"mixed{args.tiles}", "tiles": args.tiles, "sample_tiles": len(sample)},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def _pct(v, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else None
+
+
+def run_engine_mixed(args, world, rank, local):
+    import numpy as np
+    import torch
+    from terranni_b200 import engine
+
+    torch.cuda.set_device(local)
+    tdist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if tdist is not None:
+            tdist.barrier()
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if tdist is not None:
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = mixed_workload(args.tiles, rank, pinned=True)
+    npt, nout, xyz = w["npt"], w["nout"], w["xyz"]
+    tiles = mixed_tiles_abi(w)
+    eng = engine.Engine(device=local)
+    d_xyz = torch.from_numpy(xyz).cuda()
+    d_h = torch.empty(max(nout, 1), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()           # the engine launches on exactly this stream
+    sp = stream.cuda_stream
+    opts = dict(small_radius=args.small_radius, bin_target=args.bin_target)
+
+    # batched form: one graph-captured launch sequence per step
+    b = eng.batch(tiles, use_graph=True, order_by_cost=True, **opts)
+    st0 = b.run_device(d_xyz, d_h, stream=sp, stats=True)       # first warm-up: checks extents, captures
+    for _ in range(max(args.warmup - 1, 0)):
+        b.run_device(d_xyz, d_h, stream=sp)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        clk.mark("t_start")
+        evs[0].record(stream)
+        for k in range(args.steps):
+            b.run_device(d_xyz, d_h, stream=sp)
+            evs[k + 1].record(stream)
+        torch.cuda.synchronize()
+        clk.mark("t_end")
+    barrier()
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    ms_max = max_over_ranks(evs[0].elapsed_time(evs[-1]))
+    value = nout * args.steps * world / (ms_max / 1000.0)
+    b.close()
+
+    # per-phase device times from one run without the graph
+    with eng.batch(tiles, use_graph=False, order_by_cost=True, **opts) as bp:
+        bp.run_device(d_xyz, d_h, stream=sp)
+        ph = bp.run_device(d_xyz, d_h, stream=sp, stats=True)
+    phases = {k: round(getattr(ph, k), 4) for k in ("ms_bin", "ms_nearest", "ms_scatter", "ms_finalize", "ms_total")}
+
+    # plain form: one blocking call per tile, same tiles, same stream
+    d_hp = torch.empty(max(nout, 1), dtype=torch.float32, device="cuda")
+    wps = [engine.make_wp(L["side"], L["side"], L["cell"], *L["origin"]) for L in w["lay"]]
+    base_xyz, base_h = d_xyz.data_ptr(), d_hp.data_ptr()
+    tile_ms, plain_ms = [], []
+    pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for rnd in range(1 + args.plain_steps):
+        torch.cuda.synchronize()
+        barrier()
+        pa.record(stream)
+        for L, wp in zip(w["lay"], wps):
+            t0 = time.perf_counter()
+            eng.interpolate_device(wp, base_xyz + 12 * L["pt"], L["n"], base_h + 4 * L["out"], stream=sp,
+                                   stats=True)
+            if rnd:
+                tile_ms.append(1e3 * (time.perf_counter() - t0))
+        pb.record(stream)
+        torch.cuda.synchronize()
+        if rnd:
+            plain_ms.append(pa.elapsed_time(pb))
+    plain_max = max_over_ranks(sum(plain_ms))
+    plain_value = nout * len(plain_ms) * world / (plain_max / 1000.0)
+    same = bool(torch.equal(d_h.view(torch.int32), d_hp.view(torch.int32)))
+    del d_hp
+
+    # end to end: host-buffer batch call from pinned memory, graph replay
+    h_out = torch.empty(max(nout, 1), dtype=torch.float32, pin_memory=True).numpy()
+    with eng.batch(tiles, use_graph=True, order_by_cost=True, **opts) as be:
+        for _ in range(max(1, args.warmup)):
+            be.run(xyz, h_out, stats=False)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            be.run(xyz, h_out, stats=False)
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = nout * args.steps * world / e2e_s
+    h_gpu = h_out[:nout].copy()
+    nod = int(np.count_nonzero(h_gpu == np.float32(-9999.0)))
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        ms_step = ms_max / args.steps
+        alg_bytes = 12 * npt + 4 * nout
+        achieved = alg_bytes / (ms_step / 1000.0) / 1e9
+        dom = max(("ms_bin", "ms_nearest", "ms_scatter", "ms_finalize"), key=lambda k: phases[k])
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic_mixed4096.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get("dram_bytes_per_step")
+        sides = np.array([L["side"] for L in w["lay"]])
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32/int64", "data": "synthetic (seeded fBm terrain, clusters, lakes)",
+            "config": {"workload": f"mixed{args.tiles}", "tiles": args.tiles, "cells": nout, "points": npt,
+                       "side_min": int(sides.min()), "side_median": int(np.median(sides)),
+                       "side_max": int(sides.max()),
+                       "form": "batched: all tiles in one CUDA-graph launch sequence per step",
+                       "small_radius": args.small_radius or 3, "bin_target": args.bin_target or 4,
+                       "order_by_cost": True,
+                       "l2": f"inputs larger than L2 ({xyz.nbytes / 1e9:.1f} GB points per step)",
+                       "parallelism": f"dp{world} (independent tiles)"},
+            "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_max / len(plain_ms),
+                      "form": "one blocking dnni_interpolate_segment_device call per tile",
+                      "tile_ms_p50": _pct(tile_ms, 50), "tile_ms_p99": _pct(tile_ms, 99),
+                      "batched_over_plain": value / plain_value, "heights_identical_to_batched": same},
+            "latency": {"batch_ms_p50": _pct(step_ms, 50), "batch_ms_p99": _pct(step_ms, 99),
+                        "note": "batched: every tile of a step completes with its batch"},
+            "roofline": {"bound": "hbm", "kernel": "whole hot path per batch (18 launches)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": alg_bytes,
+                         "dominant_phase": dom, "phase_ms": phases},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(xyz.nbytes),
+                    "d2h_bytes_per_step": int(nout * 4)},
+            "gpu_launches": KERNELS_PER_CALL * args.steps,
+            "clocks": clk.summary(),
+            "work": {"span_pixels": st0.big_pixels, "spans": st0.spans, "max_r2": st0.max_r2,
+                     "nodata_cells": nod},
+        }
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"], out["accuracy"] = cpu_baseline_mixed(w, h_gpu, args.cpu_seconds)
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if tdist is not None:
+        tdist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist()
-    if args.impl == "reference":
-        run_reference(args, world, rank)
+    if args.workload == "mixed":
+        if args.impl == "reference":
+            run_reference_mixed(args, world, rank)
+        else:
+            run_engine_mixed(args, world, rank, local)
         return
-    run_engine(args, world, rank, local)
+    if args.impl == "reference":
+        run_reference_tile4096(args, world, rank)
+        return
+    run_engine_tile4096(args, world, rank, local)
 
 
 if __name__ == "__main__":

@@ -203,8 +203,9 @@ dnni_status dnni_batch_create(dnni_ctx *ctx, const dnni_tile *tiles, int32_t nti
 /* Runs every tile on device buffers, queued on `stream` (NULL = the
  * context's stream).  Returns with the work queued unless stats is non-NULL,
  * in which case it waits, reports totals over the tiles (ms_total is the
- * device time of the run) and checks the points against the declared
- * extents (DNNI_E_RANGE); without stats that check is not read back. */
+ * device time of the run; per-phase times too when the batch runs without
+ * a graph) and checks the points against the declared extents
+ * (DNNI_E_RANGE); without stats that check is not read back. */
 dnni_status dnni_batch_run_device(dnni_batch *batch, const int32_t *d_xyz, const uint32_t *d_gid,
                                   float *d_h, uint32_t *d_site, void *stream, dnni_stats *stats);
 /* The same from host buffers: n_rows point rows are copied in, the output

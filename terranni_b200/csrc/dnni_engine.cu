@@ -551,6 +551,10 @@ dnni_status dnni_batch_create(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
         std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
     b->hb.rs = rs_;
     for (int k : b->order) batch_add(b->hb, plan[k], tiles[k].pt_offset, tiles[k].out_offset, tiles[k].site_offset);
+    if (b->hb.too_big) {
+        delete b;
+        return set_err(c, DNNI_E_INVAL, "batch too large for one launch sequence: split it");
+    }
     dnni_status rs = ensure_scratch(c, b->scr, scratch_sizes(b->hb), b->arr);
     if (!rs) {
         b->bt = device_tables(b->arr.tables, ntiles);
@@ -597,19 +601,28 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
         }
         CK(cudaGraphLaunch(b->exec, st));
     } else {
+        // with stats, ev[1..3] mark the ends of binning, nearest sites and spans
         launch_prologue(b->hb, b->bt, b->arr, d_xyz, st);
-        launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, st, nullptr);
+        launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, st, stats ? &c->ev[1] : nullptr);
         CK(cudaGetLastError());
     }
     if (stats) {
-        CK(cudaEventRecord(c->ev[1], st));
+        CK(cudaEventRecord(c->ev[4], st));
         const int n = (int)b->hb.tiles.size();
         CK(cudaMemcpyAsync(b->h_sc.data(), b->arr.sc, sizeof(Scalars) * n, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(c->h_ctr, b->arr.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         float ms = 0;
-        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
         stats->ms_total = ms;
+        if (!b->use_graph) {
+            float ph[4];
+            for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&ph[k], c->ev[k], c->ev[k + 1]);
+            stats->ms_bin = ph[0];
+            stats->ms_nearest = ph[1];
+            stats->ms_scatter = ph[2];
+            stats->ms_finalize = ph[3];
+        }
         if (c->h_ctr->err & kErrRange)
             return set_err(c, DNNI_E_RANGE, "a point lies beyond its tile's declared extent or the coordinate range");
         fold_stats(b->h_sc.data(), n, stats);

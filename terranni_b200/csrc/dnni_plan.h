@@ -113,6 +113,9 @@ namespace dnni {
 
 // Host-side plan of a batch: every tile's geometry, bin grid and offsets,
 // plus the prefix arrays that map launch indices to tiles.
+// Largest launch index (blocks of a kind, far worklist slots) of a batch.
+constexpr int64_t kMaxLaunchIndex = INT32_MAX - 1024;
+
 struct HostBatch {
     std::vector<TileParams> tiles;
     std::vector<int> chunk_base{0}, scan_base{0}, row1_base{0}, rt_base{0}, ct_base{0}, grow_base{0};
@@ -122,6 +125,7 @@ struct HostBatch {
     int64_t out_end = 0, site_end = 0;   // extent of the caller's output arrays used
     int64_t cost = 0;
     int rs = 3;                          // stencil radius shared by the batch
+    bool too_big = false;                // a launch index or the far worklist would pass int32
 };
 
 // Worklist capacity of a tile: every dense warp (32 pixels of a tile row, the
@@ -147,17 +151,24 @@ inline void batch_add(HostBatch& hb, TileParams t, int64_t pt_off, int64_t out_o
     hb.n_bins += nbins + 1;
     hb.blk_base.push_back(t.blk_off + nbins / kBinsPerBlock);
     hb.sup_base.push_back(t.sup_off + nbins / kBinsPerSuper);
-    hb.chunk_base.push_back(hb.chunk_base.back() + (int)((t.npts + kChunk - 1) / kChunk));
-    hb.scan_base.push_back(hb.scan_base.back() + (int)((nbins + 1 + kScanTile - 1) / kScanTile));
-    hb.row1_base.push_back(hb.row1_base.back() + (t.npts > 0 ? (t.bg.nby >> 3) : 0));
-    hb.rt_base.push_back(hb.rt_base.back() + ((t.rw + kTileX - 1) / kTileX) * ((t.rh + kTileY - 1) / kTileY));
-    hb.ct_base.push_back(hb.ct_base.back() + ((t.ncols + 31) / 32) * ((t.nrows + 15) / 16));
-    hb.grow_base.push_back(hb.grow_base.back() + t.nrows);
+    // the int32 prefix arrays saturate; too_big then rejects the batch
+    auto add = [&](std::vector<int>& v, int64_t k) {
+        const int64_t x = (int64_t)v.back() + k;
+        if (x > kMaxLaunchIndex) hb.too_big = true;
+        v.push_back((int)std::min<int64_t>(x, kMaxLaunchIndex));
+    };
+    add(hb.chunk_base, (t.npts + kChunk - 1) / kChunk);
+    add(hb.scan_base, (nbins + 1 + kScanTile - 1) / kScanTile);
+    add(hb.row1_base, t.npts > 0 ? (t.bg.nby >> 3) : 0);
+    add(hb.rt_base, (int64_t)((t.rw + kTileX - 1) / kTileX) * ((t.rh + kTileY - 1) / kTileY));
+    add(hb.ct_base, (int64_t)((t.ncols + 31) / 32) * ((t.nrows + 15) / 16));
+    add(hb.grow_base, t.nrows);
     hb.n_rows = std::max<int64_t>(hb.n_rows, pt_off + t.npts);
     hb.n_pts += t.npts;
     hb.n_pix += (int64_t)t.rw * t.rh;
     hb.n_cells += (int64_t)t.ncols * t.nrows;
     hb.n_far += far_slots(t);
+    if (hb.n_far > kMaxLaunchIndex) hb.too_big = true;
     hb.out_end = std::max<int64_t>(hb.out_end, out_off + (int64_t)t.ncols * t.nrows);
     if (site_off >= 0) hb.site_end = std::max<int64_t>(hb.site_end, site_off + (int64_t)t.rw * t.rh);
     t.tile_id = (int32_t)hb.tiles.size();

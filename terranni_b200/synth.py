@@ -51,8 +51,9 @@ def lib():
 
 def generate(seed, n, width, height, kind="terrain", nclusters=64, frac_uniform=0.7, cluster_sigma=20.0,
              nlakes=16, lake_rmin=50.0, lake_rmax=400.0, relief=300.0, z_noise=0.1, hurst=0.8, octaves=8,
-             base_wavelength=None, nthreads=0):
-    """-> (xyz int32 (n,3), lakes float64 (nlakes,3) as cx, cy, r in metres)."""
+             base_wavelength=None, nthreads=0, out=None):
+    """-> (xyz int32 (n,3), lakes float64 (nlakes,3) as cx, cy, r in metres).
+    out: optional C-contiguous int32 (n,3) array to generate into."""
     p = SynthParams()
     p.seed, p.n, p.width, p.height = int(seed), int(n), float(width), float(height)
     p.xy_scale, p.z_scale = XY_SCALE, Z_SCALE
@@ -63,7 +64,12 @@ def generate(seed, n, width, height, kind="terrain", nclusters=64, frac_uniform=
     p.relief, p.z_noise, p.hurst = float(relief), float(z_noise), float(hurst)
     p.base_wavelength = float(base_wavelength if base_wavelength else max(width, height) / 2.0)
     p.nthreads = int(nthreads)
-    xyz = np.empty((int(n), 3), np.int32)
+    if out is not None:
+        if out.dtype != np.int32 or out.shape != (int(n), 3) or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a C-contiguous int32 (n, 3) array")
+        xyz = out
+    else:
+        xyz = np.empty((int(n), 3), np.int32)
     lakes = np.zeros((max(int(nlakes), 1), 3), np.float64)
     rc = lib().synth_generate(ctypes.byref(p), xyz.ctypes.data_as(ctypes.c_void_p),
                               lakes.ctypes.data_as(ctypes.c_void_p))
@@ -104,9 +110,46 @@ def mixed_tiles(count=4096, seed=BASE_SEED + 4, max_points=1_000_000):
              "seed": int(seeds[i])} for i in range(count)]
 
 
-def tile_points(spec):
+def tile_points(spec, out=None):
     ext = spec["side"] * spec["cell"] * XY_SCALE
     xyz, _ = generate(spec["seed"], spec["n"], ext, ext, kind="terrain", nclusters=8, frac_uniform=0.7,
                       cluster_sigma=max(ext / 50.0, 1.0), nlakes=spec["lakes"], lake_rmin=0.05 * ext,
-                      lake_rmax=0.3 * ext, relief=300.0, z_noise=0.1)
+                      lake_rmax=0.3 * ext, relief=300.0, z_noise=0.1, nthreads=1, out=out)
     return xyz
+
+
+def tile_origin(k):
+    """Absolute LAS origin of tile k of a mixed batch: tiles sit on a 64-wide
+    lattice of 1.1 km pitch, so every tile has its own origin."""
+    return (k % 64) * 110_000, (k // 64) * 110_000
+
+
+def mixed_layout(specs):
+    """Row offsets and output offsets of a mixed batch, in spec order."""
+    pt = out = 0
+    lay = []
+    for k, s in enumerate(specs):
+        ox, oy = tile_origin(k)
+        lay.append({"pt": pt, "n": s["n"], "out": out, "side": s["side"], "cell": s["cell"], "origin": (ox, oy)})
+        pt += s["n"]
+        out += s["side"] * s["side"]
+    return lay, pt, out
+
+
+def fill_mixed(specs, lay, xyz, nthreads=None):
+    """Generates every tile's points into its rows of xyz (absolute LAS
+    coordinates) on a thread pool; returns each tile's point extent
+    (x0, y0, x1, y1), absolute and inclusive."""
+    from concurrent.futures import ThreadPoolExecutor
+    nthreads = nthreads or os.cpu_count() or 1
+
+    def one(k):
+        s, L = specs[k], lay[k]
+        rows = xyz[L["pt"]:L["pt"] + L["n"]]
+        tile_points(s, out=rows)
+        rows[:, 0] += L["origin"][0]
+        rows[:, 1] += L["origin"][1]
+        return (int(rows[:, 0].min()), int(rows[:, 1].min()), int(rows[:, 0].max()), int(rows[:, 1].max()))
+
+    with ThreadPoolExecutor(nthreads) as ex:
+        return list(ex.map(one, range(len(specs))))
