@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", choices=["mixed", "tile4096"], default="mixed")
     ap.add_argument("--tiles", type=int, default=4096, help="tiles of the mixed workload")
-    ap.add_argument("--plain-steps", type=int, default=2, help="timed passes of the plain per-tile form")
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="timed passes of the plain per-tile form (0: skip the plain form)")
     ap.add_argument("--side", type=int, default=4096)
     ap.add_argument("--points", type=int, default=20_000_000)
     ap.add_argument("--cpu-window", type=int, default=2048, help="side of the CPU baseline sample window")
@@ -61,6 +62,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small-radius", type=int, default=0)
     ap.add_argument("--bin-target", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true", help="mixed: skip the autotuner (context defaults)")
+    ap.add_argument("--tune-sample", type=int, default=256, help="mixed: tiles the autotuner times")
     return ap.parse_args()
 
 
@@ -481,6 +484,12 @@ def run_engine_mixed(args, world, rank, local):
     stream = torch.cuda.Stream()           # the engine launches on exactly this stream
     sp = stream.cuda_stream
     opts = dict(small_radius=args.small_radius, bin_target=args.bin_target)
+    tune = None
+    if not args.no_autotune:              # outside the timed region
+        t0 = time.perf_counter()
+        opts, rep = eng.autotune(tiles, d_xyz, sample_tiles=args.tune_sample, **opts)
+        tune = {"sample_tiles": rep["sample_tiles"], "ms_default": rep["ms_default"], "best": rep["best"],
+                "trials": len(rep["trials"]), "seconds": time.perf_counter() - t0}
 
     # batched form: one graph-captured launch sequence per step
     b = eng.batch(tiles, use_graph=True, order_by_cost=True, **opts)
@@ -517,7 +526,7 @@ def run_engine_mixed(args, world, rank, local):
     base_xyz, base_h = d_xyz.data_ptr(), d_hp.data_ptr()
     tile_ms, plain_ms = [], []
     pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for rnd in range(1 + args.plain_steps):
+    for rnd in range(1 + args.plain_steps if args.plain_steps > 0 else 0):
         torch.cuda.synchronize()
         barrier()
         pa.record(stream)
@@ -532,8 +541,8 @@ def run_engine_mixed(args, world, rank, local):
         if rnd:
             plain_ms.append(pa.elapsed_time(pb))
     plain_max = max_over_ranks(sum(plain_ms))
-    plain_value = nout * len(plain_ms) * world / (plain_max / 1000.0)
-    same = bool(torch.equal(d_h.view(torch.int32), d_hp.view(torch.int32)))
+    plain_value = nout * len(plain_ms) * world / (plain_max / 1000.0) if plain_ms else None
+    same = bool(torch.equal(d_h.view(torch.int32), d_hp.view(torch.int32))) if plain_ms else None
     del d_hp
 
     # end to end: host-buffer batch call from pinned memory, graph replay
@@ -569,14 +578,16 @@ def run_engine_mixed(args, world, rank, local):
                        "side_min": int(sides.min()), "side_median": int(np.median(sides)),
                        "side_max": int(sides.max()),
                        "form": "batched: all tiles in one CUDA-graph launch sequence per step",
-                       "small_radius": args.small_radius or 3, "bin_target": args.bin_target or 4,
-                       "order_by_cost": True,
+                       "small_radius": opts["small_radius"] or 3, "bin_target": opts["bin_target"] or 4,
+                       "order_by_cost": True, "autotune": tune,
                        "l2": f"inputs larger than L2 ({xyz.nbytes / 1e9:.1f} GB points per step)",
                        "parallelism": f"dp{world} (independent tiles)"},
-            "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": plain_max / len(plain_ms),
+            "plain": {"value": plain_value, "unit": UNIT,
+                      "ms_per_step": plain_max / len(plain_ms) if plain_ms else None,
                       "form": "one blocking dnni_interpolate_segment_device call per tile",
                       "tile_ms_p50": _pct(tile_ms, 50), "tile_ms_p99": _pct(tile_ms, 99),
-                      "batched_over_plain": value / plain_value, "heights_identical_to_batched": same},
+                      "batched_over_plain": value / plain_value if plain_value else None,
+                      "heights_identical_to_batched": same},
             "latency": {"batch_ms_p50": _pct(step_ms, 50), "batch_ms_p99": _pct(step_ms, 99),
                         "note": "batched: every tile of a step completes with its batch"},
             "roofline": {"bound": "hbm", "kernel": "whole hot path per batch (18 launches)",

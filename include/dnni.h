@@ -215,6 +215,31 @@ dnni_status dnni_batch_run(dnni_batch *batch, const int32_t *xyz, const uint32_t
                            float *out_h, uint32_t *out_site, dnni_stats *stats);
 dnni_status dnni_batch_destroy(dnni_batch *batch);
 
+/* ---- autotuning of the batch options (no counterpart in the reference) ----
+ *
+ * Times candidate settings of the search-bin size (bin_target: points per
+ * bin) and of the split between the stencil path and the span path
+ * (small_radius: discs up to this radius are gathered by the stencil, larger
+ * ones spill into row spans) on a sample of the tiles stratified by size, on
+ * device buffers that already hold the points, and writes the fastest pair
+ * into *options (use_graph and order_by_cost are left as given).  Results do
+ * not depend on either setting; only the time does. */
+typedef struct dnni_tune_trial {
+    int32_t small_radius, bin_target;
+    float ms;                          /* device time of one run of the sample */
+    int32_t pad;
+} dnni_tune_trial;
+
+typedef struct dnni_tune_report {
+    int32_t ntrials, best, sample_tiles, pad;
+    double ms_default;                 /* the sample at the settings given on entry */
+    dnni_tune_trial trial[32];
+} dnni_tune_report;
+
+dnni_status dnni_batch_autotune(dnni_ctx *ctx, const dnni_tile *tiles, int32_t ntiles, const int32_t *d_xyz,
+                                const uint32_t *d_gid, int32_t sample_tiles, dnni_batch_options *options,
+                                dnni_tune_report *report);
+
 /* ---- nni::clearRenderbuffers / nni::printTimes (nni.h:87-97) ---- */
 
 /* Free the context's scratch (it is re-created on demand). */

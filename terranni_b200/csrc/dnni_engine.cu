@@ -336,6 +336,54 @@ static dnni_status run_device(dnni_ctx* c, const dnni_workpackage* wp, const int
     return DNNI_OK;
 }
 
+// Plans a batch: every tile from its geometry and declared point extent, in
+// cost order when asked.  order[k] = the caller's index of batch position k.
+static dnni_status plan_batch(dnni_ctx* c, const dnni_tile* tiles, int32_t ntiles, const dnni_batch_options& o,
+                              HostBatch& hb, std::vector<int>& order) {
+    const int rs_ = o.small_radius ? o.small_radius : c->s.small_radius;
+    const int bt_ = o.bin_target ? o.bin_target : c->s.bin_target;
+    if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0) return set_err(c, DNNI_E_INVAL, "bad batch options");
+    std::vector<TileParams> plan(ntiles);
+    std::vector<int64_t> cost(ntiles);
+    for (int k = 0; k < ntiles; ++k) {
+        const dnni_tile& d = tiles[k];
+        const char* msg = "";
+        dnni_status rs = plan_geometry(&d.wp, d.pt_count, rs_, plan[k], &msg);
+        if (rs) return set_err(c, rs, std::string("tile ") + std::to_string(k) + ": " + msg);
+        if (d.pt_offset < 0 || d.pt_count < 0 || d.out_offset < 0)
+            return set_err(c, DNNI_E_INVAL, "negative tile offset");
+        int32_t bb[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, 0, 0};
+        if (d.ext_x0 || d.ext_y0 || d.ext_x1 || d.ext_y1) {
+            const long long ex0 = (long long)d.ext_x0 - d.wp.origin_x, ex1 = (long long)d.ext_x1 - d.wp.origin_x;
+            const long long ey0 = (long long)d.ext_y0 - d.wp.origin_y, ey1 = (long long)d.ext_y1 - d.wp.origin_y;
+            if (ex1 < ex0 || ey1 < ey0) return set_err(c, DNNI_E_INVAL, "empty point extent");
+            if (ex0 <= -kCoordLimit || ex1 >= kCoordLimit || ey0 <= -kCoordLimit || ey1 >= kCoordLimit)
+                return set_err(c, DNNI_E_RANGE, "point extent beyond +-2^30 LAS units of the origin");
+            bb[0] = (int32_t)ex0;
+            bb[1] = (int32_t)ex1;
+            bb[2] = (int32_t)ey0;
+            bb[3] = (int32_t)ey1;
+        }
+        plan_bins(bb, d.pt_count, bt_, plan[k]);
+        if (bb[0] <= bb[1]) {
+            plan[k].has_ext = 1;
+            plan[k].ex0 = bb[0];
+            plan[k].ex1 = bb[1];
+            plan[k].ey0 = bb[2];
+            plan[k].ey1 = bb[3];
+        }
+        cost[k] = (int64_t)plan[k].rw * plan[k].rh + d.pt_count;
+    }
+    order.resize(ntiles);
+    std::iota(order.begin(), order.end(), 0);
+    if (o.order_by_cost) std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    hb = HostBatch();
+    hb.rs = rs_;
+    for (int k : order) batch_add(hb, plan[k], tiles[k].pt_offset, tiles[k].out_offset, tiles[k].site_offset);
+    if (hb.too_big) return set_err(c, DNNI_E_INVAL, "batch too large for one launch sequence: split it");
+    return DNNI_OK;
+}
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -507,53 +555,15 @@ dnni_status dnni_batch_create(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
     DeviceGuard g(c->device);
     dnni_batch_options o{};
     if (opt) o = *opt;
-    const int rs_ = o.small_radius ? o.small_radius : c->s.small_radius;
-    const int bt_ = o.bin_target ? o.bin_target : c->s.bin_target;
-    if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0) return set_err(c, DNNI_E_INVAL, "bad batch options");
-    // plan every tile from its geometry and declared point extent
-    std::vector<TileParams> plan(ntiles);
-    std::vector<int64_t> cost(ntiles);
-    for (int k = 0; k < ntiles; ++k) {
-        const dnni_tile& d = tiles[k];
-        const char* msg = "";
-        dnni_status rs = plan_geometry(&d.wp, d.pt_count, rs_, plan[k], &msg);
-        if (rs) return set_err(c, rs, std::string("tile ") + std::to_string(k) + ": " + msg);
-        if (d.pt_offset < 0 || d.pt_count < 0 || d.out_offset < 0)
-            return set_err(c, DNNI_E_INVAL, "negative tile offset");
-        int32_t bb[6] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, 0, 0};
-        if (d.ext_x0 || d.ext_y0 || d.ext_x1 || d.ext_y1) {
-            const long long ex0 = (long long)d.ext_x0 - d.wp.origin_x, ex1 = (long long)d.ext_x1 - d.wp.origin_x;
-            const long long ey0 = (long long)d.ext_y0 - d.wp.origin_y, ey1 = (long long)d.ext_y1 - d.wp.origin_y;
-            if (ex1 < ex0 || ey1 < ey0) return set_err(c, DNNI_E_INVAL, "empty point extent");
-            if (ex0 <= -kCoordLimit || ex1 >= kCoordLimit || ey0 <= -kCoordLimit || ey1 >= kCoordLimit)
-                return set_err(c, DNNI_E_RANGE, "point extent beyond +-2^30 LAS units of the origin");
-            bb[0] = (int32_t)ex0;
-            bb[1] = (int32_t)ex1;
-            bb[2] = (int32_t)ey0;
-            bb[3] = (int32_t)ey1;
-        }
-        plan_bins(bb, d.pt_count, bt_, plan[k]);
-        if (bb[0] <= bb[1]) {
-            plan[k].has_ext = 1;
-            plan[k].ex0 = bb[0];
-            plan[k].ex1 = bb[1];
-            plan[k].ey0 = bb[2];
-            plan[k].ey1 = bb[3];
-        }
-        cost[k] = (int64_t)plan[k].rw * plan[k].rh + d.pt_count;
-    }
     dnni_batch* b = new dnni_batch();
     b->ctx = c;
     b->use_graph = o.use_graph;
-    b->order.resize(ntiles);
-    std::iota(b->order.begin(), b->order.end(), 0);
-    if (o.order_by_cost)
-        std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-    b->hb.rs = rs_;
-    for (int k : b->order) batch_add(b->hb, plan[k], tiles[k].pt_offset, tiles[k].out_offset, tiles[k].site_offset);
-    if (b->hb.too_big) {
-        delete b;
-        return set_err(c, DNNI_E_INVAL, "batch too large for one launch sequence: split it");
+    {
+        dnni_status rs = plan_batch(c, tiles, ntiles, o, b->hb, b->order);
+        if (rs) {
+            delete b;
+            return rs;
+        }
     }
     dnni_status rs = ensure_scratch(c, b->scr, scratch_sizes(b->hb), b->arr);
     if (!rs) {
@@ -687,6 +697,99 @@ dnni_status dnni_batch_destroy(dnni_batch* b) {
         dnni_release(b->out_site, c);
     }
     delete b;
+    return DNNI_OK;
+}
+
+// ---- autotuner -------------------------------------------------------------
+
+dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t ntiles, const int32_t* d_xyz,
+                                const uint32_t* d_gid, int32_t sample_tiles, dnni_batch_options* options,
+                                dnni_tune_report* report) {
+    if (!c || !tiles || ntiles <= 0 || !options) return DNNI_E_INVAL;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    const dnni_batch_options given = *options;
+    // sample: tiles evenly spaced in cost order, so that it spans the sizes
+    std::vector<int> idx(ntiles);
+    std::iota(idx.begin(), idx.end(), 0);
+    auto cost = [&](int k) { return (int64_t)tiles[k].wp.ncols * tiles[k].wp.nrows + tiles[k].pt_count; };
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    const int m = sample_tiles > 0 && sample_tiles < ntiles ? sample_tiles : ntiles;
+    std::vector<dnni_tile> smp(m);
+    int64_t out = 0;
+    for (int k = 0; k < m; ++k) {
+        smp[k] = tiles[idx[(int64_t)k * ntiles / m]];
+        smp[k].out_offset = out;
+        smp[k].site_offset = -1;
+        out += (int64_t)smp[k].wp.ncols * smp[k].wp.nrows;
+    }
+    DevBuf hbuf;
+    Scratch tscr;
+    DevArrays a;
+    HostBatch hb;
+    std::vector<int> order;
+    std::vector<dnni_tune_trial> trials;
+    cudaStream_t st = c->stream;
+    auto trial = [&](int rs_, int bt_, float* ms) -> dnni_status {
+        dnni_batch_options o = given;
+        o.small_radius = rs_;
+        o.bin_target = bt_;
+        dnni_status rs = plan_batch(c, smp.data(), m, o, hb, order);
+        if (rs) return rs;
+        if ((rs = ensure_scratch(c, tscr, scratch_sizes(hb), a))) return rs;
+        const BatchTables bt = device_tables(a.tables, m);
+        if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
+        for (int r = 0; r < 3; ++r) {            // one warm-up run, two timed
+            if (r == 1) CK(cudaEventRecord(c->ev[0], st));
+            launch_prologue(hb, bt, a, d_xyz, st);
+            launch_body(hb, bt, a, d_xyz, d_gid, (float*)hbuf.p, nullptr, c->sm_count, st, nullptr);
+        }
+        CK(cudaEventRecord(c->ev[1], st));
+        CK(cudaGetLastError());
+        CK(cudaEventSynchronize(c->ev[1]));
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
+        *ms = t / 2;
+        trials.push_back(dnni_tune_trial{rs_, bt_, *ms, 0});
+        return DNNI_OK;
+    };
+    dnni_status rs = dnni_ensure(c, hbuf, sizeof(float) * std::max<int64_t>(out, 1));
+    const int rs0 = given.small_radius ? given.small_radius : c->s.small_radius;
+    const int bt0 = given.bin_target ? given.bin_target : (c->s.bin_target ? c->s.bin_target : 4);
+    float ms_default = 0, best_ms = 0;
+    int best_rs = rs0, best_bt = bt0;
+    if (!rs) rs = trial(rs0, bt0, &ms_default);
+    best_ms = ms_default;
+    // coordinate search: the bin size first, then the stencil/span split
+    static const int kBinTargets[] = {2, 3, 4, 6, 8, 12};
+    static const int kRadii[] = {1, 2, 3, 4, 5, 6};
+    for (int bt_ : kBinTargets) {
+        if (rs || bt_ == bt0) continue;
+        float ms = 0;
+        rs = trial(rs0, bt_, &ms);
+        if (!rs && ms < best_ms) { best_ms = ms; best_bt = bt_; }
+    }
+    for (int r_ : kRadii) {
+        if (rs || r_ == rs0 || r_ > kMaxSmallRadius) continue;
+        float ms = 0;
+        rs = trial(r_, best_bt, &ms);
+        if (!rs && ms < best_ms) { best_ms = ms; best_rs = r_; }
+    }
+    release_scratch(c, tscr);
+    dnni_release(hbuf, c);
+    if (rs) return rs;
+    options->small_radius = best_rs;
+    options->bin_target = best_bt;
+    if (report) {
+        memset(report, 0, sizeof(*report));
+        report->ntrials = (int32_t)std::min<size_t>(trials.size(), 32);
+        report->sample_tiles = m;
+        report->ms_default = ms_default;
+        for (int k = 0; k < report->ntrials; ++k) {
+            report->trial[k] = trials[k];
+            if (trials[k].small_radius == best_rs && trials[k].bin_target == best_bt) report->best = k;
+        }
+    }
     return DNNI_OK;
 }
 

@@ -79,6 +79,22 @@ class BatchOptions(ctypes.Structure):
                 ("use_graph", ctypes.c_int32), ("order_by_cost", ctypes.c_int32)]
 
 
+class TuneTrial(ctypes.Structure):
+    _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
+                ("pad", ctypes.c_int32)]
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("ntrials", ctypes.c_int32), ("best", ctypes.c_int32), ("sample_tiles", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("ms_default", ctypes.c_double), ("trial", TuneTrial * 32)]
+
+    def as_dict(self):
+        t = [{"small_radius": self.trial[k].small_radius, "bin_target": self.trial[k].bin_target,
+              "ms": self.trial[k].ms} for k in range(self.ntrials)]
+        return {"sample_tiles": self.sample_tiles, "ms_default": self.ms_default,
+                "best": t[self.best] if t else None, "trials": t}
+
+
 # every symbol include/dnni.h declares, with (argtypes, restype)
 _P = ctypes.c_void_p
 _SIGS = {
@@ -102,6 +118,8 @@ _SIGS = {
     "dnni_batch_run_device": ([_P, _P, _P, _P, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
     "dnni_batch_run": ([_P, _P, _P, ctypes.c_int64, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
     "dnni_batch_destroy": ([_P], ctypes.c_int),
+    "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
+                             ctypes.POINTER(BatchOptions), ctypes.POINTER(TuneReport)], ctypes.c_int),
 }
 
 _lib = None
@@ -219,6 +237,15 @@ class Engine:
     def batch(self, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False):
         """Plans a batch of tiles (dnni_batch_create) -> Batch."""
         return Batch(self, tiles, small_radius, bin_target, use_graph, order_by_cost)
+
+    def autotune(self, tiles, d_xyz, d_gid=None, sample_tiles=256, small_radius=0, bin_target=0):
+        """dnni_batch_autotune -> (dict(small_radius, bin_target), report dict)."""
+        arr = (Tile * len(tiles))(*tiles)
+        opt = BatchOptions(int(small_radius), int(bin_target), 0, 0)
+        rep = TuneReport()
+        self._check(lib().dnni_batch_autotune(self._h, arr, len(tiles), _ptr(d_xyz), _ptr(d_gid), int(sample_tiles),
+                                              ctypes.byref(opt), ctypes.byref(rep)))
+        return {"small_radius": opt.small_radius, "bin_target": opt.bin_target}, rep.as_dict()
 
     def clear(self):
         self._check(lib().dnni_clear(self._h))

@@ -192,3 +192,18 @@ def test_batch_point_outside_declared_extent_is_a_range_error(eng):
     with pytest.raises(engine.DnniError) as ei:          # extent beyond the coordinate range
         eng.batch([engine.make_tile(wp, 0, 10, 0, -1, extent=(0, 0, 1 << 30, 10))])
     assert ei.value.status == 5
+
+
+def test_autotuned_options_give_the_same_heights(eng):
+    import torch
+    xyz, tiles, meta, nout, nsite = _layout(_tiles(seed=21, count=10))
+    d_xyz = torch.from_numpy(xyz).cuda()
+    opts, rep = eng.autotune(tiles, d_xyz, sample_tiles=6)
+    assert rep["sample_tiles"] == 6 and len(rep["trials"]) >= 8
+    assert rep["best"]["small_radius"] == opts["small_radius"] and rep["best"]["bin_target"] == opts["bin_target"]
+    assert rep["best"]["ms"] <= rep["ms_default"] + 1e-6
+    assert all(t["ms"] > 0 for t in rep["trials"])
+    ref = _per_tile(eng, xyz, meta)
+    with eng.batch(tiles, use_graph=True, **opts) as b:
+        h, s, _ = _run_device(b, xyz, nout, nsite)
+    _check(meta, ref, h, s)
