@@ -215,6 +215,48 @@ dnni_status dnni_batch_run(dnni_batch *batch, const int32_t *xyz, const uint32_t
                            float *out_h, uint32_t *out_site, dnni_stats *stats);
 dnni_status dnni_batch_destroy(dnni_batch *batch);
 
+/* ---- segment driver: one large grid in tiles with halos ----
+ *
+ * Replaces the reference's out-of-core pipeline around performNNI for one
+ * grid: binning of the points into work packages with duplicated borders
+ * (terranni.cpp:203-368, 271-302), the work-package loop of binRun
+ * (terranni.cpp:394-426) and the assembly of the grid (terranni.cpp:430-488).
+ * The points (absolute int32 LAS xyz, host memory, pinned for full copy
+ * speed) are uploaded in chunks and bucketed by position on the device; the
+ * grid is cut into tile x tile cell tiles, each interpolated with a raster
+ * halo and a point halo, in batches.  After each batch every tile's largest
+ * nearest-site distance is checked against its halo: a tile whose halo could
+ * have missed a pixel whose disc reaches it, or a site nearer than the one
+ * found, runs again with a larger halo.  The result (heights and site map,
+ * gid = the point's index in the input) is therefore bit-identical to one
+ * work package covering the whole grid with raster = grid. */
+typedef struct dnni_segment {
+    int32_t ncols, nrows;          /* the whole grid, cells (each side <= 2^20) */
+    int32_t cell_size;             /* LAS units */
+    int32_t origin_x, origin_y;    /* LAS position of cell (0,0) */
+    int32_t tile;                  /* tile side in cells (0 = 2048) */
+    int32_t halo;                  /* first raster halo tried, cells (0 = 64) */
+    int32_t tiles_per_batch;       /* 0 = 16 */
+    double z_scale, z_offset;
+    float nodata;
+    int32_t small_radius;          /* 0 = the context's setting */
+} dnni_segment;
+
+typedef struct dnni_segment_stats {
+    double ms_total;               /* wall time of the call */
+    double ms_upload, ms_bucket;   /* host->device copy, device bucketing */
+    int64_t points, cells, tiles;
+    int64_t tile_runs;             /* tiles + reruns with a larger halo */
+    int64_t h2d_bytes, d2h_bytes;
+    int32_t max_halo;              /* largest raster halo any tile needed */
+    int32_t pad;
+} dnni_segment_stats;
+
+/* h_out: nrows x ncols floats, row-major, row 0 = lowest y; h_site (optional):
+ * nrows x ncols uint32 site ids. */
+dnni_status dnni_segment_run(dnni_ctx *ctx, const dnni_segment *seg, const int32_t *h_xyz, int64_t n,
+                             float *h_out, uint32_t *h_site, dnni_segment_stats *stats);
+
 /* ---- autotuning of the batch options (no counterpart in the reference) ----
  *
  * Times candidate settings of the search-bin size (bin_target: points per

@@ -10,6 +10,7 @@
 //   binRun's loop over work packages    terranni.cpp:394-426 (the batch API)
 // The GL context, framebuffers, renderbuffers and GL/CUDA interop of the
 // reference have no counterpart: the engine works on plain device buffers.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -936,3 +937,5 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
     if (cudaGetLastError() != cudaSuccess) return DNNI_E_CUDA;
     return DNNI_OK;
 }
+
+#include "dnni_segment.cuh"

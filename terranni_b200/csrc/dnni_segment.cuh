@@ -1,0 +1,359 @@
+// dnni_segment.cuh -- the segment driver: one large grid interpolated as
+// tiles with halos (dnni_segment_run).  Included by dnni_engine.cu, whose
+// scratch, planning and launch helpers it uses.
+//
+// Replaces the reference's out-of-core pipeline around performNNI for one
+// grid: TPIE binning of the points into work packages with duplicated borders
+// (terranni.cpp:203-368, border copies terranni.cpp:271-302), the loop over
+// work packages (binRun, terranni.cpp:394-426) and the grid assembly
+// (terranni.cpp:430-488).  Here the points go to HBM once and are bucketed
+// there (buckets of 256 x 256 cells, row-major, so one row of buckets is one
+// contiguous range of the bucketed points); each tile gathers the buckets of
+// its point box into a staging area and a batch of tiles runs through the
+// ordinary launch sequence.
+#pragma once
+
+namespace dnni {
+
+constexpr int kSegBucketCells = 256;        // bucket side in cells
+constexpr int kSegGatherChunk = 1 << 16;    // points per gather block
+
+struct SegGrid {
+    long long ox, oy;   // LAS origin of cell (0,0)
+    long long w;        // bucket side in LAS units
+    int nbx, nby;
+};
+
+// Bucket of a point; points beyond the grid fall into the edge buckets.
+__device__ __forceinline__ int seg_bucket(const SegGrid& g, int x, int y) {
+    const long long rx = (long long)x - g.ox, ry = (long long)y - g.oy;
+    long long bx = rx >= 0 ? rx / g.w : 0, by = ry >= 0 ? ry / g.w : 0;
+    bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
+    by = by < g.nby - 1 ? by : g.nby - 1;
+    return (int)(by * g.nbx + bx);
+}
+
+__global__ void __launch_bounds__(256) k_seg_count(SegGrid g, const int32_t* __restrict__ xyz, int64_t n,
+                                                   unsigned* __restrict__ cnt, unsigned* __restrict__ rank) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        rank[i] = atomicAdd(&cnt[seg_bucket(g, xyz[3 * i], xyz[3 * i + 1])], 1u);
+}
+
+__global__ void __launch_bounds__(256) k_seg_scatter(SegGrid g, const int32_t* __restrict__ xyz, int64_t n,
+                                                     const long long* __restrict__ start,
+                                                     const unsigned* __restrict__ rank, int32_t* __restrict__ oxyz,
+                                                     uint32_t* __restrict__ ogid) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        const long long pos = start[seg_bucket(g, x, y)] + rank[i];
+        oxyz[3 * pos] = x;
+        oxyz[3 * pos + 1] = y;
+        oxyz[3 * pos + 2] = z;
+        ogid[pos] = (uint32_t)i;
+    }
+}
+
+// One block per bucket: bounding box {minx, miny, maxx, maxy} of its points
+// (INT_MAX, INT_MAX, INT_MIN, INT_MIN when empty).
+__global__ void __launch_bounds__(256) k_seg_bbox(const int32_t* __restrict__ sxyz, const long long* __restrict__ start,
+                                                  int4* __restrict__ bbox) {
+    __shared__ int red[4][8];
+    const long long s0 = start[blockIdx.x], s1 = start[blockIdx.x + 1];
+    int mnx = INT_MAX, mny = INT_MAX, mxx = INT_MIN, mxy = INT_MIN;
+    for (long long i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+        const int x = sxyz[3 * i], y = sxyz[3 * i + 1];
+        mnx = min(mnx, x); mxx = max(mxx, x);
+        mny = min(mny, y); mxy = max(mxy, y);
+    }
+    mnx = __reduce_min_sync(0xffffffffu, mnx); mny = __reduce_min_sync(0xffffffffu, mny);
+    mxx = __reduce_max_sync(0xffffffffu, mxx); mxy = __reduce_max_sync(0xffffffffu, mxy);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = mnx; red[1][w] = mny; red[2][w] = mxx; red[3][w] = mxy; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int4 b = make_int4(INT_MAX, INT_MAX, INT_MIN, INT_MIN);
+        for (int k = 0; k < 8; ++k) {
+            b.x = min(b.x, red[0][k]); b.y = min(b.y, red[1][k]);
+            b.z = max(b.z, red[2][k]); b.w = max(b.w, red[3][k]);
+        }
+        bbox[blockIdx.x] = b;
+    }
+}
+
+// Gather of bucket ranges into a tile's staging rows: one block per chunk.
+struct SegChunk {
+    long long src, dst;
+    int count, pad;
+};
+
+__global__ void __launch_bounds__(256) k_seg_gather(const SegChunk* __restrict__ ch, const int32_t* __restrict__ sxyz,
+                                                    const uint32_t* __restrict__ sgid, int32_t* __restrict__ dxyz,
+                                                    uint32_t* __restrict__ dgid) {
+    const SegChunk c = ch[blockIdx.x];
+    const int32_t* s = sxyz + 3 * c.src;
+    int32_t* d = dxyz + 3 * c.dst;
+    for (int k = threadIdx.x; k < 3 * c.count; k += blockDim.x) d[k] = s[k];
+    for (int k = threadIdx.x; k < c.count; k += blockDim.x) dgid[c.dst + k] = sgid[c.src + k];
+}
+
+}  // namespace dnni
+
+namespace {
+
+struct SegTile {
+    int x0, y0, x1, y1;   // core cells [x0,x1) x [y0,y1)
+    int hr;               // raster halo (cells); the point box is the raster +- hr
+};
+
+struct SegBufs {
+    DevBuf xin, sxyz, sgid, rank, cnt, start, bbox, gxyz, ggid, gout, gsite, chunks;
+    void release(dnni_ctx* c) {
+        DevBuf* all[] = {&xin, &sxyz, &sgid, &rank, &cnt, &start, &bbox, &gxyz, &ggid, &gout, &gsite, &chunks};
+        for (DevBuf* b : all) dnni_release(*b, c);
+    }
+};
+
+long long floor_div_ll(long long a, long long b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz, int64_t n, float* h_out,
+                        uint32_t* h_site, dnni_segment_stats* stats, SegBufs& B, Scratch& scr) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    cudaStream_t st = c->stream;
+    const int nbx = (s.ncols + kSegBucketCells - 1) / kSegBucketCells;
+    const int nby = (s.nrows + kSegBucketCells - 1) / kSegBucketCells;
+    const int nb = nbx * nby;
+    const SegGrid G{s.origin_x, s.origin_y, (long long)kSegBucketCells * s.cell_size, nbx, nby};
+    dnni_status rs;
+    const size_t npts = (size_t)std::max<int64_t>(n, 1);
+    if ((rs = dnni_ensure(c, B.xin, 12 * npts)) || (rs = dnni_ensure(c, B.sxyz, 12 * npts)) ||
+        (rs = dnni_ensure(c, B.sgid, 4 * npts)) || (rs = dnni_ensure(c, B.rank, 4 * npts)) ||
+        (rs = dnni_ensure(c, B.cnt, 4 * (size_t)nb)) || (rs = dnni_ensure(c, B.start, 8 * (size_t)(nb + 1))) ||
+        (rs = dnni_ensure(c, B.bbox, 16 * (size_t)nb)))
+        return rs;
+    // 1. upload, in chunks of 64 Mi points
+    CK(cudaEventRecord(c->ev[0], st));
+    const int64_t kUp = 64ll << 20;
+    for (int64_t o = 0; o < n; o += kUp) {
+        const int64_t m = std::min(kUp, n - o);
+        CK(cudaMemcpyAsync((int32_t*)B.xin.p + 3 * o, h_xyz + 3 * o, 12 * (size_t)m, cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaEventRecord(c->ev[1], st));
+    // 2. bucket: count, scan (host), scatter, per-bucket bounding boxes
+    CK(cudaMemsetAsync(B.cnt.p, 0, 4 * (size_t)nb, st));
+    const int grid = c->sm_count * 8;
+    if (n > 0) k_seg_count<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (unsigned*)B.cnt.p, (unsigned*)B.rank.p);
+    std::vector<unsigned> cnt(nb);
+    std::vector<long long> start(nb + 1, 0);
+    CK(cudaMemcpyAsync(cnt.data(), B.cnt.p, 4 * (size_t)nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int b = 0; b < nb; ++b) start[b + 1] = start[b] + cnt[b];
+    CK(cudaMemcpyAsync(B.start.p, start.data(), 8 * (size_t)(nb + 1), cudaMemcpyHostToDevice, st));
+    if (n > 0)
+        k_seg_scatter<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (const long long*)B.start.p,
+                                            (const unsigned*)B.rank.p, (int32_t*)B.sxyz.p, (uint32_t*)B.sgid.p);
+    k_seg_bbox<<<nb, 256, 0, st>>>((const int32_t*)B.sxyz.p, (const long long*)B.start.p, (int4*)B.bbox.p);
+    std::vector<int4> bbox(nb);
+    CK(cudaMemcpyAsync(bbox.data(), B.bbox.p, 16 * (size_t)nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(c->ev[2], st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    float ms_up = 0, ms_bk = 0;
+    cudaEventElapsedTime(&ms_up, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&ms_bk, c->ev[1], c->ev[2]);
+    dnni_release(B.xin, c);     // room for the staging areas
+    dnni_release(B.rank, c);
+
+    // 3. tiles, in batches; a tile whose halo proves too small runs again
+    std::vector<SegTile> queue;
+    for (int y = 0; y < s.nrows; y += s.tile)
+        for (int x = 0; x < s.ncols; x += s.tile)
+            queue.push_back(SegTile{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows), s.halo});
+    const int64_t ntiles = (int64_t)queue.size();
+    int64_t runs = 0, d2h = 0;
+    int max_halo = 0;
+    size_t qi = 0;
+    dnni_batch_options bo{};
+    bo.small_radius = s.small_radius;
+    std::vector<dnni_tile> tl;
+    std::vector<SegChunk> chunks;
+    std::vector<int> order;
+    std::vector<Scalars> hsc;
+    HostBatch hb;
+    DevArrays a;
+    while (qi < queue.size()) {
+        const size_t q1 = std::min(queue.size(), qi + (size_t)s.tiles_per_batch);
+        const int ng = (int)(q1 - qi);
+        tl.assign(ng, dnni_tile{});
+        chunks.clear();
+        std::vector<int> rx0(ng), ry0(ng), rw(ng);
+        std::vector<char> all_buckets(ng), all_raster(ng);
+        int64_t pt = 0, out = 0, site = 0;
+        for (int k = 0; k < ng; ++k) {
+            const SegTile& T = queue[qi + k];
+            const int ax0 = std::max(0, T.x0 - T.hr), ay0 = std::max(0, T.y0 - T.hr);
+            const int ax1 = std::min(s.ncols, T.x1 + T.hr), ay1 = std::min(s.nrows, T.y1 + T.hr);
+            all_raster[k] = ax0 == 0 && ay0 == 0 && ax1 == s.ncols && ay1 == s.nrows;
+            rx0[k] = ax0;
+            ry0[k] = ay0;
+            rw[k] = ax1 - ax0;
+            // point box: the raster +- hr, as a range of buckets
+            const int bx0 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ax0 - T.hr, kSegBucketCells), 0), nbx - 1);
+            const int bx1 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ax1 + T.hr - 1, kSegBucketCells), 0), nbx - 1);
+            const int by0 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ay0 - T.hr, kSegBucketCells), 0), nby - 1);
+            const int by1 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ay1 + T.hr - 1, kSegBucketCells), 0), nby - 1);
+            all_buckets[k] = bx0 == 0 && by0 == 0 && bx1 == nbx - 1 && by1 == nby - 1;
+            const int64_t p0 = pt;
+            int4 ext = make_int4(INT_MAX, INT_MAX, INT_MIN, INT_MIN);
+            for (int by = by0; by <= by1; ++by) {
+                const long long a0 = start[(size_t)by * nbx + bx0], a1 = start[(size_t)by * nbx + bx1 + 1];
+                for (long long o = a0; o < a1; o += kSegGatherChunk) {
+                    const int m = (int)std::min<long long>(kSegGatherChunk, a1 - o);
+                    chunks.push_back(SegChunk{o, pt, m, 0});
+                    pt += m;
+                }
+                for (int bx = bx0; bx <= bx1; ++bx) {
+                    const int4 bb = bbox[(size_t)by * nbx + bx];
+                    if (bb.x > bb.z) continue;
+                    ext.x = std::min(ext.x, bb.x); ext.y = std::min(ext.y, bb.y);
+                    ext.z = std::max(ext.z, bb.z); ext.w = std::max(ext.w, bb.w);
+                }
+            }
+            dnni_tile& t = tl[k];
+            t.wp.ncols = T.x1 - T.x0;
+            t.wp.nrows = T.y1 - T.y0;
+            t.wp.cell_size = s.cell_size;
+            t.wp.origin_x = (int32_t)(s.origin_x + (long long)T.x0 * s.cell_size);
+            t.wp.origin_y = (int32_t)(s.origin_y + (long long)T.y0 * s.cell_size);
+            t.wp.raster_x0 = ax0 - T.x0;
+            t.wp.raster_y0 = ay0 - T.y0;
+            t.wp.raster_x1 = ax1 - T.x0;
+            t.wp.raster_y1 = ay1 - T.y0;
+            t.wp.z_scale = s.z_scale;
+            t.wp.z_offset = s.z_offset;
+            t.wp.nodata = s.nodata;
+            t.pt_offset = p0;
+            t.pt_count = pt - p0;
+            if (pt > p0) {
+                t.ext_x0 = ext.x;
+                t.ext_y0 = ext.y;
+                t.ext_x1 = ext.z;
+                t.ext_y1 = ext.w;
+            }
+            t.out_offset = out;
+            t.site_offset = h_site ? site : -1;
+            out += (int64_t)t.wp.ncols * t.wp.nrows;
+            site += (int64_t)(ax1 - ax0) * (ay1 - ay0);
+        }
+        const size_t gp = (size_t)std::max<int64_t>(pt, 1);
+        if ((rs = dnni_ensure(c, B.gxyz, 12 * gp)) || (rs = dnni_ensure(c, B.ggid, 4 * gp)) ||
+            (rs = dnni_ensure(c, B.gout, 4 * (size_t)std::max<int64_t>(out, 1))) ||
+            (h_site && (rs = dnni_ensure(c, B.gsite, 4 * (size_t)std::max<int64_t>(site, 1)))) ||
+            (rs = dnni_ensure(c, B.chunks, sizeof(SegChunk) * std::max<size_t>(chunks.size(), 1))))
+            return rs;
+        if (!chunks.empty()) {
+            CK(cudaMemcpyAsync(B.chunks.p, chunks.data(), sizeof(SegChunk) * chunks.size(), cudaMemcpyHostToDevice, st));
+            k_seg_gather<<<(int)chunks.size(), 256, 0, st>>>((const SegChunk*)B.chunks.p, (const int32_t*)B.sxyz.p,
+                                                             (const uint32_t*)B.sgid.p, (int32_t*)B.gxyz.p,
+                                                             (uint32_t*)B.ggid.p);
+        }
+        if ((rs = plan_batch(c, tl.data(), ng, bo, hb, order))) return rs;
+        if ((rs = ensure_scratch(c, scr, scratch_sizes(hb), a))) return rs;
+        const BatchTables bt = device_tables(a.tables, ng);
+        if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
+        launch_prologue(hb, bt, a, (const int32_t*)B.gxyz.p, st);
+        launch_body(hb, bt, a, (const int32_t*)B.gxyz.p, (const uint32_t*)B.ggid.p, (float*)B.gout.p,
+                    h_site ? (uint32_t*)B.gsite.p : nullptr, c->sm_count, st, nullptr);
+        CK(cudaGetLastError());
+        hsc.resize(ng);
+        CK(cudaMemcpyAsync(hsc.data(), a.sc, sizeof(Scalars) * ng, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(c->h_ctr, a.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (c->h_ctr->err & kErrRange)
+            return set_err(c, DNNI_E_RANGE, "a point lies beyond +-2^30 LAS units of a tile origin");
+        runs += ng;
+        // accept or rerun each tile (batch position k is tile k: no cost order)
+        for (int k = 0; k < ng; ++k) {
+            const SegTile T = queue[qi + k];
+            int mr2 = -1;
+            for (int l = 0; l < kStatSlots; ++l) mr2 = std::max(mr2, hsc[k].max_r2[l]);
+            // Every raster pixel's nearest-site distance d is below
+            // R = sqrt(R2 + 1) cells.  (B) With R <= hr no point outside the
+            // point box (the raster +- hr) is as near as the site found, so
+            // the found sites are exact.  (A) A pixel p outside the raster
+            // reaching a core cell q needs d(p) >= |p - q|; on the segment p-q
+            // the point c at L-inf distance hr - 1/2 from the core has a
+            // raster pixel p' within sqrt(2)/2, and d is 1-Lipschitz, so
+            // d(p') >= |c - q| - sqrt(2)/2 > hr - 1.21: R <= hr - 2 rules
+            // that out.
+            const double R = std::sqrt((double)mr2 + 1.0);
+            const bool okA = all_raster[k] || R <= T.hr - 2;
+            const bool okB = all_buckets[k] || R <= T.hr;
+            if (!(okA && okB)) {
+                SegTile U = T;
+                U.hr = std::max(2 * T.hr, (int)std::ceil(R) + 3);
+                queue.push_back(U);
+                continue;
+            }
+            max_halo = std::max(max_halo, T.hr);
+            const dnni_tile& t = tl[k];
+            const size_t w = (size_t)t.wp.ncols, h = (size_t)t.wp.nrows;
+            CK(cudaMemcpy2DAsync(h_out + (size_t)T.y0 * s.ncols + T.x0, 4 * (size_t)s.ncols,
+                                 (const float*)B.gout.p + t.out_offset, 4 * w, 4 * w, h, cudaMemcpyDeviceToHost, st));
+            d2h += (int64_t)(4 * w * h);
+            if (h_site) {
+                const uint32_t* src = (const uint32_t*)B.gsite.p + t.site_offset +
+                                      (size_t)(T.y0 - ry0[k]) * rw[k] + (T.x0 - rx0[k]);
+                CK(cudaMemcpy2DAsync(h_site + (size_t)T.y0 * s.ncols + T.x0, 4 * (size_t)s.ncols, src,
+                                     4 * (size_t)rw[k], 4 * w, h, cudaMemcpyDeviceToHost, st));
+                d2h += (int64_t)(4 * w * h);
+            }
+        }
+        CK(cudaStreamSynchronize(st));
+        qi = q1;
+    }
+    if (stats) {
+        stats->ms_total = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        stats->ms_upload = ms_up;
+        stats->ms_bucket = ms_bk;
+        stats->points = n;
+        stats->cells = (int64_t)s.ncols * s.nrows;
+        stats->tiles = ntiles;
+        stats->tile_runs = runs;
+        stats->h2d_bytes = 12 * n;
+        stats->d2h_bytes = d2h;
+        stats->max_halo = max_halo;
+    }
+    return DNNI_OK;
+}
+
+}  // namespace
+
+extern "C" dnni_status dnni_segment_run(dnni_ctx* c, const dnni_segment* sp, const int32_t* h_xyz, int64_t n,
+                                        float* h_out, uint32_t* h_site, dnni_segment_stats* stats) {
+    if (!c || !sp || !h_out || n < 0 || (n > 0 && !h_xyz)) return DNNI_E_INVAL;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    dnni_segment s = *sp;
+    if (!s.tile) s.tile = 2048;
+    if (!s.halo) s.halo = 64;
+    if (!s.tiles_per_batch) s.tiles_per_batch = 16;
+    if (!s.small_radius) s.small_radius = c->s.small_radius;
+    if (s.ncols <= 0 || s.nrows <= 0 || s.ncols > (1 << 20) || s.nrows > (1 << 20))
+        return set_err(c, DNNI_E_INVAL, "grid sides must be in [1, 2^20]");
+    if (s.cell_size <= 0) return set_err(c, DNNI_E_INVAL, "cell_size must be positive");
+    if (s.tile < 32 || s.tile > 16384) return set_err(c, DNNI_E_INVAL, "tile side must be in [32, 16384]");
+    if (s.halo < 2 || s.tiles_per_batch < 1 || s.tiles_per_batch > 4096)
+        return set_err(c, DNNI_E_INVAL, "bad halo or tiles_per_batch");
+    if (s.small_radius < 1 || s.small_radius > kMaxSmallRadius) return set_err(c, DNNI_E_INVAL, "bad small_radius");
+    if ((long long)s.ncols * s.cell_size >= (1LL << 30) || (long long)s.nrows * s.cell_size >= (1LL << 30))
+        return set_err(c, DNNI_E_RANGE, "grid extent must stay below 2^30 LAS units");
+    if ((uint64_t)n >= 0xFFFFFFFFull) return set_err(c, DNNI_E_INVAL, "more points than 32-bit site ids can name");
+    SegBufs B;
+    Scratch scr;
+    const dnni_status rs = segment_run(c, s, h_xyz, n, h_out, h_site, stats, B, scr);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    release_scratch(c, scr);
+    B.release(c);
+    return rs;
+}

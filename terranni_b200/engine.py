@@ -79,6 +79,24 @@ class BatchOptions(ctypes.Structure):
                 ("use_graph", ctypes.c_int32), ("order_by_cost", ctypes.c_int32)]
 
 
+class Segment(ctypes.Structure):
+    _fields_ = [("ncols", ctypes.c_int32), ("nrows", ctypes.c_int32), ("cell_size", ctypes.c_int32),
+                ("origin_x", ctypes.c_int32), ("origin_y", ctypes.c_int32), ("tile", ctypes.c_int32),
+                ("halo", ctypes.c_int32), ("tiles_per_batch", ctypes.c_int32),
+                ("z_scale", ctypes.c_double), ("z_offset", ctypes.c_double),
+                ("nodata", ctypes.c_float), ("small_radius", ctypes.c_int32)]
+
+
+class SegmentStats(ctypes.Structure):
+    _fields_ = [("ms_total", ctypes.c_double), ("ms_upload", ctypes.c_double), ("ms_bucket", ctypes.c_double),
+                ("points", ctypes.c_int64), ("cells", ctypes.c_int64), ("tiles", ctypes.c_int64),
+                ("tile_runs", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+                ("max_halo", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("pad", ctypes.c_int32)]
@@ -118,6 +136,8 @@ _SIGS = {
     "dnni_batch_run_device": ([_P, _P, _P, _P, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
     "dnni_batch_run": ([_P, _P, _P, ctypes.c_int64, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
     "dnni_batch_destroy": ([_P], ctypes.c_int),
+    "dnni_segment_run": ([_P, ctypes.POINTER(Segment), _P, ctypes.c_int64, _P, _P, ctypes.POINTER(SegmentStats)],
+                         ctypes.c_int),
     "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
                              ctypes.POINTER(BatchOptions), ctypes.POINTER(TuneReport)], ctypes.c_int),
 }
@@ -246,6 +266,20 @@ class Engine:
         self._check(lib().dnni_batch_autotune(self._h, arr, len(tiles), _ptr(d_xyz), _ptr(d_gid), int(sample_tiles),
                                               ctypes.byref(opt), ctypes.byref(rep)))
         return {"small_radius": opt.small_radius, "bin_target": opt.bin_target}, rep.as_dict()
+
+    def segment_run(self, xyz, ncols, nrows, cell_size, origin=(0, 0), tile=0, halo=0, tiles_per_batch=0,
+                    z_scale=0.01, z_offset=0.0, nodata=-9999.0, small_radius=0, site=False, out_h=None):
+        """dnni_segment_run: the whole grid from host points in tiles with
+        halos -> (h, site map or None, SegmentStats)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1, 3)
+        sg = Segment(int(ncols), int(nrows), int(cell_size), int(origin[0]), int(origin[1]), int(tile), int(halo),
+                     int(tiles_per_batch), float(z_scale), float(z_offset), float(nodata), int(small_radius))
+        h = out_h if out_h is not None else np.empty((nrows, ncols), np.float32)
+        sm = np.empty((nrows, ncols), np.uint32) if site else None
+        st = SegmentStats()
+        self._check(lib().dnni_segment_run(self._h, ctypes.byref(sg), _ptr(xyz), xyz.shape[0], _ptr(h), _ptr(sm),
+                                           ctypes.byref(st)))
+        return h, sm, st
 
     def clear(self):
         self._check(lib().dnni_clear(self._h))

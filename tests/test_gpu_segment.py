@@ -1,0 +1,64 @@
+"""Segment driver (dnni_segment_run): one grid interpolated as tiles with
+halos, from host memory.
+
+Each tile's halo is checked after it runs and grown until no pixel outside
+its raster can reach its cells and no point outside its point box can be
+nearer than the site found, so the stitched grid must be bit-identical —
+heights and site map, seams included — to one work package covering the
+whole grid (raster = grid), which the other tests tie to the oracle."""
+import numpy as np
+import pytest
+
+from conftest import terrain_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    import torch
+    from terranni_b200 import engine
+    torch.cuda.set_device(0)
+    e = engine.Engine(device=0)
+    yield e
+    e.close()
+
+
+def _cloud(seed, ncols, nrows, n, cell=100, margin=30, lakes=3):
+    """Terrain points over the grid plus a margin of cells on every side."""
+    side = max(ncols, nrows) + 2 * margin
+    xyz = terrain_case(seed, side, n, cell=cell, lakes=lakes, lake_r=(0.02 * side, 0.12 * side))
+    xyz = xyz - np.array([margin * cell, margin * cell, 0], np.int32)
+    return xyz
+
+
+@pytest.mark.parametrize("ncols,nrows,tile,halo,tpb,n,lakes", [
+    (1100, 900, 256, 8, 4, 500_000, 3),     # halos start too small: reruns
+    (700, 650, 200, 64, 1, 150_000, 2),     # odd tiles, one per batch
+    (500, 300, 512, 4, 16, 20_000, 4),      # one tile row, sparse points
+])
+def test_segment_equals_one_work_package(eng, ncols, nrows, tile, halo, tpb, n, lakes):
+    from terranni_b200 import engine
+    ox, oy = 50_000_000, 400_000_000
+    xyz = _cloud(7 + ncols, ncols, nrows, n, lakes=lakes) + np.array([ox, oy, 0], np.int32)
+    ref_h, ref_s, _ = eng.interpolate(engine.make_wp(ncols, nrows, 100, ox, oy), xyz, site=True)
+    h, s, st = eng.segment_run(xyz, ncols, nrows, 100, origin=(ox, oy), tile=tile, halo=halo, tiles_per_batch=tpb,
+                               site=True)
+    assert np.array_equal(s, ref_s)
+    assert np.array_equal(h.view(np.uint32), ref_h.view(np.uint32))
+    ntile = -(-ncols // tile) * -(-nrows // tile)
+    assert st.tiles == ntile and st.tile_runs >= ntile and st.max_halo >= halo
+    assert st.points == xyz.shape[0] and st.cells == ncols * nrows
+
+
+def test_segment_reruns_tiles_whose_halo_is_too_small(eng):
+    ncols = nrows = 600
+    xyz = _cloud(3, ncols, nrows, 40_000, lakes=4)
+    _, _, st = eng.segment_run(xyz, ncols, nrows, 100, tile=128, halo=2)
+    assert st.tile_runs > st.tiles and st.max_halo > 2
+
+
+def test_segment_without_points_is_all_nodata(eng):
+    h, s, st = eng.segment_run(np.zeros((0, 3), np.int32), 300, 200, 100, tile=128, site=True)
+    assert np.all(h == np.float32(-9999.0)) and np.all(s == 0xFFFFFFFF)
+    assert st.tile_runs == st.tiles

@@ -1,0 +1,66 @@
+"""The C++ drop-in for TerraNNI's nni:: interface (include/nni/nni.h).
+
+A caller written against the reference's interface, the way binRun
+(terranni.cpp:394-426) drives it, is compiled against the shim and linked
+with libdnni.so (CPU test); on a GPU its OutPoint stream must equal the
+oracle's heights for the same work package, in the reference's order
+(nni.cpp:836-858: i-major, clipped to the global grid)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "native", "nni_shim_demo.cpp")
+EXE = os.path.join(ROOT, "tests", "native", "nni_shim_demo")
+LIBDIR = os.path.join(ROOT, "terranni_b200")
+
+POINT4D = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("t", "<i4"), ("pad", "<i4")])
+OUTPOINT = np.dtype([("i", "<i4"), ("j", "<i4"), ("h", "<f4")])
+
+
+def build_demo():
+    deps = [SRC, os.path.join(ROOT, "include", "nni", "nni.h"), os.path.join(ROOT, "include", "tpie", "stream.h"),
+            os.path.join(ROOT, "include", "dnni.h"), os.path.join(LIBDIR, "libdnni.so")]
+    if not os.path.exists(EXE) or any(os.path.getmtime(d) > os.path.getmtime(EXE) for d in deps):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), SRC, "-o", EXE,
+               "-L", LIBDIR, "-ldnni", f"-Wl,-rpath,{LIBDIR}"]
+        subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return EXE
+
+
+def test_reference_caller_compiles_and_links_against_the_shim():
+    exe = build_demo()
+    assert os.access(exe, os.X_OK)
+    assert POINT4D.itemsize == 32 and OUTPOINT.itemsize == 12     # nni.h:34-64 layouts
+
+
+@pytest.mark.gpu
+def test_reference_caller_matches_oracle(tmp_path, oracle):
+    from conftest import terrain_case
+    exe = build_demo()
+    ncols, nrows, cell_m, qr = 90, 70, 1.0, 3.0
+    ox, oy = 1000.0, 2000.0                      # exactly representable as float
+    gox, goy, tot_c, tot_r = 10, 20, 95, 85      # the work package's last 5 columns fall outside
+    xyz = terrain_case(17, 100, 6000, lakes=1, lake_r=(5.0, 15.0))
+    xyz = xyz - np.array([500, 500, 0], np.int32)           # some points in the halo, some negative
+    pts = np.zeros(xyz.shape[0], POINT4D)
+    pts["x"] = ox + xyz[:, 0] * 0.01
+    pts["y"] = oy + xyz[:, 1] * 0.01
+    pts["z"] = xyz[:, 2] * 0.01
+    pin, pout = tmp_path / "pts.bin", tmp_path / "out.bin"
+    pts.tofile(pin)
+    r = subprocess.run([exe, str(pin), str(pout), str(ncols), str(nrows), str(cell_m), str(ox), str(oy), str(gox),
+                        str(goy), str(tot_c), str(tot_r), str(qr)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(pout, OUTPOINT)
+    po = int(np.ceil(qr / cell_m)) + 1           # nni.cpp:881-883 with scale 1
+    wp = oracle.make_wp(ncols, nrows, 100, raster=(-po, -po, ncols + po, nrows + po))
+    ref = oracle.interpolate(wp, xyz)["h"]
+    want = [(i + gox, j + goy, ref[j, i]) for i in range(ncols) for j in range(nrows)
+            if i + gox < tot_c and j + goy < tot_r]
+    assert got.shape[0] == len(want)
+    assert np.array_equal(got["i"], np.array([w[0] for w in want], np.int32))
+    assert np.array_equal(got["j"], np.array([w[1] for w in want], np.int32))
+    assert np.array_equal(got["h"].view(np.uint32), np.array([w[2] for w in want], np.float32).view(np.uint32))
