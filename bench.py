@@ -51,7 +51,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["mixed", "tile4096"], default="mixed")
+    ap.add_argument("--workload", choices=["mixed", "tile4096", "segment"], default="mixed")
+    ap.add_argument("--seg-side", type=int, default=32768, help="segment: grid side in cells (1 m)")
+    ap.add_argument("--seg-points", type=int, default=1_500_000_000, help="segment: points")
+    ap.add_argument("--seg-tile", type=int, default=2048)
+    ap.add_argument("--seg-halo", type=int, default=64, help="segment: first raster halo tried (cells)")
+    ap.add_argument("--seg-batch", type=int, default=16, help="segment: tiles per batch")
     ap.add_argument("--tiles", type=int, default=4096, help="tiles of the mixed workload")
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="timed passes of the plain per-tile form (0: skip the plain form)")
@@ -609,9 +614,98 @@ def run_engine_mixed(args, world, rank, local):
         tdist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# segment-streamed grid
+# ---------------------------------------------------------------------------
+
+def run_engine_segment(args, world, rank, local):
+    """One side x side grid at 1 m from points in pinned host memory, through
+    dnni_segment_run (upload, device bucketing, tiles with self-checked halos,
+    download into the host grid).  Each step is one whole call, host to host."""
+    import numpy as np
+    import torch
+    from terranni_b200 import engine, synth
+
+    torch.cuda.set_device(local)
+    tdist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if tdist is not None:
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    side, n = args.seg_side, args.seg_points
+    t0 = time.perf_counter()
+    h_xyz = torch.empty((n, 3), dtype=torch.int32, pin_memory=True)
+    xyz = h_xyz.numpy()
+    synth.config3(seed=BASE_SEED + 3 + 1000 * rank, n=n, side=side, out=xyz)
+    h_out = torch.empty((side, side), dtype=torch.float32, pin_memory=True).numpy()
+    gen_s = time.perf_counter() - t0
+    eng = engine.Engine(device=local)
+    kw = dict(tile=args.seg_tile, halo=args.seg_halo, tiles_per_batch=args.seg_batch, out_h=h_out)
+    for _ in range(args.warmup):
+        eng.segment_run(xyz, side, side, 100, **kw)
+    stats = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if tdist is not None:
+            tdist.barrier()
+        clk.mark("t_start")
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            _, _, st = eng.segment_run(xyz, side, side, 100, **kw)
+            stats.append(st)
+        dt = time.perf_counter() - t1
+        clk.mark("t_end")
+    dt_max = max_over_ranks(dt)
+    cells = side * side
+    value = cells * args.steps * world / dt_max
+    nod = int(np.count_nonzero(h_out == np.float32(-9999.0)))
+    if rank == 0:
+        peak, peak_kind = peaks()
+        ms_step = 1000 * dt_max / args.steps
+        alg = 12 * n + 4 * cells
+        achieved = alg / (ms_step / 1000) / 1e9
+        st = stats[-1]
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32/int64", "data": "synthetic (seeded fBm terrain, clusters, lakes)",
+            "config": {"workload": f"segment{side}", "side": side, "cell_m": 1.0, "points": n, "cells": cells,
+                       "tile": args.seg_tile, "first_halo": args.seg_halo, "tiles_per_batch": args.seg_batch,
+                       "form": "dnni_segment_run: pinned host points -> host grid, timed host to host",
+                       "l2": f"inputs larger than L2 ({12 * n / 1e9:.1f} GB points per step)",
+                       "parallelism": f"dp{world} (independent grids)", "generate_s": round(gen_s, 1)},
+            "segment": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.as_dict().items()},
+            "roofline": {"bound": "hbm", "kernel": "whole segment call, host to host", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes": alg},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(st.h2d_bytes),
+                    "d2h_bytes_per_step": int(st.d2h_bytes),
+                    "note": "the segment call is host to host: its value is already end to end"},
+            "gpu_launches": int(sum(3 + x.batches * (KERNELS_PER_CALL + 1) for x in stats)),
+            "clocks": clk.summary(), "nodata_cells": nod,
+        }), flush=True)
+    eng.close()
+    if tdist is not None:
+        tdist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist()
+    if args.workload == "segment":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "metric": METRIC, "unit": UNIT, "workload": "segment",
+                              "note": "the CPU reference arm is measured on the mixed workload"}))
+            return
+        run_engine_segment(args, world, rank, local)
+        return
     if args.workload == "mixed":
         if args.impl == "reference":
             run_reference_mixed(args, world, rank)

@@ -249,7 +249,7 @@ typedef struct dnni_segment_stats {
     int64_t tile_runs;             /* tiles + reruns with a larger halo */
     int64_t h2d_bytes, d2h_bytes;
     int32_t max_halo;              /* largest raster halo any tile needed */
-    int32_t pad;
+    int32_t batches;               /* launch sequences run */
 } dnni_segment_stats;
 
 /* h_out: nrows x ncols floats, row-major, row 0 = lowest y; h_site (optional):

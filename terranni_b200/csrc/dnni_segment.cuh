@@ -171,6 +171,7 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
             queue.push_back(SegTile{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows), s.halo});
     const int64_t ntiles = (int64_t)queue.size();
     int64_t runs = 0, d2h = 0;
+    int batches = 0;
     int max_halo = 0;
     size_t qi = 0;
     dnni_batch_options bo{};
@@ -272,6 +273,7 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         if (c->h_ctr->err & kErrRange)
             return set_err(c, DNNI_E_RANGE, "a point lies beyond +-2^30 LAS units of a tile origin");
         runs += ng;
+        ++batches;
         // accept or rerun each tile (batch position k is tile k: no cost order)
         for (int k = 0; k < ng; ++k) {
             const SegTile T = queue[qi + k];
@@ -323,6 +325,7 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         stats->h2d_bytes = 12 * n;
         stats->d2h_bytes = d2h;
         stats->max_halo = max_halo;
+        stats->batches = batches;
     }
     return DNNI_OK;
 }

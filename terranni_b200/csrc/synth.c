@@ -108,8 +108,57 @@ int synth_layout(const synth_params *p, double *lakes, double *clusters) {
     return 0;
 }
 
-static inline int in_lake(const double *lakes, int nl, double x, double y) {
-    for (int i = 0; i < nl; i++) {
+/* Uniform grid over the area listing the lakes whose bounding box meets each
+ * grid cell (CSR), so that a point is tested only against the lakes near it;
+ * a point is in a lake when it is strictly inside any lake's circle. */
+typedef struct {
+    int g;            /* cells per side */
+    double cw, ch;    /* cell size */
+    int *start, *ids;
+} lake_grid;
+
+static void lake_grid_build(lake_grid *lg, const double *lakes, int nl, double width, double height) {
+    int g = (int)ceil(sqrt((double)nl));
+    if (g < 1) g = 1;
+    if (g > 1024) g = 1024;
+    lg->g = g;
+    lg->cw = width / g;
+    lg->ch = height / g;
+    lg->start = (int *)calloc((size_t)g * g + 1, sizeof(int));
+    for (int pass = 0; pass < 2; pass++) {
+        int *fill = pass ? (int *)calloc((size_t)g * g, sizeof(int)) : NULL;
+        for (int i = 0; i < nl; i++) {
+            double r = lakes[3 * i + 2];
+            int x0 = (int)floor((lakes[3 * i] - r) / lg->cw), x1 = (int)floor((lakes[3 * i] + r) / lg->cw);
+            int y0 = (int)floor((lakes[3 * i + 1] - r) / lg->ch), y1 = (int)floor((lakes[3 * i + 1] + r) / lg->ch);
+            if (x0 < 0) x0 = 0;
+            if (y0 < 0) y0 = 0;
+            if (x1 > g - 1) x1 = g - 1;
+            if (y1 > g - 1) y1 = g - 1;
+            for (int y = y0; y <= y1; y++)
+                for (int x = x0; x <= x1; x++) {
+                    if (pass == 0) lg->start[y * g + x + 1]++;
+                    else lg->ids[lg->start[y * g + x] + fill[y * g + x]++] = i;
+                }
+        }
+        if (pass == 0) {
+            for (int k = 0; k < g * g; k++) lg->start[k + 1] += lg->start[k];
+            lg->ids = (int *)malloc(sizeof(int) * (size_t)(lg->start[g * g] > 0 ? lg->start[g * g] : 1));
+        } else {
+            free(fill);
+        }
+    }
+}
+
+static inline int in_lake_grid(const lake_grid *lg, const double *lakes, double x, double y) {
+    int cx = (int)(x / lg->cw), cy = (int)(y / lg->ch);
+    if (cx < 0) cx = 0;
+    if (cy < 0) cy = 0;
+    if (cx > lg->g - 1) cx = lg->g - 1;
+    if (cy > lg->g - 1) cy = lg->g - 1;
+    const int c = cy * lg->g + cx;
+    for (int k = lg->start[c]; k < lg->start[c + 1]; k++) {
+        const int i = lg->ids[k];
         double dx = x - lakes[3 * i], dy = y - lakes[3 * i + 1];
         if (dx * dx + dy * dy < lakes[3 * i + 2] * lakes[3 * i + 2]) return 1;
     }
@@ -153,6 +202,8 @@ int synth_generate(const synth_params *p, int32_t *xyz, double *lakes_out) {
             sn[k].phi = 6.283185307179586 * rng_u01(&r);
         }
     }
+    lake_grid lg;
+    lake_grid_build(&lg, lakes, nl, p->width, p->height);
     int64_t n = p->n;
     int64_t xmax_u = (int64_t)floor(p->width / p->xy_scale), ymax_u = (int64_t)floor(p->height / p->xy_scale);
 #ifdef _OPENMP
@@ -173,7 +224,7 @@ int synth_generate(const synth_params *p, int32_t *xyz, double *lakes_out) {
                 y = clus[2 * c + 1] + p->cluster_sigma * rng_normal(&r);
                 if (x < 0 || y < 0 || x >= p->width || y >= p->height) continue;
             }
-            if (!in_lake(lakes, nl, x, y)) break;
+            if (!in_lake_grid(&lg, lakes, x, y)) break;
         }
         double z;
         if (p->kind == 1) {
@@ -192,6 +243,7 @@ int synth_generate(const synth_params *p, int32_t *xyz, double *lakes_out) {
         xyz[3 * i + 1] = (int32_t)Y;
         xyz[3 * i + 2] = (int32_t)llround(z / p->z_scale);
     }
+    free(lg.start); free(lg.ids);
     free(lakes); free(clus);
     return 0;
 }

@@ -95,6 +95,17 @@ def config2(seed=BASE_SEED + 2, n=20_000_000, side=4096):
     return {"xyz": xyz, "ncols": side, "nrows": side, "cell": 100, "lakes": lakes}
 
 
+def config3(seed=BASE_SEED + 3, n=1_500_000_000, side=32768, out=None, nthreads=0):
+    """Segment-streamed grid: side x side cells at 1 m, n points of the config-2
+    generator scaled to the area (64 clusters and 16 lakes per 4096 m square,
+    i.e. 4096 clusters and 1024 lakes at 32768 m)."""
+    scale = (side / 4096.0) ** 2
+    xyz, lakes = generate(seed, n, float(side), float(side), kind="terrain", nclusters=max(1, int(64 * scale)),
+                          frac_uniform=0.7, cluster_sigma=20.0, nlakes=max(1, int(16 * scale)), lake_rmin=50.0,
+                          lake_rmax=400.0, relief=300.0, z_noise=0.1, nthreads=nthreads, out=out)
+    return {"xyz": xyz, "ncols": side, "nrows": side, "cell": 100, "lakes": lakes}
+
+
 def mixed_tiles(count=4096, seed=BASE_SEED + 4, max_points=1_000_000):
     """Tile specs of the mixed batch: side log-uniform in [64, 1024] cells,
     cell 0.5/1/2 m, density log-uniform in [0.05, 8] points/cell,
