@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--seg-side", type=int, default=32768, help="segment: grid side in cells (1 m)")
     ap.add_argument("--seg-points", type=int, default=1_500_000_000, help="segment: points")
     ap.add_argument("--seg-tile", type=int, default=2048)
-    ap.add_argument("--seg-halo", type=int, default=64, help="segment: first raster halo tried (cells)")
+    ap.add_argument("--seg-halo", type=int, default=0,
+                    help="segment: first raster halo tried (cells); 0 = bound from block occupancy")
     ap.add_argument("--seg-batch", type=int, default=16, help="segment: tiles per batch")
     ap.add_argument("--tiles", type=int, default=4096, help="tiles of the mixed workload")
     ap.add_argument("--plain-steps", type=int, default=2,

@@ -235,7 +235,9 @@ typedef struct dnni_segment {
     int32_t cell_size;             /* LAS units */
     int32_t origin_x, origin_y;    /* LAS position of cell (0,0) */
     int32_t tile;                  /* tile side in cells (0 = 2048) */
-    int32_t halo;                  /* first raster halo tried, cells (0 = 64) */
+    int32_t halo;                  /* first raster halo tried, cells; 0 = per tile, from an
+                                      upper bound of the nearest-site distance computed
+                                      from the occupancy of 16-cell blocks */
     int32_t tiles_per_batch;       /* 0 = 16 */
     double z_scale, z_offset;
     float nodata;

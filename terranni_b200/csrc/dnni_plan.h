@@ -175,6 +175,58 @@ inline void batch_add(HostBatch& hb, TileParams t, int64_t pt_off, int64_t out_o
     hb.tiles.push_back(t);
 }
 
+// Squared distance transform in one dimension: d[q] = min_p (q - p)^2 + f[p],
+// from the lower envelope of the parabolas rooted at each p (Felzenszwalb and
+// Huttenlocher, "Distance Transforms of Sampled Functions", Theory of
+// Computing 8, 2012).  Empty entries carry kEdtFar, far above any real
+// squared distance.  v, z: scratch of n and n + 1 entries.
+constexpr double kEdtFar = 1e20;
+inline void edt_1d(const double* f, int n, double* d, int* v, double* z) {
+    if (n <= 0) return;
+    auto meet = [&](int q, int p) { return ((f[q] + (double)q * q) - (f[p] + (double)p * p)) / (2.0 * (q - p)); };
+    int k = 0;
+    v[0] = 0;
+    z[0] = -1e300;
+    z[1] = 1e300;
+    for (int q = 1; q < n; ++q) {
+        double sq = meet(q, v[k]);
+        while (sq <= z[k]) {       // z[0] = -inf ends the loop at k = 0
+            --k;
+            sq = meet(q, v[k]);
+        }
+        ++k;
+        v[k] = q;
+        z[k] = sq;
+        z[k + 1] = 1e300;
+    }
+    k = 0;
+    for (int q = 0; q < n; ++q) {
+        while (z[k + 1] < q) ++k;
+        const double dq = (double)q - v[k];
+        d[q] = dq * dq + f[v[k]];
+    }
+}
+
+// Squared distance (in blocks) from every block of an nx x ny grid to the
+// nearest occupied one (kEdtFar or more when there is none).
+inline std::vector<double> edt_2d(const unsigned char* occ, int nx, int ny) {
+    std::vector<double> g((size_t)nx * ny);
+    const int m = std::max(nx, ny);
+    std::vector<double> f(m), d(m), z(m + 1);
+    std::vector<int> v(m);
+    for (int x = 0; x < nx; ++x) {
+        for (int y = 0; y < ny; ++y) f[y] = occ[(size_t)y * nx + x] ? 0.0 : kEdtFar;
+        edt_1d(f.data(), ny, d.data(), v.data(), z.data());
+        for (int y = 0; y < ny; ++y) g[(size_t)y * nx + x] = d[y];
+    }
+    for (int y = 0; y < ny; ++y) {
+        for (int x = 0; x < nx; ++x) f[x] = g[(size_t)y * nx + x];
+        edt_1d(f.data(), nx, d.data(), v.data(), z.data());
+        for (int x = 0; x < nx; ++x) g[(size_t)y * nx + x] = d[x];
+    }
+    return g;
+}
+
 // Byte layout of the device copy of a batch's tables (one upload).
 struct TableLayout {
     size_t tiles, chunk, scan, blk, sup, row1, rt, ct, grow, total;

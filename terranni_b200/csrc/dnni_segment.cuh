@@ -80,6 +80,19 @@ __global__ void __launch_bounds__(256) k_seg_bbox(const int32_t* __restrict__ sx
     }
 }
 
+// Occupancy of the fine blocks (fw LAS units square) that partition the
+// grid; points beyond the grid are left out.
+__global__ void __launch_bounds__(256) k_seg_occ(SegGrid g, long long fw, int nfx, int nfy,
+                                                 const int32_t* __restrict__ xyz, int64_t n,
+                                                 unsigned char* __restrict__ occ) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const long long rx = (long long)xyz[3 * i] - g.ox, ry = (long long)xyz[3 * i + 1] - g.oy;
+        if (rx < 0 || ry < 0) continue;
+        const long long fx = rx / fw, fy = ry / fw;
+        if (fx < nfx && fy < nfy) occ[fy * nfx + fx] = 1;
+    }
+}
+
 // Gather of bucket ranges into a tile's staging rows: one block per chunk.
 struct SegChunk {
     long long src, dst;
@@ -164,11 +177,50 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     dnni_release(B.xin, c);     // room for the staging areas
     dnni_release(B.rank, c);
 
-    // 3. tiles, in batches; a tile whose halo proves too small runs again
+    // 3. first halo of each tile: unless the caller fixed it, an upper bound
+    // of the nearest-site distance from the occupancy of fine blocks (fb
+    // cells square, at most 4096 per side): a pixel in block b has a site
+    // within fb * (sqrt(edt2(b)) + sqrt(2)) cells, and a halo of that + 3 over
+    // the whole raster passes the exactness check below.
+    const int fb = std::max(16, (std::max(s.ncols, s.nrows) + 4095) / 4096);
+    const int nfx = (s.ncols + fb - 1) / fb, nfy = (s.nrows + fb - 1) / fb;
+    std::vector<double> edt2;
+    if (s.halo == 0) {
+        DevBuf occ_d;
+        if ((rs = dnni_ensure(c, occ_d, (size_t)nfx * nfy))) return rs;
+        CK(cudaMemsetAsync(occ_d.p, 0, (size_t)nfx * nfy, st));
+        if (n > 0)
+            k_seg_occ<<<grid, 256, 0, st>>>(G, (long long)fb * s.cell_size, nfx, nfy, (const int32_t*)B.sxyz.p, n,
+                                            (unsigned char*)occ_d.p);
+        std::vector<unsigned char> occ((size_t)nfx * nfy);
+        CK(cudaMemcpyAsync(occ.data(), occ_d.p, occ.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        dnni_release(occ_d, c);
+        edt2 = edt_2d(occ.data(), nfx, nfy);
+    }
+    const int hmax = std::max(s.ncols, s.nrows) + 4;
+    auto bound_halo = [&](int x0, int y0, int x1, int y1) {   // cells [x0,x1) x [y0,y1), clipped
+        double m = 0;
+        for (int fy = y0 / fb; fy <= (y1 - 1) / fb; ++fy)
+            for (int fx = x0 / fb; fx <= (x1 - 1) / fb; ++fx) m = std::max(m, edt2[(size_t)fy * nfx + fx]);
+        if (m >= kEdtFar / 2) return hmax;
+        return std::min(hmax, (int)std::ceil(fb * (std::sqrt(m) + 1.4143)) + 3);
+    };
     std::vector<SegTile> queue;
     for (int y = 0; y < s.nrows; y += s.tile)
-        for (int x = 0; x < s.ncols; x += s.tile)
-            queue.push_back(SegTile{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows), s.halo});
+        for (int x = 0; x < s.ncols; x += s.tile) {
+            SegTile T{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows), s.halo};
+            if (s.halo == 0) {
+                T.hr = bound_halo(T.x0, T.y0, T.x1, T.y1);
+                for (int it = 0; it < 16; ++it) {    // the bound over the raster the halo implies
+                    const int h2 = bound_halo(std::max(0, T.x0 - T.hr), std::max(0, T.y0 - T.hr),
+                                              std::min(s.ncols, T.x1 + T.hr), std::min(s.nrows, T.y1 + T.hr));
+                    if (h2 <= T.hr) break;
+                    T.hr = h2;
+                }
+            }
+            queue.push_back(T);
+        }
     const int64_t ntiles = (int64_t)queue.size();
     int64_t runs = 0, d2h = 0;
     int batches = 0;
@@ -339,14 +391,13 @@ extern "C" dnni_status dnni_segment_run(dnni_ctx* c, const dnni_segment* sp, con
     DeviceGuard g(c->device);
     dnni_segment s = *sp;
     if (!s.tile) s.tile = 2048;
-    if (!s.halo) s.halo = 64;
     if (!s.tiles_per_batch) s.tiles_per_batch = 16;
     if (!s.small_radius) s.small_radius = c->s.small_radius;
     if (s.ncols <= 0 || s.nrows <= 0 || s.ncols > (1 << 20) || s.nrows > (1 << 20))
         return set_err(c, DNNI_E_INVAL, "grid sides must be in [1, 2^20]");
     if (s.cell_size <= 0) return set_err(c, DNNI_E_INVAL, "cell_size must be positive");
     if (s.tile < 32 || s.tile > 16384) return set_err(c, DNNI_E_INVAL, "tile side must be in [32, 16384]");
-    if (s.halo < 2 || s.tiles_per_batch < 1 || s.tiles_per_batch > 4096)
+    if (s.halo < 0 || s.halo == 1 || s.tiles_per_batch < 1 || s.tiles_per_batch > 4096)
         return set_err(c, DNNI_E_INVAL, "bad halo or tiles_per_batch");
     if (s.small_radius < 1 || s.small_radius > kMaxSmallRadius) return set_err(c, DNNI_E_INVAL, "bad small_radius");
     if ((long long)s.ncols * s.cell_size >= (1LL << 30) || (long long)s.nrows * s.cell_size >= (1LL << 30))

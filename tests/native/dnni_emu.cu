@@ -249,3 +249,9 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
 
 // exposes the device helpers r2_of and udiv32 for direct tests
 extern "C" int emu_r2_of(long long d2, long long cs2, int cap) { return r2_of(d2, cs2, cap); }
+
+// exposes the planning distance transform used for the segment driver's halos
+extern "C" void emu_edt_2d(const unsigned char* occ, int nx, int ny, double* out) {
+    const std::vector<double> g = edt_2d(occ, nx, ny);
+    for (size_t k = 0; k < g.size(); ++k) out[k] = g[k];
+}

@@ -36,6 +36,7 @@ def _cloud(seed, ncols, nrows, n, cell=100, margin=30, lakes=3):
     (1100, 900, 256, 8, 4, 500_000, 3),     # halos start too small: reruns
     (700, 650, 200, 64, 1, 150_000, 2),     # odd tiles, one per batch
     (500, 300, 512, 4, 16, 20_000, 4),      # one tile row, sparse points
+    (1300, 1000, 256, 0, 8, 400_000, 4),    # halos from the occupancy bound
 ])
 def test_segment_equals_one_work_package(eng, ncols, nrows, tile, halo, tpb, n, lakes):
     from terranni_b200 import engine
@@ -48,6 +49,8 @@ def test_segment_equals_one_work_package(eng, ncols, nrows, tile, halo, tpb, n, 
     assert np.array_equal(h.view(np.uint32), ref_h.view(np.uint32))
     ntile = -(-ncols // tile) * -(-nrows // tile)
     assert st.tiles == ntile and st.tile_runs >= ntile and st.max_halo >= halo
+    if halo == 0:                            # the bound is an upper bound: no reruns
+        assert st.tile_runs == ntile
     assert st.points == xyz.shape[0] and st.cells == ncols * nrows
 
 
