@@ -259,6 +259,73 @@ typedef struct dnni_segment_stats {
 dnni_status dnni_segment_run(dnni_ctx *ctx, const dnni_segment *seg, const int32_t *h_xyz, int64_t n,
                              float *h_out, uint32_t *h_site, dnni_segment_stats *stats);
 
+/* ---- serving: DEM requests against a resident point cloud ----
+ *
+ * No counterpart in the reference (its CLI interpolates one whole dataset per
+ * run, terranni.cpp:544-700).  dnni_server_create uploads and buckets a
+ * point cloud once and keeps it in HBM; requests (a bounding box at a cell
+ * size) are submitted at any time from any thread and run by a server thread
+ * with continuous batching: queued requests are admitted in arrival order
+ * into the next batch while their device footprint fits a free slot's arena,
+ * and up to `slots` batches are in flight at once on separate streams.
+ *
+ * A request's result is the window of the interpolation whose raster is the
+ * cloud's bounding box on the request's cell lattice, with every point of
+ * the cloud as a site: its raster halo and point box come from an upper bound
+ * of the nearest-site distance (exact distance transform of the occupancy of
+ * fine blocks) and are checked after the run as in dnni_segment_run (a
+ * request that fails the check runs again with a larger halo).  So a result
+ * does not depend on which other requests share its batch. */
+typedef struct dnni_server_options {
+    int32_t bucket;                /* bucket side, LAS units (0 = 25600) */
+    int32_t fine;                  /* fine block side of the halo bound, LAS units
+                                      (0 = at least 1600, at most 4096 blocks a side) */
+    int32_t slots;                 /* batches in flight (0 = 2) */
+    int32_t max_batch;             /* requests per batch (0 = 64) */
+    uint64_t slot_bytes;           /* device arena of each slot (0 = 16 GiB) */
+    int32_t small_radius, bin_target;   /* 0 = the context's settings */
+} dnni_server_options;
+
+typedef struct dnni_server dnni_server;
+
+typedef struct dnni_request {
+    int32_t x0, y0;                /* absolute LAS position of cell (0,0) */
+    int32_t ncols, nrows;          /* cells, each side <= 32767 */
+    int32_t cell_size;             /* LAS units */
+    int32_t pad0;
+    double z_scale, z_offset;
+    float nodata;
+    int32_t pad1;
+    float *out_h;                  /* host, nrows x ncols; must stay valid until the wait */
+    uint32_t *out_site;            /* optional host site map, nrows x ncols */
+} dnni_request;
+
+typedef struct dnni_request_result {
+    int32_t status;                /* DNNI_OK or why the request failed */
+    int32_t halo;                  /* raster halo used, cells */
+    double ms_queue;               /* submit -> launch */
+    double ms_latency;             /* submit -> result in host memory */
+    int64_t points, cells;
+    int32_t batch_size, runs;      /* requests in its batch; runs (1 + reruns) */
+} dnni_request_result;
+
+typedef struct dnni_server_stats {
+    int64_t submitted, completed, failed, batches, cells, points;
+    int64_t resident_bytes;        /* the bucketed cloud */
+    double ms_build;               /* upload, bucketing and bound at creation */
+} dnni_server_stats;
+
+dnni_status dnni_server_create(dnni_ctx *ctx, const int32_t *h_xyz, int64_t n, const dnni_server_options *options,
+                               dnni_server **out);
+/* Queues a request; returns at once with its ticket. Thread-safe. */
+dnni_status dnni_server_submit(dnni_server *srv, const dnni_request *req, uint64_t *ticket);
+/* Waits up to timeout_s (< 0: forever) for the ticket's result; DNNI_E_TIMEOUT
+ * leaves the ticket pending.  Each ticket is waited for once. Thread-safe. */
+dnni_status dnni_server_wait(dnni_server *srv, uint64_t ticket, double timeout_s, dnni_request_result *result);
+dnni_status dnni_server_get_stats(dnni_server *srv, dnni_server_stats *stats);
+/* Finishes the queued requests, stops the server thread, frees the cloud. */
+dnni_status dnni_server_destroy(dnni_server *srv);
+
 /* ---- autotuning of the batch options (no counterpart in the reference) ----
  *
  * Times candidate settings of the search-bin size (bin_target: points per

@@ -939,3 +939,4 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
 }
 
 #include "dnni_segment.cuh"
+#include "dnni_server.cuh"

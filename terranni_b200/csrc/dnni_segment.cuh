@@ -93,6 +93,22 @@ __global__ void __launch_bounds__(256) k_seg_occ(SegGrid g, long long fw, int nf
     }
 }
 
+// Bounding box {minx, miny, maxx, maxy} of n points (ext pre-set to empty).
+__global__ void __launch_bounds__(256) k_seg_extent(const int32_t* __restrict__ xyz, int64_t n, int* __restrict__ ext) {
+    int mnx = INT_MAX, mny = INT_MAX, mxx = INT_MIN, mxy = INT_MIN;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = xyz[3 * i], y = xyz[3 * i + 1];
+        mnx = min(mnx, x); mxx = max(mxx, x);
+        mny = min(mny, y); mxy = max(mxy, y);
+    }
+    mnx = __reduce_min_sync(0xffffffffu, mnx); mny = __reduce_min_sync(0xffffffffu, mny);
+    mxx = __reduce_max_sync(0xffffffffu, mxx); mxy = __reduce_max_sync(0xffffffffu, mxy);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&ext[0], mnx); atomicMin(&ext[1], mny);
+        atomicMax(&ext[2], mxx); atomicMax(&ext[3], mxy);
+    }
+}
+
 // Gather of bucket ranges into a tile's staging rows: one block per chunk.
 struct SegChunk {
     long long src, dst;
@@ -128,6 +144,85 @@ struct SegBufs {
 
 long long floor_div_ll(long long a, long long b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
+// Uploads n points (chunks of 64 Mi) and buckets them on the device by G:
+// afterwards B.sxyz / B.sgid hold the points in bucket order (gid = input
+// index), start / bbox the bucket ranges and bounding boxes; B.xin and
+// B.rank are released again.
+dnni_status upload_points(dnni_ctx* c, cudaStream_t st, const int32_t* h_xyz, int64_t n, SegBufs& B) {
+    dnni_status rs;
+    if ((rs = dnni_ensure(c, B.xin, 12 * (size_t)std::max<int64_t>(n, 1)))) return rs;
+    CK(cudaEventRecord(c->ev[0], st));
+    const int64_t kUp = 64ll << 20;
+    for (int64_t o = 0; o < n; o += kUp) {
+        const int64_t m = std::min(kUp, n - o);
+        CK(cudaMemcpyAsync((int32_t*)B.xin.p + 3 * o, h_xyz + 3 * o, 12 * (size_t)m, cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaEventRecord(c->ev[1], st));
+    return DNNI_OK;
+}
+
+// Buckets the n points already uploaded to B.xin (see bucket_points).
+dnni_status bucket_uploaded(dnni_ctx* c, cudaStream_t st, const SegGrid& G, int64_t n, SegBufs& B,
+                            std::vector<long long>& start, std::vector<int4>& bbox, float* ms_up, float* ms_bk) {
+    const int nb = G.nbx * G.nby;
+    dnni_status rs;
+    const size_t npts = (size_t)std::max<int64_t>(n, 1);
+    if ((rs = dnni_ensure(c, B.sxyz, 12 * npts)) || (rs = dnni_ensure(c, B.sgid, 4 * npts)) ||
+        (rs = dnni_ensure(c, B.rank, 4 * npts)) || (rs = dnni_ensure(c, B.cnt, 4 * (size_t)nb)) ||
+        (rs = dnni_ensure(c, B.start, 8 * (size_t)(nb + 1))) || (rs = dnni_ensure(c, B.bbox, 16 * (size_t)nb)))
+        return rs;
+    CK(cudaMemsetAsync(B.cnt.p, 0, 4 * (size_t)nb, st));
+    const int grid = c->sm_count * 8;
+    if (n > 0) k_seg_count<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (unsigned*)B.cnt.p, (unsigned*)B.rank.p);
+    std::vector<unsigned> cnt(nb);
+    start.assign(nb + 1, 0);
+    CK(cudaMemcpyAsync(cnt.data(), B.cnt.p, 4 * (size_t)nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int b = 0; b < nb; ++b) start[b + 1] = start[b] + cnt[b];
+    CK(cudaMemcpyAsync(B.start.p, start.data(), 8 * (size_t)(nb + 1), cudaMemcpyHostToDevice, st));
+    if (n > 0)
+        k_seg_scatter<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (const long long*)B.start.p,
+                                            (const unsigned*)B.rank.p, (int32_t*)B.sxyz.p, (uint32_t*)B.sgid.p);
+    k_seg_bbox<<<nb, 256, 0, st>>>((const int32_t*)B.sxyz.p, (const long long*)B.start.p, (int4*)B.bbox.p);
+    bbox.resize(nb);
+    CK(cudaMemcpyAsync(bbox.data(), B.bbox.p, 16 * (size_t)nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(c->ev[2], st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    cudaEventElapsedTime(ms_up, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(ms_bk, c->ev[1], c->ev[2]);
+    dnni_release(B.xin, c);
+    dnni_release(B.rank, c);
+    return DNNI_OK;
+}
+
+dnni_status bucket_points(dnni_ctx* c, cudaStream_t st, const SegGrid& G, const int32_t* h_xyz, int64_t n, SegBufs& B,
+                          std::vector<long long>& start, std::vector<int4>& bbox, float* ms_up, float* ms_bk) {
+    dnni_status rs = upload_points(c, st, h_xyz, n, B);
+    if (rs) return rs;
+    return bucket_uploaded(c, st, G, n, B, start, bbox, ms_up, ms_bk);
+}
+
+// Squared distance, in fine blocks (fw LAS units square, nfx x nfy from the
+// grid origin), from every fine block to the nearest one holding a point.
+dnni_status occupancy_edt(dnni_ctx* c, cudaStream_t st, const SegGrid& G, long long fw, int nfx, int nfy,
+                          const SegBufs& B, int64_t n, std::vector<double>& edt2) {
+    DevBuf occ_d;
+    dnni_status rs;
+    if ((rs = dnni_ensure(c, occ_d, (size_t)nfx * nfy))) return rs;
+    std::vector<unsigned char> occ((size_t)nfx * nfy);
+    cudaError_t e = cudaMemsetAsync(occ_d.p, 0, occ.size(), st);
+    if (e == cudaSuccess && n > 0)
+        k_seg_occ<<<c->sm_count * 8, 256, 0, st>>>(G, fw, nfx, nfy, (const int32_t*)B.sxyz.p, n,
+                                                   (unsigned char*)occ_d.p);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(occ.data(), occ_d.p, occ.size(), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    dnni_release(occ_d, c);
+    if (e != cudaSuccess) return cuda_err(c, e, "occupancy");
+    edt2 = edt_2d(occ.data(), nfx, nfy);
+    return DNNI_OK;
+}
+
 dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz, int64_t n, float* h_out,
                         uint32_t* h_site, dnni_segment_stats* stats, SegBufs& B, Scratch& scr) {
     using clk = std::chrono::steady_clock;
@@ -138,44 +233,10 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     const int nb = nbx * nby;
     const SegGrid G{s.origin_x, s.origin_y, (long long)kSegBucketCells * s.cell_size, nbx, nby};
     dnni_status rs;
-    const size_t npts = (size_t)std::max<int64_t>(n, 1);
-    if ((rs = dnni_ensure(c, B.xin, 12 * npts)) || (rs = dnni_ensure(c, B.sxyz, 12 * npts)) ||
-        (rs = dnni_ensure(c, B.sgid, 4 * npts)) || (rs = dnni_ensure(c, B.rank, 4 * npts)) ||
-        (rs = dnni_ensure(c, B.cnt, 4 * (size_t)nb)) || (rs = dnni_ensure(c, B.start, 8 * (size_t)(nb + 1))) ||
-        (rs = dnni_ensure(c, B.bbox, 16 * (size_t)nb)))
-        return rs;
-    // 1. upload, in chunks of 64 Mi points
-    CK(cudaEventRecord(c->ev[0], st));
-    const int64_t kUp = 64ll << 20;
-    for (int64_t o = 0; o < n; o += kUp) {
-        const int64_t m = std::min(kUp, n - o);
-        CK(cudaMemcpyAsync((int32_t*)B.xin.p + 3 * o, h_xyz + 3 * o, 12 * (size_t)m, cudaMemcpyHostToDevice, st));
-    }
-    CK(cudaEventRecord(c->ev[1], st));
-    // 2. bucket: count, scan (host), scatter, per-bucket bounding boxes
-    CK(cudaMemsetAsync(B.cnt.p, 0, 4 * (size_t)nb, st));
-    const int grid = c->sm_count * 8;
-    if (n > 0) k_seg_count<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (unsigned*)B.cnt.p, (unsigned*)B.rank.p);
-    std::vector<unsigned> cnt(nb);
-    std::vector<long long> start(nb + 1, 0);
-    CK(cudaMemcpyAsync(cnt.data(), B.cnt.p, 4 * (size_t)nb, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (int b = 0; b < nb; ++b) start[b + 1] = start[b] + cnt[b];
-    CK(cudaMemcpyAsync(B.start.p, start.data(), 8 * (size_t)(nb + 1), cudaMemcpyHostToDevice, st));
-    if (n > 0)
-        k_seg_scatter<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (const long long*)B.start.p,
-                                            (const unsigned*)B.rank.p, (int32_t*)B.sxyz.p, (uint32_t*)B.sgid.p);
-    k_seg_bbox<<<nb, 256, 0, st>>>((const int32_t*)B.sxyz.p, (const long long*)B.start.p, (int4*)B.bbox.p);
-    std::vector<int4> bbox(nb);
-    CK(cudaMemcpyAsync(bbox.data(), B.bbox.p, 16 * (size_t)nb, cudaMemcpyDeviceToHost, st));
-    CK(cudaEventRecord(c->ev[2], st));
-    CK(cudaStreamSynchronize(st));
-    CK(cudaGetLastError());
+    std::vector<long long> start;
+    std::vector<int4> bbox;
     float ms_up = 0, ms_bk = 0;
-    cudaEventElapsedTime(&ms_up, c->ev[0], c->ev[1]);
-    cudaEventElapsedTime(&ms_bk, c->ev[1], c->ev[2]);
-    dnni_release(B.xin, c);     // room for the staging areas
-    dnni_release(B.rank, c);
+    if ((rs = bucket_points(c, st, G, h_xyz, n, B, start, bbox, &ms_up, &ms_bk))) return rs;
 
     // 3. first halo of each tile: unless the caller fixed it, an upper bound
     // of the nearest-site distance from the occupancy of fine blocks (fb
@@ -185,19 +246,7 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     const int fb = std::max(16, (std::max(s.ncols, s.nrows) + 4095) / 4096);
     const int nfx = (s.ncols + fb - 1) / fb, nfy = (s.nrows + fb - 1) / fb;
     std::vector<double> edt2;
-    if (s.halo == 0) {
-        DevBuf occ_d;
-        if ((rs = dnni_ensure(c, occ_d, (size_t)nfx * nfy))) return rs;
-        CK(cudaMemsetAsync(occ_d.p, 0, (size_t)nfx * nfy, st));
-        if (n > 0)
-            k_seg_occ<<<grid, 256, 0, st>>>(G, (long long)fb * s.cell_size, nfx, nfy, (const int32_t*)B.sxyz.p, n,
-                                            (unsigned char*)occ_d.p);
-        std::vector<unsigned char> occ((size_t)nfx * nfy);
-        CK(cudaMemcpyAsync(occ.data(), occ_d.p, occ.size(), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        dnni_release(occ_d, c);
-        edt2 = edt_2d(occ.data(), nfx, nfy);
-    }
+    if (s.halo == 0 && (rs = occupancy_edt(c, st, G, (long long)fb * s.cell_size, nfx, nfy, B, n, edt2))) return rs;
     const int hmax = std::max(s.ncols, s.nrows) + 4;
     auto bound_halo = [&](int x0, int y0, int x1, int y1) {   // cells [x0,x1) x [y0,y1), clipped
         double m = 0;

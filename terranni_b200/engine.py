@@ -97,6 +97,37 @@ class SegmentStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("bucket", ctypes.c_int32), ("fine", ctypes.c_int32), ("slots", ctypes.c_int32),
+                ("max_batch", ctypes.c_int32), ("slot_bytes", ctypes.c_uint64), ("small_radius", ctypes.c_int32),
+                ("bin_target", ctypes.c_int32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("x0", ctypes.c_int32), ("y0", ctypes.c_int32), ("ncols", ctypes.c_int32), ("nrows", ctypes.c_int32),
+                ("cell_size", ctypes.c_int32), ("pad0", ctypes.c_int32), ("z_scale", ctypes.c_double),
+                ("z_offset", ctypes.c_double), ("nodata", ctypes.c_float), ("pad1", ctypes.c_int32),
+                ("out_h", ctypes.c_void_p), ("out_site", ctypes.c_void_p)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("halo", ctypes.c_int32), ("ms_queue", ctypes.c_double),
+                ("ms_latency", ctypes.c_double), ("points", ctypes.c_int64), ("cells", ctypes.c_int64),
+                ("batch_size", ctypes.c_int32), ("runs", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("batches", ctypes.c_int64), ("cells", ctypes.c_int64), ("points", ctypes.c_int64),
+                ("resident_bytes", ctypes.c_int64), ("ms_build", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("pad", ctypes.c_int32)]
@@ -138,6 +169,11 @@ _SIGS = {
     "dnni_batch_destroy": ([_P], ctypes.c_int),
     "dnni_segment_run": ([_P, ctypes.POINTER(Segment), _P, ctypes.c_int64, _P, _P, ctypes.POINTER(SegmentStats)],
                          ctypes.c_int),
+    "dnni_server_create": ([_P, _P, ctypes.c_int64, ctypes.POINTER(ServerOptions), ctypes.POINTER(_P)], ctypes.c_int),
+    "dnni_server_submit": ([_P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    "dnni_server_wait": ([_P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestResult)], ctypes.c_int),
+    "dnni_server_get_stats": ([_P, ctypes.POINTER(ServerStats)], ctypes.c_int),
+    "dnni_server_destroy": ([_P], ctypes.c_int),
     "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
                              ctypes.POINTER(BatchOptions), ctypes.POINTER(TuneReport)], ctypes.c_int),
 }
@@ -281,6 +317,10 @@ class Engine:
                                            ctypes.byref(st)))
         return h, sm, st
 
+    def server(self, xyz, **options):
+        """dnni_server_create over host points (absolute LAS xyz) -> Server."""
+        return Server(self, xyz, **options)
+
     def clear(self):
         self._check(lib().dnni_clear(self._h))
 
@@ -343,3 +383,73 @@ class Batch:
         self._eng._check(lib().dnni_batch_run(self._h, _ptr(xyz), _ptr(gid), xyz.shape[0], _ptr(out_h),
                                               _ptr(out_site), ctypes.byref(st) if st is not None else None))
         return st
+
+
+class Server:
+    """DEM requests against a resident cloud (dnni_server_*)."""
+
+    def __init__(self, eng: Engine, xyz, bucket=0, fine=0, slots=0, max_batch=0, slot_bytes=0, small_radius=0,
+                 bin_target=0):
+        import threading
+        self._eng = eng
+        xyz = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1, 3)
+        o = ServerOptions(int(bucket), int(fine), int(slots), int(max_batch), int(slot_bytes), int(small_radius),
+                          int(bin_target))
+        h = _P()
+        eng._check(lib().dnni_server_create(eng.handle, _ptr(xyz), xyz.shape[0], ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._bufs = {}
+        self._mu = threading.Lock()
+
+    def submit(self, x0, y0, ncols, nrows, cell_size, site=False, z_scale=0.01, z_offset=0.0, nodata=-9999.0,
+               out_h=None, out_site=None):
+        """Queues a request; returns its ticket.  Buffers (numpy, pinned or
+        not) are kept alive until wait() returns them."""
+        h = out_h if out_h is not None else np.empty((nrows, ncols), np.float32)
+        sm = out_site if out_site is not None else (np.empty((nrows, ncols), np.uint32) if site else None)
+        r = Request(int(x0), int(y0), int(ncols), int(nrows), int(cell_size), 0, float(z_scale), float(z_offset),
+                    float(nodata), 0, _ptr(h), _ptr(sm))
+        t = ctypes.c_uint64()
+        rc = lib().dnni_server_submit(self._h, ctypes.byref(r), ctypes.byref(t))
+        if rc:
+            raise DnniError(rc, "dnni_server_submit")
+        with self._mu:
+            self._bufs[t.value] = (h, sm)
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        """-> (heights, site map or None, result dict); raises DnniError when
+        the request failed (its result dict is on the exception)."""
+        res = RequestResult()
+        rc = lib().dnni_server_wait(self._h, int(ticket), float(timeout), ctypes.byref(res))
+        if rc == 3:                      # DNNI_E_TIMEOUT: still pending
+            raise DnniError(rc, "timeout")
+        with self._mu:
+            h, sm = self._bufs.pop(ticket)
+        if rc:
+            e = DnniError(rc, "request failed")
+            e.result = res.as_dict()
+            raise e
+        return h, sm, res.as_dict()
+
+    def stats(self):
+        st = ServerStats()
+        self._eng._check(lib().dnni_server_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self._h:
+            lib().dnni_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
