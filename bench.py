@@ -51,7 +51,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["mixed", "tile4096", "segment"], default="mixed")
+    ap.add_argument("--workload", choices=["mixed", "tile4096", "segment", "served"], default="mixed")
+    ap.add_argument("--srv-points", type=int, default=2_000_000_000, help="served: cloud points")
+    ap.add_argument("--srv-side", type=float, default=64000.0, help="served: cloud side, metres")
+    ap.add_argument("--srv-requests", type=int, default=200, help="served: requests per arrival rate")
+    ap.add_argument("--srv-rates", default="100,1000,5000,20000", help="served: Poisson arrival rates, 1/s")
     ap.add_argument("--seg-side", type=int, default=32768, help="segment: grid side in cells (1 m)")
     ap.add_argument("--seg-points", type=int, default=1_500_000_000, help="segment: points")
     ap.add_argument("--seg-tile", type=int, default=2048)
@@ -697,9 +701,130 @@ def run_engine_segment(args, world, rank, local):
         tdist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# served: DEM requests against a resident cloud
+# ---------------------------------------------------------------------------
+
+def run_engine_served(args, world, rank, local):
+    """A resident cloud on each GPU (per-rank seed) and a Poisson stream of
+    box requests per arrival rate, submitted by a client thread at their
+    arrival times and collected by another; latency = submit -> heights in
+    (pinned) host memory.  Each rank serves its own stream."""
+    import numpy as np
+    import torch
+    from terranni_b200 import engine, synth
+
+    torch.cuda.set_device(local)
+    tdist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if tdist is not None:
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.srv_points
+    t0 = time.perf_counter()
+    h_xyz = torch.empty((n, 3), dtype=torch.int32, pin_memory=True)
+    xyz = h_xyz.numpy()
+    synth.config5(seed=BASE_SEED + 5 + 1000 * rank, n=n, side_m=args.srv_side, out=xyz)
+    gen_s = time.perf_counter() - t0
+    reqs = synth.served_requests(args.srv_requests, seed=BASE_SEED + 6 + 1000 * rank, side_m=args.srv_side)
+    sizes = [r["ncols"] * r["nrows"] for r in reqs]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    pool = torch.empty(int(offs[-1]), dtype=torch.float32, pin_memory=True).numpy()
+    outs = [pool[offs[k]:offs[k + 1]].reshape(reqs[k]["nrows"], reqs[k]["ncols"]) for k in range(len(reqs))]
+    eng = engine.Engine(device=local)
+    srv = eng.server(xyz)
+    rates = [float(x) for x in args.srv_rates.split(",") if x]
+    rng = np.random.default_rng(BASE_SEED + 7 + rank)
+    results = []
+    with ClockSampler(local) as clk:
+        # warm-up: a few requests alone
+        for k in range(min(args.warmup, len(reqs))):
+            srv.wait(srv.submit(**reqs[k], out_h=outs[k]), timeout=600)
+        clk.mark("t_start")
+        for rate in rates:
+            if tdist is not None:
+                tdist.barrier()
+            gaps = rng.exponential(1.0 / rate, len(reqs))
+            arrive = np.cumsum(gaps) - gaps[0]
+            tickets = [None] * len(reqs)
+            lat = [None] * len(reqs)
+            ready = threading.Semaphore(0)
+
+            def client():
+                base = time.perf_counter()
+                for k, r in enumerate(reqs):
+                    d = base + arrive[k] - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    tickets[k] = srv.submit(**r, out_h=outs[k])
+                    ready.release()
+
+            c = threading.Thread(target=client)
+            t_first = time.perf_counter()
+            c.start()
+            for k in range(len(reqs)):
+                ready.acquire()
+                _, _, res = srv.wait(tickets[k], timeout=600)
+                lat[k] = res
+            t_last = time.perf_counter()
+            c.join()
+            span = max_over_ranks(t_last - t_first)
+            cells = sum(sizes)
+            ms = np.array([x["ms_latency"] for x in lat])
+            results.append({"rate_per_s": rate, "requests": len(reqs), "cells": cells,
+                            "cells_per_s": cells * world / span, "p50_ms": float(np.percentile(ms, 50)),
+                            "p99_ms": float(np.percentile(ms, 99)), "max_ms": float(ms.max()),
+                            "mean_batch": float(np.mean([x["batch_size"] for x in lat])),
+                            "queue_p50_ms": float(np.percentile([x["ms_queue"] for x in lat], 50))})
+        clk.mark("t_end")
+    st = srv.stats()
+    srv.close()
+    if rank == 0:
+        best = max(results, key=lambda r: r["cells_per_s"])
+        top = results[-1]
+        peak, peak_kind = peaks()
+        print(json.dumps({
+            "metric": METRIC, "value": top["cells_per_s"], "unit": UNIT, "n_gpus": world,
+            "steps": len(rates), "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64",
+            "data": "synthetic (seeded fBm terrain, clusters, lakes)",
+            "config": {"workload": "served", "cloud_points": n, "cloud_side_m": args.srv_side,
+                       "requests_per_rate": len(reqs), "request_side_m": "log-U[128, 8192]",
+                       "cell_m": [0.5, 1, 2], "rates": rates, "generate_s": round(gen_s, 1),
+                       "form": "continuous batching over 2 slots of 16 GiB, footprint admission",
+                       "parallelism": f"dp{world} (independent servers)"},
+            "served": results, "best_cells_per_s": best["cells_per_s"],
+            "latency": {"p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "at_rate": top["rate_per_s"]},
+            "server": st,
+            "e2e": {"value": top["cells_per_s"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(4 * sum(sizes)),
+                    "note": "requests return heights in host memory: the value is already end to end"},
+            "roofline": {"bound": "hbm", "kernel": "whole request path", "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "achieved": None, "frac": None, "traffic": None},
+            "gpu_launches": int(st["batches"] * (KERNELS_PER_CALL + 1)), "clocks": clk.summary(),
+        }), flush=True)
+    eng.close()
+    if tdist is not None:
+        tdist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist()
+    if args.workload == "served":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "metric": METRIC, "unit": UNIT, "workload": "served",
+                              "note": "the CPU reference arm is measured on the mixed workload"}))
+            return
+        run_engine_served(args, world, rank, local)
+        return
     if args.workload == "segment":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "metric": METRIC, "unit": UNIT, "workload": "segment",

@@ -106,6 +106,34 @@ def config3(seed=BASE_SEED + 3, n=1_500_000_000, side=32768, out=None, nthreads=
     return {"xyz": xyz, "ncols": side, "nrows": side, "cell": 100, "lakes": lakes}
 
 
+def config5(seed=BASE_SEED + 5, n=2_000_000_000, side_m=64000.0, out=None, nthreads=0):
+    """Served cloud: n points over side_m x side_m metres (0.49 points/m^2 at
+    the defaults), the config-2 generator scaled to the area (64 clusters and
+    16 lakes per 4096 m square)."""
+    scale = (side_m / 4096.0) ** 2
+    xyz, lakes = generate(seed, n, side_m, side_m, kind="terrain", nclusters=max(1, int(64 * scale)),
+                          frac_uniform=0.7, cluster_sigma=20.0, nlakes=max(1, int(16 * scale)), lake_rmin=50.0,
+                          lake_rmax=400.0, relief=300.0, z_noise=0.1, base_wavelength=4096.0, nthreads=nthreads,
+                          out=out)
+    return {"xyz": xyz, "side_m": side_m, "lakes": lakes}
+
+
+def served_requests(count, seed=BASE_SEED + 6, side_m=64000.0):
+    """Request boxes: side log-uniform in 128 m - 8 km, cell 0.5/1/2 m, placed
+    uniformly inside the cloud's area (LAS units at 0.01 m)."""
+    rng = np.random.default_rng(seed)
+    side = np.exp(rng.uniform(math.log(128.0), math.log(8192.0), count))
+    cell = rng.choice(np.array([50, 100, 200]), count)
+    out = []
+    for k in range(count):
+        n = max(1, int(round(side[k] * 100 / cell[k])))
+        span = n * int(cell[k])
+        x0 = int(rng.integers(0, max(1, int(side_m * 100) - span)))
+        y0 = int(rng.integers(0, max(1, int(side_m * 100) - span)))
+        out.append({"x0": x0, "y0": y0, "ncols": n, "nrows": n, "cell_size": int(cell[k])})
+    return out
+
+
 def mixed_tiles(count=4096, seed=BASE_SEED + 4, max_points=1_000_000):
     """Tile specs of the mixed batch: side log-uniform in [64, 1024] cells,
     cell 0.5/1/2 m, density log-uniform in [0.05, 8] points/cell,
