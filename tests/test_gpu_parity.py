@@ -159,3 +159,24 @@ def test_engine_window_fallbacks(oracle, k):
     with engine.Engine(device=0, bin_target=bt) as e:
         h, site, _ = e.interpolate(engine.make_wp(side, side, cs), xyz, site=True)
     assert np.array_equal(site, ref["site"]) and _same(h, ref["h"])
+
+
+@pytest.mark.parametrize("kind", ["wide_z", "wide_discs"])
+def test_span_path_extremes(eng, oracle, kind):
+    """Extremes of the span path: a z range near the int32 limit (unpacked
+    accumulators), and discs of up to 1700 cells (one site on a long grid)."""
+    from terranni_b200 import engine
+    rng = np.random.default_rng(9)
+    if kind == "wide_z":
+        side, n = 200, 3000
+        xyz = terrain_case(12, side, n, lakes=2, lake_r=(10.0, 40.0))
+        xyz[:, 2] = rng.integers(-400_000_000, 400_000_000, n, dtype=np.int64).astype(np.int32)
+    else:                       # a thin grid with one site at its left end: radii up to 1700 cells
+        side, n = 1700, 1
+        xyz = np.array([[0, 1500, 777]], np.int32)
+    rows = side if kind == "wide_z" else 40
+    wp = engine.make_wp(side, rows, 100)
+    ref = oracle.interpolate(oracle.make_wp(side, rows, 100), xyz)
+    h, site, st = eng.interpolate(wp, xyz, site=True)
+    assert np.array_equal(site, ref["site"])
+    assert _same(h, ref["h"])
