@@ -148,8 +148,8 @@ dnni_status dnni_interpolate_segment_device(dnni_ctx *ctx, const dnni_workpackag
  * loads the library holds it until the process exits.
  *
  * Limit: the work package must fit that array, at about 12 B per grid cell +
- * 16 B per raster pixel + 20 B per point + 8.2 B per search bin (about one
- * bin per two points), each region rounded up to 256 B; e.g. a 512 x 512
+ * 24 B per raster pixel + 20 B per point + 8.2 B per search bin (about one
+ * bin per four points), each region rounded up to 256 B; e.g. a 512 x 512
  * grid with 500k points fits.  Larger work packages return DNNI_E_SCRATCH, before
  * any work is queued or, for the search bins (sized from the point bounding
  * box), right after the bounding-box pass.
