@@ -343,12 +343,17 @@ def run_engine_tile4096(args, world, rank, local):
 # mixed-tile batch
 # ---------------------------------------------------------------------------
 
-def mixed_workload(count, rank, pinned):
+def mixed_workload(count, rank, pinned, world=1):
     """Specs, layout, points (absolute LAS xyz rows, pinned when asked) and
-    per-tile point extents of the mixed batch of this rank."""
+    per-tile point extents of this rank's share of the mixed batch: world x
+    count tiles are drawn and split over the ranks by estimated cost
+    (terranni_b200.shard), so each rank gets about `count` tiles."""
     import numpy as np
-    from terranni_b200 import synth
-    specs = synth.mixed_tiles(count=count, seed=BASE_SEED + 4 + 1000 * rank)
+    from terranni_b200 import shard, synth
+    specs = synth.mixed_tiles(count=count * world, seed=BASE_SEED + 4)
+    if world > 1:
+        parts = shard.partition_by_cost([shard.tile_cost(s["side"], s["side"], s["n"]) for s in specs], world)
+        specs = [specs[k] for k in parts[rank]]
     lay, npt, nout = synth.mixed_layout(specs)
     if pinned:
         import torch
@@ -485,7 +490,7 @@ def run_engine_mixed(args, world, rank, local):
             tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         return float(t.item())
 
-    w = mixed_workload(args.tiles, rank, pinned=True)
+    w = mixed_workload(args.tiles, rank, pinned=True, world=world)
     npt, nout, xyz = w["npt"], w["nout"], w["xyz"]
     tiles = mixed_tiles_abi(w)
     eng = engine.Engine(device=local)
