@@ -351,6 +351,49 @@ dnni_status dnni_batch_autotune(dnni_ctx *ctx, const dnni_tile *tiles, int32_t n
                                 const uint32_t *d_gid, int32_t sample_tiles, dnni_batch_options *options,
                                 dnni_tune_report *report);
 
+/* ---- input: LAS point files ----
+ *
+ * Replaces the reference's nni_io::las_reader (las_reader.h:34-58,
+ * las_reader.inl:25-84, on libLAS 1.6) for the engine's input: the public
+ * LAS layout (1.0-1.4, point formats 0-10, uncompressed) read directly.
+ * dnni_las_read returns the records' raw X, Y, Z integers -- the engine's
+ * int32 LAS units, position = integer * scale + offset from the header --
+ * for records [first, first + count), parsed on nthreads host threads
+ * (0 = all cores), optionally with each record's intensity (which the
+ * reference reads as the point's time, las_reader.inl:64). */
+typedef struct dnni_las_header {
+    uint8_t version_major, version_minor, point_format, pad0;
+    uint16_t record_length, pad1;
+    uint32_t offset_to_points;
+    uint64_t n_points;
+    double scale[3], offset[3], min[3], max[3];
+} dnni_las_header;
+
+dnni_status dnni_las_read_header(const char *path, dnni_las_header *header);
+dnni_status dnni_las_read(const char *path, int64_t first, int64_t count, int32_t *xyz, uint16_t *intensity,
+                          int32_t nthreads);
+/* Writes n points as a LAS 1.2 file of point format 0 (for fixtures and
+ * exchange); scale/offset: 3 doubles each (NULL = 0.01 and 0). */
+dnni_status dnni_las_write(const char *path, const int32_t *xyz, const uint16_t *intensity, int64_t n,
+                           const double *scale, const double *offset);
+
+/* ---- output: grids ----
+ *
+ * dnni_write_asc writes an ESRI ASCII grid as the reference's outputASC does
+ * (terranni.cpp:428-488): header NROWS, NCOLS, XLLCORNER, YLLCORNER,
+ * CELLSIZE, NODATA_VALUE, then one line per grid row from the top (highest
+ * y) row, each value in 6 significant digits followed by a space.  The grid
+ * is row-major with row 0 the lowest y, as the engine writes it, so no sort
+ * of an OutPoint stream is needed; corner and cell size are printed in 10
+ * significant digits (the reference's stream default of 6 rounds UTM
+ * coordinates).  dnni_write_grid_bin writes a 64-byte header ("DNNIGRD1",
+ * ncols, nrows as int32, xll, yll, cellsize as double, nodata as float, zero
+ * padding) and the float32 cells row-major from row 0. */
+dnni_status dnni_write_asc(const char *path, const float *h, int32_t ncols, int32_t nrows, double xll, double yll,
+                           double cellsize, float nodata, int32_t nthreads);
+dnni_status dnni_write_grid_bin(const char *path, const float *h, int32_t ncols, int32_t nrows, double xll,
+                                double yll, double cellsize, float nodata);
+
 /* ---- nni::clearRenderbuffers / nni::printTimes (nni.h:87-97) ---- */
 
 /* Free the context's scratch (it is re-created on demand). */

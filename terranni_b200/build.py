@@ -22,7 +22,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-
            "-I" + os.path.join(ROOT, "include")]
 
 CUDA_SOURCES = ["dnni_engine.cu"]
-CXX_SOURCES = []
+CXX_SOURCES = ["dnni_io.cpp"]
 
 
 def _run(cmd):

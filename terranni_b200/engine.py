@@ -128,6 +128,20 @@ class ServerStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class LasHeader(ctypes.Structure):
+    _fields_ = [("version_major", ctypes.c_uint8), ("version_minor", ctypes.c_uint8),
+                ("point_format", ctypes.c_uint8), ("pad0", ctypes.c_uint8), ("record_length", ctypes.c_uint16),
+                ("pad1", ctypes.c_uint16), ("offset_to_points", ctypes.c_uint32), ("n_points", ctypes.c_uint64),
+                ("scale", ctypes.c_double * 3), ("offset", ctypes.c_double * 3), ("min", ctypes.c_double * 3),
+                ("max", ctypes.c_double * 3)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("pad")}
+        for k in ("scale", "offset", "min", "max"):
+            d[k] = list(d[k])
+        return d
+
+
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("pad", ctypes.c_int32)]
@@ -174,6 +188,13 @@ _SIGS = {
     "dnni_server_wait": ([_P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestResult)], ctypes.c_int),
     "dnni_server_get_stats": ([_P, ctypes.POINTER(ServerStats)], ctypes.c_int),
     "dnni_server_destroy": ([_P], ctypes.c_int),
+    "dnni_las_read_header": ([ctypes.c_char_p, ctypes.POINTER(LasHeader)], ctypes.c_int),
+    "dnni_las_read": ([ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64, _P, _P, ctypes.c_int32], ctypes.c_int),
+    "dnni_las_write": ([ctypes.c_char_p, _P, _P, ctypes.c_int64, _P, _P], ctypes.c_int),
+    "dnni_write_asc": ([ctypes.c_char_p, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                        ctypes.c_double, ctypes.c_float, ctypes.c_int32], ctypes.c_int),
+    "dnni_write_grid_bin": ([ctypes.c_char_p, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                             ctypes.c_double, ctypes.c_float], ctypes.c_int),
     "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
                              ctypes.POINTER(BatchOptions), ctypes.POINTER(TuneReport)], ctypes.c_int),
 }
@@ -453,3 +474,51 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ---- host I/O (no device needed) ----
+
+def _rc(rc, what):
+    if rc:
+        raise DnniError(rc, what)
+
+
+def las_read_header(path):
+    h = LasHeader()
+    _rc(lib().dnni_las_read_header(os.fsencode(path), ctypes.byref(h)), f"dnni_las_read_header {path}")
+    return h.as_dict()
+
+
+def las_read(path, first=0, count=None, intensity=False, out=None, nthreads=0):
+    """Raw record integers (n, 3) int32 of records [first, first+count); with
+    intensity also the (n,) uint16 intensities."""
+    hd = las_read_header(path)
+    if count is None:
+        count = hd["n_points"] - first
+    xyz = out if out is not None else np.empty((count, 3), np.int32)
+    it = np.empty(count, np.uint16) if intensity else None
+    _rc(lib().dnni_las_read(os.fsencode(path), int(first), int(count), _ptr(xyz), _ptr(it), int(nthreads)),
+        f"dnni_las_read {path}")
+    return (xyz, it) if intensity else xyz
+
+
+def las_write(path, xyz, intensity=None, scale=(0.01, 0.01, 0.01), offset=(0.0, 0.0, 0.0)):
+    xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
+    if intensity is not None:
+        intensity = np.ascontiguousarray(intensity, np.uint16)
+    sc = (ctypes.c_double * 3)(*scale)
+    of = (ctypes.c_double * 3)(*offset)
+    _rc(lib().dnni_las_write(os.fsencode(path), _ptr(xyz), _ptr(intensity), xyz.shape[0], sc, of),
+        f"dnni_las_write {path}")
+
+
+def write_asc(path, h, xll, yll, cellsize, nodata=-9999.0, nthreads=0):
+    h = np.ascontiguousarray(h, np.float32)
+    _rc(lib().dnni_write_asc(os.fsencode(path), _ptr(h), h.shape[1], h.shape[0], float(xll), float(yll),
+                             float(cellsize), float(nodata), int(nthreads)), f"dnni_write_asc {path}")
+
+
+def write_grid_bin(path, h, xll, yll, cellsize, nodata=-9999.0):
+    h = np.ascontiguousarray(h, np.float32)
+    _rc(lib().dnni_write_grid_bin(os.fsencode(path), _ptr(h), h.shape[1], h.shape[0], float(xll), float(yll),
+                                  float(cellsize), float(nodata)), f"dnni_write_grid_bin {path}")
