@@ -58,6 +58,8 @@ struct BatchTables {
 struct BatchCounters {
     int nfar;                    // far worklist slots used
     int err;                     // kErrRange when a point was out of range
+    int far_next;                // next far group to hand out
+    int pad;
 };
 
 template <typename B>
@@ -82,7 +84,7 @@ __global__ void k_init_scalars(BatchTables bt, Scalars* sc, BatchCounters* ctr) 
         s->bbox[2] = INT_MAX; s->bbox[3] = INT_MIN;
         s->bbox[4] = INT_MAX; s->bbox[5] = INT_MIN;
         s->err = 0; s->packed = 0; s->kbits = 0; s->zbase = 0;
-        if (t == 0) { ctr->nfar = 0; ctr->err = 0; }
+        if (t == 0) { ctr->nfar = 0; ctr->err = 0; ctr->far_next = 0; }
     }
     if (l < kStatSlots) {
         s->max_r2[l] = -1; s->big_pixels[l] = 0; s->spans[l] = 0; s->nodata[l] = 0;
@@ -600,24 +602,55 @@ __device__ __forceinline__ unsigned box_lb32(int rx, int ry, int x0, int x1, int
     return (unsigned)(dx * dx) + (unsigned)(dy * dy);
 }
 
+// 8 x 8 mask of the cells (u wide, origin (X0, Y0)) that the union of the
+// active lanes' discs may touch, row by row: in cell row r the lanes' disc
+// chords, widened by one unit, are merged into their hull across the warp.
+// A superset of the cells within some lane's bound, so the search stays
+// exact; the lanes of a group are neighbouring pixels of one row, whose
+// chords overlap, so the hull adds little.  Warp-uniform result.
+__device__ __forceinline__ uint64_t chord_mask8(bool act, long long px, long long py, long long d2, long long X0,
+                                                long long Y0, long long u, bool small) {
+    uint64_t m = 0;
+#pragma unroll 1
+    for (int r = 0; r < 8; ++r) {
+        int a = 8, e = -1;
+        if (act) {
+            const long long gy = axis_gap(py, Y0 + r * u, Y0 + (r + 1) * u - 1);
+            if (gy * gy <= d2) {
+                const long long v = d2 - gy * gy;
+                const long long w = (small ? (long long)sqrtf((float)v) : (long long)sqrt((double)v)) + 1;
+                const long long lo = px - w - X0, hi = px + w - X0;
+                if (hi >= 0 && lo < 8 * u) {
+                    a = lo <= 0 ? 0 : udiv32(lo, u);
+                    e = hi >= 8 * u ? 7 : udiv32(hi, u);
+                }
+            }
+        }
+        a = __reduce_min_sync(0xffffffffu, a);
+        e = __reduce_max_sync(0xffffffffu, e);
+        if (a <= e) m |= (uint64_t)((0xFFu >> (7 - e)) & (0xFFu << a) & 0xFFu) << (8 * r);
+    }
+    return m;
+}
+
 // Warp-cooperative exact search for the 32 pixels of one worklist group
 // (neighbouring pixels of one tile row; inactive lanes have act = false).
 // The warp walks the superblocks of the union of the lanes' bound boxes
-// (rows outward from the group's centre).  Inside a superblock, candidate
-// blocks are the non-empty ones inside some lane's bound box (an OR of the
-// lanes' box masks); each candidate gets every lane's exact box test and is
-// entered when any lane needs it; bins likewise; every point of an entered
-// bin is loaded once and considered by the lanes that need the bin.  All
-// control flow is uniform across the warp.  Complete for each active lane
-// whose b holds a real site on entry, by the same argument as search_disc.
+// (rows outward from the group's centre); inside a superblock the candidate
+// blocks are the non-empty ones under the chord hull of the lanes' discs
+// (chord_mask8), inside a candidate block the candidate bins likewise, and
+// every point of a candidate bin is considered by every active lane (the
+// comparison is exact, so extra candidates cost time, never correctness).
+// All control flow is uniform across the warp.  Complete for each active
+// lane whose b holds a real site on entry, by the same argument as
+// search_disc.
 __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                                  const uint64_t* __restrict__ bmask, const uint64_t* __restrict__ smask, bool act,
                                  int px, int py, Best& b) {
     const unsigned full = 0xffffffffu;
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
     const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
-    const float inv_u1 = 1.0f / (float)u1, inv_bs = 1.0f / (float)bs;
-    long long reach = act ? reach_of(b.d2) : 0;
+    const long long reach = act ? reach_of(b.d2) : 0;
     const long long xlo = warp_min64(act ? px - reach : LLONG_MAX), xhi = warp_max64(act ? px + reach : LLONG_MIN);
     const long long ylo = warp_min64(act ? py - reach : LLONG_MAX), yhi = warp_max64(act ? py + reach : LLONG_MIN);
     if (xlo > xhi) return;   // no active lane
@@ -625,8 +658,6 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
     cell_range((xlo + xhi) / 2, (xhi - xlo) / 2 + 1, gx0, u2, g.n2x, sx0, sx1);
     cell_range((ylo + yhi) / 2, (yhi - ylo) / 2 + 1, gy0, u2, g.n2y, sy0, sy1);
     if (sx0 > sx1 || sy0 > sy1) return;
-    // 32-bit tests are exact while every active lane's bound is below 2^31
-    const bool small = __all_sync(full, !act || b.d2 < (1LL << 31));
     const long long cyy = warp_min64(act ? py : LLONG_MAX);
     int csy = udiv32((cyy < gy0 ? gy0 : cyy) - gy0, u2);
     csy = csy < sy0 ? sy0 : (csy > sy1 ? sy1 : csy);
@@ -642,52 +673,25 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
             const long long SX0 = gx0 + (long long)sx * u2;
             const bool need_s = act && box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) <= b.d2;
             if (!__any_sync(full, need_s)) continue;
-            // candidate blocks: inside some needing lane's bound box
-            reach = act ? reach_of(b.d2) : 0;
-            uint64_t lm = 0;
-            if (need_s) {
-                int a0, a1, b0, b1;
-                cell_span8(px, reach, SX0, inv_u1, a0, a1);
-                cell_span8(py, reach, SY0, inv_u1, b0, b1);
-                lm = box_mask8(a0, a1, b0, b1);
-            }
-            uint64_t cand = sm & warp_or64(lm);
-            // pixel relative to the superblock (in range whenever the lane needs it)
-            const long long rxl = px - SX0, ryl = py - SY0;
-            const int rx = (int)(rxl < -(1LL << 30) ? -(1LL << 30) : (rxl > (1LL << 30) ? (1LL << 30) : rxl));
-            const int ry = (int)(ryl < -(1LL << 30) ? -(1LL << 30) : (ryl > (1LL << 30) ? (1LL << 30) : ryl));
+            // 32-bit square roots are within one unit while every bound is below 2^31
+            bool small = __all_sync(full, !act || b.d2 < (1LL << 31));
+            uint64_t cand = sm & chord_mask8(act, px, py, b.d2, SX0, SY0, u1, small);
             while (cand) {
                 const int m = ffs64(cand);
                 cand &= cand - 1;
-                const int bx0 = (m & 7) * (int)u1, by0 = (m >> 3) * (int)u1;
-                bool need_b;
-                if (small) need_b = act && (long long)box_lb32(rx, ry, bx0, bx0 + (int)u1 - 1, by0, by0 + (int)u1 - 1) <= b.d2;
-                else need_b = act && box_lb(px, py, SX0 + bx0, SX0 + bx0 + u1 - 1, SY0 + by0, SY0 + by0 + u1 - 1) <= b.d2;
-                if (!__any_sync(full, need_b)) continue;
+                const long long BX0 = SX0 + (long long)(m & 7) * u1, BY0 = SY0 + (long long)(m >> 3) * u1;
                 const int64_t blk = ((int64_t)sidx << 6) + m;
                 const uint64_t bm = __ldg(&bmask[blk]);
-                uint64_t lq = 0;
-                if (need_b) {
-                    int a0, a1, b0, b1;
-                    const long long rr = reach_of(b.d2);
-                    cell_span8(px, rr, SX0 + bx0, inv_bs, a0, a1);
-                    cell_span8(py, rr, SY0 + by0, inv_bs, b0, b1);
-                    lq = box_mask8(a0, a1, b0, b1);
-                }
-                uint64_t qc = bm & warp_or64(lq);
+                small = __all_sync(full, !act || b.d2 < (1LL << 31));
+                uint64_t qc = bm & chord_mask8(act, px, py, b.d2, BX0, BY0, bs, small);
                 while (qc) {
                     const int l = ffs64(qc);
                     qc &= qc - 1;
-                    const int qx0 = bx0 + (l & 7) * (int)bs, qy0 = by0 + (l >> 3) * (int)bs;
-                    bool need;
-                    if (small) need = act && (long long)box_lb32(rx, ry, qx0, qx0 + (int)bs - 1, qy0, qy0 + (int)bs - 1) <= b.d2;
-                    else need = act && box_lb(px, py, SX0 + qx0, SX0 + qx0 + bs - 1, SY0 + qy0, SY0 + qy0 + bs - 1) <= b.d2;
-                    if (!__any_sync(full, need)) continue;
                     const int64_t id = (blk << 6) + l;
                     const int s0 = __ldg(&start[id]), e0 = __ldg(&start[id + 1]);
                     for (int q = s0; q < e0; ++q) {
                         const int4 p = __ldg(&pts[q]);
-                        if (need) consider(b, p, q, px, py);
+                        if (act) consider(b, p, q, px, py);
                     }
                 }
             }
@@ -695,7 +699,7 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
     }
 }
 
-// Far pass over the worklist: one warp per group of 32 slots (grid-stride;
+// Far pass over the worklist: one warp per group of 32 slots (handed out by a counter;
 // all slots of a group belong to one tile).  Each lane seeds its bound (its
 // best site so far, else the nearest non-empty block's closest bin, else the
 // nearest non-empty superblock) and the warp searches the union of the bound
@@ -707,10 +711,17 @@ __global__ void __launch_bounds__(256, 3) k_near_far(BatchTables bt, const int4*
                                                      const int64_t* __restrict__ near_all,
                                                      const FarSlot* __restrict__ far, int2* __restrict__ pix,
                                                      uint32_t* __restrict__ site, Scalars* __restrict__ sc,
-                                                     const BatchCounters* __restrict__ ctr) {
+                                                     BatchCounters* __restrict__ ctr) {
     const int count = ctr->nfar;
     const int lane = threadIdx.x & 31;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += gridDim.x * blockDim.x) {
+    // groups differ in cost by orders of magnitude (a lake's centre against
+    // its shore), so each warp takes the next group from a counter instead of
+    // a fixed stride
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&ctr->far_next, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
         const FarSlot item = far[base + lane];
         const int t = __shfl_sync(0xffffffffu, item.tile, 0);
         const TileParams& T = bt.tiles[t];
