@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--srv-points", type=int, default=2_000_000_000, help="served: cloud points")
     ap.add_argument("--srv-side", type=float, default=64000.0, help="served: cloud side, metres")
     ap.add_argument("--srv-requests", type=int, default=200, help="served: requests per arrival rate")
-    ap.add_argument("--srv-rates", default="100,1000,5000,20000", help="served: Poisson arrival rates, 1/s")
+    ap.add_argument("--srv-rates", default="20,100,1000,20000", help="served: Poisson arrival rates, 1/s")
     ap.add_argument("--seg-side", type=int, default=32768, help="segment: grid side in cells (1 m)")
     ap.add_argument("--seg-points", type=int, default=1_500_000_000, help="segment: points")
     ap.add_argument("--seg-tile", type=int, default=2048)

@@ -415,8 +415,8 @@ struct FarSlot {
     int tile, pix, idx, pad;
 };
 
-// Dense pass.  One CTA per 32 x 8 raster tile of a work package (blockDim
-// 32 x 8, warp = one pixel row of the tile): the tile's bin window (bin rings
+// Dense pass.  One CTA per 32 x kTileY raster tile of a work package (blockDim
+// 32 x 8; warp w takes pixel rows w, w + 8, ... of the tile): the tile's bin window (bin rings
 // of every pixel) is staged in shared memory and the rings are searched
 // there; windows too large for shared memory use the global arrays.  A warp
 // with pixels the rings do not settle appends its whole row as one group of
@@ -441,8 +441,7 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
     const int lt = blockIdx.x - __ldg(&bt.rt_base[t]);
     const int ntx = (T.rw + kTileX - 1) / kTileX;
     const int i0 = (lt % ntx) * kTileX, j0 = (lt / ntx) * kTileY;
-    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-    const bool valid = i < T.rw && j < T.rh;
+    const int i = i0 + threadIdx.x;
     int wx0 = 0, wy0 = 0, wnx = 0, wny = 0;
     bool staged = false;
     if (T.npts > 0) {
@@ -514,6 +513,10 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
             __syncthreads();
         }
     }
+#pragma unroll 1
+    for (int sub = 0; sub < kDenseSub; ++sub) {
+    const int j = j0 + threadIdx.y + 8 * sub;
+    const bool valid = i < T.rw && j < T.rh;
     int R2 = -1;
     bool far_pixel = false;
     Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
@@ -551,7 +554,8 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
         base = __shfl_sync(0xffffffffu, base, 0);
         far[base + lane] = far_pixel ? FarSlot{t, j * T.rw + i, b.idx, 0} : FarSlot{t, -1, -1, 0};
     }
-    warp_stats(T, R2, sc + t, blockIdx.x + threadIdx.y);
+    warp_stats(T, R2, sc + t, blockIdx.x + threadIdx.y + 8 * sub);
+    }
 }
 
 __device__ __forceinline__ long long warp_min64(long long v) {
@@ -810,7 +814,9 @@ __global__ void __launch_bounds__(256) k_scatter_spans(BatchTables bt, const int
     const TileParams& T = bt.tiles[t];
     const int lt = blockIdx.x - __ldg(&bt.rt_base[t]);
     const int ntx = (T.rw + kTileX - 1) / kTileX;
-    const int i = (lt % ntx) * kTileX + threadIdx.x, j = (lt / ntx) * kTileY + threadIdx.y;
+#pragma unroll 1
+    for (int sub = 0; sub < kDenseSub; ++sub) {
+    const int i = (lt % ntx) * kTileX + threadIdx.x, j = (lt / ntx) * kTileY + threadIdx.y + 8 * sub;
     int R2 = -1, z = 0;
     if (i < T.rw && j < T.rh) {
         const int2 r = pix[T.pix_off + (int64_t)j * T.rw + i];
@@ -818,7 +824,7 @@ __global__ void __launch_bounds__(256) k_scatter_spans(BatchTables bt, const int
         R2 = r.y;
     }
     const bool big = R2 > T.rs * T.rs;
-    if (!__any_sync(0xffffffffu, big)) return;
+    if (!__any_sync(0xffffffffu, big)) continue;
     const int r = big ? isqrt_i32(R2) : -1;
     const int rmax = __reduce_max_sync(0xffffffffu, r);
     const Scalars& s = sc[t];
@@ -835,6 +841,7 @@ __global__ void __launch_bounds__(256) k_scatter_spans(BatchTables bt, const int
             emit_span(py + dy, px - w, px + w, T.ncols, T.nrows, packed, v, z, D, Dc);
             if (dy) emit_span(py - dy, px - w, px + w, T.ncols, T.nrows, packed, v, z, D, Dc);
         }
+    }
     }
 }
 

@@ -442,7 +442,11 @@ DNNI_HD int window_global_index(const BinWindow& w, int q) {
 }
 
 // Window of the 32 x 8 pixel tile whose first pixel is raster (i0, j0).
-constexpr int kTileX = 32, kTileY = 8;
+// Raster tiles are 32 x kTileY pixels, one CTA of 32 x 8 threads each; a
+// thread takes kDenseSub pixels of its column, so that one staged bin window
+// serves kTileY rows.
+constexpr int kDenseSub = 2;
+constexpr int kTileX = 32, kTileY = 8 * kDenseSub;
 DNNI_HD void tile_window(const TileParams& t, int i0, int j0, int& wx0, int& wy0, int& wnx, int& wny) {
     const BinGrid& g = t.bg;
     const int i1 = (i0 + kTileX - 1 < t.rw - 1) ? i0 + kTileX - 1 : t.rw - 1;
