@@ -708,7 +708,7 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
 // best site so far, else the nearest non-empty block's closest bin, else the
 // nearest non-empty superblock) and the warp searches the union of the bound
 // discs cooperatively.
-__global__ void __launch_bounds__(256, 3) k_near_far(BatchTables bt, const int4* __restrict__ pts_all,
+__global__ void __launch_bounds__(256, 4) k_near_far(BatchTables bt, const int4* __restrict__ pts_all,
                                                      const int* __restrict__ start_all,
                                                      const uint64_t* __restrict__ bmask_all,
                                                      const uint64_t* __restrict__ smask_all,
