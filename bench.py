@@ -40,7 +40,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "DEM cells/s batched vs plain GPU NNI at ≤1e-4 m err vs FP64; p50/p99 tile latency"
 UNIT = "cells/s"
-KERNELS_PER_CALL = 18      # own kernel launches per interpolate call or batch run with points (2 + 16)
+KERNELS_PER_CALL = 17      # own kernel launches per single-work-package call with points
+KERNELS_PER_BATCH = 16     # per batch run (the bounding boxes come with the bin counts)
 FALLBACK_HBM_GBS = 6650.0
 BASE_SEED = 20261203
 
@@ -317,7 +318,7 @@ def run_engine_tile4096(args, world, rank, local):
                        "form": "plain per-tile (one work package per call)",
                        "l2": "inputs larger than L2 (240 MB points, ~1 GB scratch per step)",
                        "parallelism": f"dp{world} (independent tiles)"},
-            "roofline": {"bound": "hbm", "kernel": "whole hot path per tile (13 launches)",
+            "roofline": {"bound": "hbm", "kernel": f"whole hot path per tile ({KERNELS_PER_CALL} launches)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes": alg_bytes, "dominant_phase": dom,
@@ -605,13 +606,13 @@ def run_engine_mixed(args, world, rank, local):
                       "heights_identical_to_batched": same},
             "latency": {"batch_ms_p50": _pct(step_ms, 50), "batch_ms_p99": _pct(step_ms, 99),
                         "note": "batched: every tile of a step completes with its batch"},
-            "roofline": {"bound": "hbm", "kernel": "whole hot path per batch (18 launches)",
+            "roofline": {"bound": "hbm", "kernel": f"whole hot path per batch ({KERNELS_PER_BATCH} launches)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": alg_bytes,
                          "dominant_phase": dom, "phase_ms": phases},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(xyz.nbytes),
                     "d2h_bytes_per_step": int(nout * 4)},
-            "gpu_launches": KERNELS_PER_CALL * args.steps,
+            "gpu_launches": KERNELS_PER_BATCH * args.steps,
             "clocks": clk.summary(),
             "work": {"span_pixels": st0.big_pixels, "spans": st0.spans, "max_r2": st0.max_r2,
                      "nodata_cells": nod},
@@ -698,7 +699,7 @@ def run_engine_segment(args, world, rank, local):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(st.h2d_bytes),
                     "d2h_bytes_per_step": int(st.d2h_bytes),
                     "note": "the segment call is host to host: its value is already end to end"},
-            "gpu_launches": int(sum(3 + x.batches * (KERNELS_PER_CALL + 1) for x in stats)),
+            "gpu_launches": int(sum(4 + x.batches * (KERNELS_PER_BATCH + 1) for x in stats)),
             "clocks": clk.summary(), "nodata_cells": nod,
         }), flush=True)
     eng.close()
@@ -813,7 +814,7 @@ def run_engine_served(args, world, rank, local):
                     "note": "requests return heights in host memory: the value is already end to end"},
             "roofline": {"bound": "hbm", "kernel": "whole request path", "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "achieved": None, "frac": None, "traffic": None},
-            "gpu_launches": int(st["batches"] * (KERNELS_PER_CALL + 1)), "clocks": clk.summary(),
+            "gpu_launches": int(st["batches"] * (KERNELS_PER_BATCH + 1)), "clocks": clk.summary(),
         }), flush=True)
     eng.close()
     if tdist is not None:

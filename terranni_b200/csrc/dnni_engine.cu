@@ -141,13 +141,15 @@ void set_dense_smem_attr() {
     }
 }
 
-// Launch sequence, part 1: per-tile scalars and the point bounding boxes.
+// Launch sequence, part 1: per-tile scalars and (with bbox) the point
+// bounding boxes, which a single work package needs before its bins are
+// planned; batches pass bbox = false and have k_bin_count take the boxes.
 void launch_prologue(const HostBatch& hb, const BatchTables& bt, const DevArrays& a, const int32_t* d_xyz,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool bbox = true) {
     const int n = (int)hb.tiles.size();
     k_init_scalars<<<n, 32, 0, st>>>(bt, a.sc, a.ctr);
     const int nchunk = hb.chunk_base.back();
-    if (nchunk > 0) k_bbox<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.sc, a.ctr);
+    if (bbox && nchunk > 0) k_bbox<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.sc, a.ctr);
 }
 
 // Launch sequence, part 2: binning, nearest sites, spans, stencil, finalize.
@@ -155,12 +157,12 @@ void launch_prologue(const HostBatch& hb, const BatchTables& bt, const DevArrays
 // ev[0..2] (optional) mark the ends of binning, nearest sites and spans.
 void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a, const int32_t* d_xyz,
                  const uint32_t* d_gid, float* d_h, uint32_t* d_site, int sms, cudaStream_t st,
-                 const cudaEvent_t* ev) {
+                 const cudaEvent_t* ev, bool bbox_in_count = false) {
     const int nchunk = hb.chunk_base.back();
     const int64_t nblk = hb.blk_base.back(), nsup = hb.sup_base.back();
     if (nchunk > 0) {
         cudaMemsetAsync(a.cnt, 0, sizeof(int) * hb.n_bins, st);
-        k_bin_count<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.cnt, a.rank, a.ctr);
+        k_bin_count<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.cnt, a.rank, a.sc, a.ctr, bbox_in_count ? 1 : 0);
         const int nscan = hb.scan_base.back();
         k_scan_partial<<<nscan, kScanThreads, 0, st>>>(bt, a.cnt, a.bsum);
         k_scan_bsum<<<(int)hb.tiles.size(), 1024, 0, st>>>(bt, a.bsum);
@@ -185,8 +187,7 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     k_scatter_spans<<<nrt, dim3(32, 8), 0, st>>>(bt, a.pix, a.sc, a.D, a.Dc);
     if (ev) cudaEventRecord(ev[2], st);
     const int ngrow = hb.grow_base.back();
-    k_rowscan<unsigned long long><<<ngrow, kScanThreads, 0, st>>>(bt, a.D, a.sc, 0);
-    k_rowscan<int><<<ngrow, kScanThreads, 0, st>>>(bt, a.Dc, a.sc, 1);
+    k_rowscan<<<ngrow, kScanThreads, 0, st>>>(bt, a.D, a.Dc, a.sc);
     launch_final(bt, hb.ct_base.back(), hb.rs, a.pix, a.sc, a.D, a.Dc, d_h, st);
 }
 
@@ -601,8 +602,8 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
             CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
             cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
-                launch_prologue(b->hb, b->bt, b->arr, d_xyz, cap);
-                launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, cap, nullptr);
+                launch_prologue(b->hb, b->bt, b->arr, d_xyz, cap, false);
+                launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, cap, nullptr, true);
                 e = cudaStreamEndCapture(cap, &b->graph);
             }
             cudaStreamDestroy(cap);
@@ -613,8 +614,9 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
         CK(cudaGraphLaunch(b->exec, st));
     } else {
         // with stats, ev[1..3] mark the ends of binning, nearest sites and spans
-        launch_prologue(b->hb, b->bt, b->arr, d_xyz, st);
-        launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, st, stats ? &c->ev[1] : nullptr);
+        launch_prologue(b->hb, b->bt, b->arr, d_xyz, st, false);
+        launch_body(b->hb, b->bt, b->arr, d_xyz, d_gid, d_h, d_site, c->sm_count, st, stats ? &c->ev[1] : nullptr,
+                    true);
         CK(cudaGetLastError());
     }
     if (stats) {
@@ -742,8 +744,8 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
         if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
         for (int r = 0; r < 3; ++r) {            // one warm-up run, two timed
             if (r == 1) CK(cudaEventRecord(c->ev[0], st));
-            launch_prologue(hb, bt, a, d_xyz, st);
-            launch_body(hb, bt, a, d_xyz, d_gid, (float*)hbuf.p, nullptr, c->sm_count, st, nullptr);
+            launch_prologue(hb, bt, a, d_xyz, st, false);
+            launch_body(hb, bt, a, d_xyz, d_gid, (float*)hbuf.p, nullptr, c->sm_count, st, nullptr, true);
         }
         CK(cudaEventRecord(c->ev[1], st));
         CK(cudaGetLastError());

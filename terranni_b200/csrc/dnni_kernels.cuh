@@ -92,7 +92,38 @@ __global__ void k_init_scalars(BatchTables bt, Scalars* sc, BatchCounters* ctr) 
 }
 
 // Bounding box of each tile's points relative to its origin, with range checks
-// (the coordinate range, and the declared extent where the caller gave one).
+// (the coordinate range, and the declared extent where the caller gave one):
+// bbox_point per point, bbox_flush once per warp.
+struct BBoxAcc {
+    int mnx = INT_MAX, mxx = INT_MIN, mny = INT_MAX, mxy = INT_MIN, mnz = INT_MAX, mxz = INT_MIN;
+    unsigned bad = 0;
+};
+
+__device__ __forceinline__ void bbox_point(const TileParams& T, int xr, int yr, int zr, BBoxAcc& acc) {
+    const long long x = (long long)xr - T.ox, y = (long long)yr - T.oy, z = zr;
+    if (x <= -kCoordLimit || x >= kCoordLimit || y <= -kCoordLimit || y >= kCoordLimit || z <= -kCoordLimit ||
+        z >= kCoordLimit || (T.has_ext && (x < T.ex0 || x > T.ex1 || y < T.ey0 || y > T.ey1))) {
+        acc.bad = 1;
+        return;
+    }
+    acc.mnx = min(acc.mnx, (int)x); acc.mxx = max(acc.mxx, (int)x);
+    acc.mny = min(acc.mny, (int)y); acc.mxy = max(acc.mxy, (int)y);
+    acc.mnz = min(acc.mnz, (int)z); acc.mxz = max(acc.mxz, (int)z);
+}
+
+__device__ __forceinline__ void bbox_flush(BBoxAcc& acc, Scalars* s, BatchCounters* ctr) {
+    acc.mnx = __reduce_min_sync(0xffffffffu, acc.mnx); acc.mxx = __reduce_max_sync(0xffffffffu, acc.mxx);
+    acc.mny = __reduce_min_sync(0xffffffffu, acc.mny); acc.mxy = __reduce_max_sync(0xffffffffu, acc.mxy);
+    acc.mnz = __reduce_min_sync(0xffffffffu, acc.mnz); acc.mxz = __reduce_max_sync(0xffffffffu, acc.mxz);
+    acc.bad = __reduce_or_sync(0xffffffffu, acc.bad);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&s->bbox[0], acc.mnx); atomicMax(&s->bbox[1], acc.mxx);
+        atomicMin(&s->bbox[2], acc.mny); atomicMax(&s->bbox[3], acc.mxy);
+        atomicMin(&s->bbox[4], acc.mnz); atomicMax(&s->bbox[5], acc.mxz);
+        if (acc.bad) { atomicOr(&s->err, kErrRange); atomicOr(&ctr->err, kErrRange); }
+    }
+}
+
 __global__ void __launch_bounds__(256) k_bbox(BatchTables bt, const int32_t* __restrict__ xyz, Scalars* sc,
                                               BatchCounters* ctr) {
     const int t = find_tile(bt.chunk_base, bt.ntiles, blockIdx.x);
@@ -100,32 +131,9 @@ __global__ void __launch_bounds__(256) k_bbox(BatchTables bt, const int32_t* __r
     const int64_t c0 = (int64_t)(blockIdx.x - __ldg(&bt.chunk_base[t])) * kChunk;
     const int64_t c1 = c0 + kChunk < T.npts ? c0 + kChunk : T.npts;
     const int32_t* p = xyz + 3 * T.pt_off;
-    int mnx = INT_MAX, mxx = INT_MIN, mny = INT_MAX, mxy = INT_MIN, mnz = INT_MAX, mxz = INT_MIN;
-    unsigned bad = 0;
-    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-        const long long x = (long long)p[3 * i] - T.ox, y = (long long)p[3 * i + 1] - T.oy;
-        const long long z = p[3 * i + 2];
-        if (x <= -kCoordLimit || x >= kCoordLimit || y <= -kCoordLimit || y >= kCoordLimit ||
-            z <= -kCoordLimit || z >= kCoordLimit ||
-            (T.has_ext && (x < T.ex0 || x > T.ex1 || y < T.ey0 || y > T.ey1))) {
-            bad = 1;
-            continue;
-        }
-        mnx = min(mnx, (int)x); mxx = max(mxx, (int)x);
-        mny = min(mny, (int)y); mxy = max(mxy, (int)y);
-        mnz = min(mnz, (int)z); mxz = max(mxz, (int)z);
-    }
-    mnx = __reduce_min_sync(0xffffffffu, mnx); mxx = __reduce_max_sync(0xffffffffu, mxx);
-    mny = __reduce_min_sync(0xffffffffu, mny); mxy = __reduce_max_sync(0xffffffffu, mxy);
-    mnz = __reduce_min_sync(0xffffffffu, mnz); mxz = __reduce_max_sync(0xffffffffu, mxz);
-    bad = __reduce_or_sync(0xffffffffu, bad);
-    if ((threadIdx.x & 31) == 0) {
-        Scalars* s = sc + t;
-        atomicMin(&s->bbox[0], mnx); atomicMax(&s->bbox[1], mxx);
-        atomicMin(&s->bbox[2], mny); atomicMax(&s->bbox[3], mxy);
-        atomicMin(&s->bbox[4], mnz); atomicMax(&s->bbox[5], mxz);
-        if (bad) { atomicOr(&s->err, kErrRange); atomicOr(&ctr->err, kErrRange); }
-    }
+    BBoxAcc acc;
+    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) bbox_point(T, p[3 * i], p[3 * i + 1], p[3 * i + 2], acc);
+    bbox_flush(acc, sc + t, ctr);
 }
 
 // A tile's points outside its bin grid (possible only when the caller's
@@ -142,9 +150,11 @@ __device__ __forceinline__ int64_t point_bin_checked(const BinGrid& g, int xr, i
 }
 
 // Counting-sort pass 1: per-bin counts; each point keeps its rank in its bin.
+// with_bbox: also the bounding box and range checks of k_bbox (batches,
+// whose bin grids are planned before any point is seen, skip k_bbox).
 __global__ void __launch_bounds__(256) k_bin_count(BatchTables bt, const int32_t* __restrict__ xyz,
-                                                   int* __restrict__ cnt, int* __restrict__ rank,
-                                                   BatchCounters* ctr) {
+                                                   int* __restrict__ cnt, int* __restrict__ rank, Scalars* sc,
+                                                   BatchCounters* ctr, int with_bbox) {
     const int t = find_tile(bt.chunk_base, bt.ntiles, blockIdx.x);
     const TileParams& T = bt.tiles[t];
     const int64_t c0 = (int64_t)(blockIdx.x - __ldg(&bt.chunk_base[t])) * kChunk;
@@ -152,10 +162,14 @@ __global__ void __launch_bounds__(256) k_bin_count(BatchTables bt, const int32_t
     const int32_t* p = xyz + 3 * T.pt_off;
     int* c = cnt + T.bin_off;
     unsigned bad = 0;
+    BBoxAcc acc;
     for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-        const int64_t id = point_bin_checked(T.bg, rel_coord(p[3 * i], T.ox), rel_coord(p[3 * i + 1], T.oy), bad);
+        const int xr = p[3 * i], yr = p[3 * i + 1];
+        if (with_bbox) bbox_point(T, xr, yr, p[3 * i + 2], acc);
+        const int64_t id = point_bin_checked(T.bg, rel_coord(xr, T.ox), rel_coord(yr, T.oy), bad);
         rank[T.srt_off + i] = atomicAdd(&c[id], 1);
     }
+    if (with_bbox) bbox_flush(acc, sc + t, ctr);
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&ctr->err, kErrRange);
 }
 
@@ -845,17 +859,9 @@ __global__ void __launch_bounds__(256) k_scatter_spans(BatchTables bt, const int
     }
 }
 
-// In-place inclusive prefix along each grid row of each tile.  which: 0 = the
-// 64-bit words (always), 1 = the int32 counts (only when not packed).
+// In-place inclusive prefix of one grid row (256 threads, 4 values each per step).
 template <typename V>
-__global__ void __launch_bounds__(kScanThreads) k_rowscan(BatchTables bt, V* __restrict__ D_all,
-                                                          const Scalars* __restrict__ sc, int which) {
-    const int t = find_tile(bt.grow_base, bt.ntiles, blockIdx.x);
-    if (which == 1 && sc[t].packed) return;
-    const TileParams& T = bt.tiles[t];
-    __shared__ V wsum[8];
-    const int ncols = T.ncols;
-    V* row = D_all + T.cell_off + (int64_t)(blockIdx.x - __ldg(&bt.grow_base[t])) * ncols;
+__device__ __forceinline__ void row_prefix(V* __restrict__ row, int ncols, V* wsum) {
     V carry = 0;
     for (int base = 0; base < ncols; base += kScanThreads * 4) {
         const int idx = base + threadIdx.x * 4;
@@ -869,6 +875,19 @@ __global__ void __launch_bounds__(kScanThreads) k_rowscan(BatchTables bt, V* __r
         for (int k = 0; k < 4; ++k) if (idx + k < ncols) row[idx + k] = v[k] + excl;
         carry += total;
     }
+}
+
+// One block per grid row: prefix of the span words, and of the int32 counts
+// when the tile's accumulators are not packed.
+__global__ void __launch_bounds__(kScanThreads) k_rowscan(BatchTables bt, unsigned long long* __restrict__ D_all,
+                                                          int* __restrict__ Dc_all, const Scalars* __restrict__ sc) {
+    __shared__ unsigned long long wsum[8];
+    __shared__ int wsumc[8];
+    const int t = find_tile(bt.grow_base, bt.ntiles, blockIdx.x);
+    const TileParams& T = bt.tiles[t];
+    const int64_t off = T.cell_off + (int64_t)(blockIdx.x - __ldg(&bt.grow_base[t])) * T.ncols;
+    row_prefix(D_all + off, T.ncols, wsum);
+    if (!sc[t].packed) row_prefix(Dc_all + off, T.ncols, wsumc);
 }
 
 __device__ __forceinline__ float finalize_height(long long Z, long long C, double zs, double zo, float nodata) {

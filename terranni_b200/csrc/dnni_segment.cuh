@@ -363,9 +363,9 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         if ((rs = ensure_scratch(c, scr, scratch_sizes(hb), a))) return rs;
         const BatchTables bt = device_tables(a.tables, ng);
         if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
-        launch_prologue(hb, bt, a, (const int32_t*)B.gxyz.p, st);
+        launch_prologue(hb, bt, a, (const int32_t*)B.gxyz.p, st, false);
         launch_body(hb, bt, a, (const int32_t*)B.gxyz.p, (const uint32_t*)B.ggid.p, (float*)B.gout.p,
-                    h_site ? (uint32_t*)B.gsite.p : nullptr, c->sm_count, st, nullptr);
+                    h_site ? (uint32_t*)B.gsite.p : nullptr, c->sm_count, st, nullptr, true);
         CK(cudaGetLastError());
         hsc.resize(ng);
         CK(cudaMemcpyAsync(hsc.data(), a.sc, sizeof(Scalars) * ng, cudaMemcpyDeviceToHost, st));

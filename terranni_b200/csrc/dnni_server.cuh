@@ -302,8 +302,8 @@ dnni_status srv_launch(dnni_server* s, SrvSlot& sl, std::vector<SrvItem>& items,
     }
     if (nt) {
         const BatchTables bt = device_tables(a.tables, nt);
-        launch_prologue(hb, bt, a, gxyz, st);
-        launch_body(hb, bt, a, gxyz, ggid, gout, site ? gsite : nullptr, c->sm_count, st, nullptr);
+        launch_prologue(hb, bt, a, gxyz, st, false);
+        launch_body(hb, bt, a, gxyz, ggid, gout, site ? gsite : nullptr, c->sm_count, st, nullptr, true);
         CK(cudaMemcpyAsync(sl.h_sc, a.sc, sizeof(Scalars) * nt, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(sl.h_ctr, a.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
     }
