@@ -456,15 +456,23 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
     const int ntx = (T.rw + kTileX - 1) / kTileX;
     const int i0 = (lt % ntx) * kTileX, j0 = (lt / ntx) * kTileY;
     const int i = i0 + threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    // the tile's rows go in bands, each with its own staged window: the whole
+    // tile when its window fits shared memory, else halves, down to 8 rows
+    int band = kTileY;
+    for (int jb = 0; jb < kTileY && j0 + jb < T.rh; jb += band) {
     int wx0 = 0, wy0 = 0, wnx = 0, wny = 0;
     bool staged = false;
-    if (T.npts > 0) {
-        tile_window(T, i0, j0, wx0, wy0, wnx, wny);
+    while (T.npts > 0) {
+        tile_window(T, i0, j0 + jb, band, wx0, wy0, wnx, wny);
         const int nwb = wnx * wny;
-        if (nwb <= kWinMaxBins && wny <= kWinMaxRows) {
+        if (nwb > kWinMaxBins || wny > kWinMaxRows) {
+            if (band > 8) { band >>= 1; continue; }
+            break;
+        }
+        {
             // per-bin counts -> local starts: warp w takes window rows w, w+8,
             // ...; lanes take columns, with a warp scan along the row
-            const int warp = tid >> 5, lane = tid & 31;
             for (int r = warp; r < wny; r += 8) {
                 int rowsum = 0;
                 for (int c0 = 0; c0 < wnx; c0 += 32) {
@@ -508,6 +516,11 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
             for (int r = warp; r < wny; r += 8)
                 for (int c = lane; c < wnx; c += 32) s_lstart[r * wnx + c] += s_rowbase[r];
             __syncthreads();
+            if (s_total > kWinMaxPts && band > 8) {   // too many points: a shorter band
+                band >>= 1;
+                __syncthreads();
+                continue;
+            }
             staged = s_total <= kWinMaxPts;
             if (staged) {
                 // copy the window's points run by run: the bins of one window
@@ -526,10 +539,11 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
             }
             __syncthreads();
         }
+        break;
     }
 #pragma unroll 1
-    for (int sub = 0; sub < kDenseSub; ++sub) {
-    const int j = j0 + threadIdx.y + 8 * sub;
+    for (int sub = 0; sub < band / 8; ++sub) {
+    const int j = j0 + jb + threadIdx.y + 8 * sub;
     const bool valid = i < T.rw && j < T.rh;
     int R2 = -1;
     bool far_pixel = false;
@@ -561,7 +575,6 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
     // slots as one group (settled or absent pixels as empty slots), so that
     // a far warp later takes 32 neighbouring pixels of one tile
     const unsigned mfar = __ballot_sync(0xffffffffu, far_pixel);
-    const int lane = threadIdx.x;
     if (mfar) {
         int base = 0;
         if (lane == 0) base = atomicAdd(&ctr->nfar, 32);
@@ -569,6 +582,8 @@ __global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int
         far[base + lane] = far_pixel ? FarSlot{t, j * T.rw + i, b.idx, 0} : FarSlot{t, -1, -1, 0};
     }
     warp_stats(T, R2, sc + t, blockIdx.x + threadIdx.y + 8 * sub);
+    }
+    __syncthreads();     // the next band restages the window
     }
 }
 

@@ -441,16 +441,16 @@ DNNI_HD int window_global_index(const BinWindow& w, int q) {
     return w.gstart[lo] + (q - w.lstart[lo]);
 }
 
-// Window of the 32 x 8 pixel tile whose first pixel is raster (i0, j0).
+// Window of the 32 x rows pixel band whose first pixel is raster (i0, j0).
 // Raster tiles are 32 x kTileY pixels, one CTA of 32 x 8 threads each; a
 // thread takes kDenseSub pixels of its column, so that one staged bin window
 // serves kTileY rows.
 constexpr int kDenseSub = 4;
 constexpr int kTileX = 32, kTileY = 8 * kDenseSub;
-DNNI_HD void tile_window(const TileParams& t, int i0, int j0, int& wx0, int& wy0, int& wnx, int& wny) {
+DNNI_HD void tile_window(const TileParams& t, int i0, int j0, int rows, int& wx0, int& wy0, int& wnx, int& wny) {
     const BinGrid& g = t.bg;
     const int i1 = (i0 + kTileX - 1 < t.rw - 1) ? i0 + kTileX - 1 : t.rw - 1;
-    const int j1 = (j0 + kTileY - 1 < t.rh - 1) ? j0 + kTileY - 1 : t.rh - 1;
+    const int j1 = (j0 + rows - 1 < t.rh - 1) ? j0 + rows - 1 : t.rh - 1;
     long long bxa = udiv32((long long)(t.rx0 + i0) * t.cs - g.gx0, g.bs), bxb = udiv32((long long)(t.rx0 + i1) * t.cs - g.gx0, g.bs);
     long long bya = udiv32((long long)(t.ry0 + j0) * t.cs - g.gy0, g.bs), byb = udiv32((long long)(t.ry0 + j1) * t.cs - g.gy0, g.bs);
     bxa = bxa < g.nbx - 1 ? bxa : g.nbx - 1;

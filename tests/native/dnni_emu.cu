@@ -117,7 +117,7 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
             bool staged = false;
             int wx0 = 0, wy0 = 0, wnx = 0, wny = 0;
             if (n > 0) {
-                tile_window(t, i0, j0, wx0, wy0, wnx, wny);
+                tile_window(t, i0, j0, kTileY, wx0, wy0, wnx, wny);
                 const int nwb = wnx * wny;
                 if (nwb <= kWinMaxBins && wny <= kWinMaxRows) {
                     int run2 = 0;
