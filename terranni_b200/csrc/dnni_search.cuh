@@ -445,7 +445,7 @@ DNNI_HD int window_global_index(const BinWindow& w, int q) {
 // Raster tiles are 32 x kTileY pixels, one CTA of 32 x 8 threads each; a
 // thread takes kDenseSub pixels of its column, so that one staged bin window
 // serves kTileY rows.
-constexpr int kDenseSub = 4;
+constexpr int kDenseSub = 8;
 constexpr int kTileX = 32, kTileY = 8 * kDenseSub;
 DNNI_HD void tile_window(const TileParams& t, int i0, int j0, int rows, int& wx0, int& wy0, int& wnx, int& wny) {
     const BinGrid& g = t.bg;
