@@ -560,6 +560,8 @@ dnni_status dnni_batch_create(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
     dnni_batch* b = new dnni_batch();
     b->ctx = c;
     b->use_graph = o.use_graph;
+    b->opt = o;
+    b->tiles_in.assign(tiles, tiles + ntiles);
     {
         dnni_status rs = plan_batch(c, tiles, ntiles, o, b->hb, b->order);
         if (rs) {
@@ -646,6 +648,97 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
     return DNNI_OK;
 }
 
+// Cuts a batch into up to kSlices slices of consecutive point rows with
+// about equal work, plans each and uploads its tables; the slices share the
+// batch's scratch (they run one after another on the compute stream).
+static dnni_status plan_slices(dnni_batch* b) {
+    dnni_ctx* c = b->ctx;
+    constexpr int kSlices = 4;
+    const int n = (int)b->tiles_in.size();
+    const int S = (b->hb.n_rows >= (4 << 20) && n >= kSlices) ? kSlices : 1;
+    b->sliced = S > 1;
+    b->slices.clear();
+    if (!b->sliced) {
+        b->slices_planned = true;
+        return DNNI_OK;
+    }
+    std::vector<int> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int x, int y) { return b->tiles_in[x].pt_offset < b->tiles_in[y].pt_offset; });
+    auto cost = [&](int k) {
+        const dnni_tile& t = b->tiles_in[k];
+        return (double)t.wp.ncols * t.wp.nrows + (double)t.pt_count;
+    };
+    double total = 0;
+    for (int k : idx) total += cost(k);
+    dnni_batch_options o = b->opt;
+    o.order_by_cost = 0;
+    double run = 0;
+    size_t k0 = 0;
+    for (int s = 0; s < S; ++s) {
+        size_t k1 = k0;
+        const double goal = total * (s + 1) / S;
+        while (k1 < idx.size() && (s == S - 1 || run + cost(idx[k1]) <= goal || k1 == k0)) run += cost(idx[k1++]);
+        if (k1 == k0) break;
+        std::vector<dnni_tile> part;
+        for (size_t k = k0; k < k1; ++k) part.push_back(b->tiles_in[idx[k]]);
+        BatchSlice sl;
+        std::vector<int> order;
+        dnni_status rs = plan_batch(c, part.data(), (int)part.size(), o, sl.hb, order);
+        if (rs) return rs;
+        sl.row0 = INT64_MAX;
+        sl.out0 = INT64_MAX;
+        sl.site0 = INT64_MAX;
+        for (const dnni_tile& t : part) {
+            sl.row0 = std::min(sl.row0, t.pt_offset);
+            sl.row1 = std::max(sl.row1, t.pt_offset + t.pt_count);
+            sl.out0 = std::min<int64_t>(sl.out0, t.out_offset);
+            sl.out1 = std::max<int64_t>(sl.out1, t.out_offset + (int64_t)t.wp.ncols * t.wp.nrows);
+        }
+        for (const TileParams& t : sl.hb.tiles)
+            if (t.site_off >= 0) {
+                sl.site0 = std::min<int64_t>(sl.site0, t.site_off);
+                sl.site1 = std::max<int64_t>(sl.site1, t.site_off + (int64_t)t.rw * t.rh);
+            }
+        if (sl.site0 == INT64_MAX) sl.site0 = sl.site1 = 0;
+        if ((rs = dnni_ensure(c, sl.tables, TableLayout((int)part.size()).total))) return rs;
+        sl.bt = device_tables((const unsigned char*)sl.tables.p, (int)part.size());
+        if ((rs = stage_tables(c, sl.hb, (unsigned char*)sl.tables.p, c->stream))) return rs;
+        DevArrays tmp;
+        if ((rs = ensure_scratch(c, b->scr, scratch_sizes(sl.hb), tmp))) return rs;
+        b->slices.push_back(std::move(sl));
+        k0 = k1;
+    }
+    // the shared scratch may have moved while it grew: the full batch's view
+    // and its captured graph are rebuilt
+    DevArrays full;
+    dnni_status rs = ensure_scratch(c, b->scr, scratch_sizes(b->hb), full);
+    if (rs) return rs;
+    full.tables = b->arr.tables;
+    if (full.sorted != b->arr.sorted || full.pix != b->arr.pix) {
+        if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+        if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    }
+    b->arr = full;
+    const int ns = (int)b->slices.size();
+    if (cudaStreamCreateWithFlags(&b->s_in, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost((void**)&b->h_ctrs, sizeof(BatchCounters) * ns) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, DNNI_E_CUDA, "slice streams");
+    }
+    b->ev_in.assign(ns, nullptr);
+    b->ev_done.assign(ns, nullptr);
+    for (int s = 0; s < ns; ++s)
+        if (cudaEventCreateWithFlags(&b->ev_in[s], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->ev_done[s], cudaEventDisableTiming) != cudaSuccess)
+            return set_err(c, DNNI_E_CUDA, "slice events");
+    CK(cudaStreamSynchronize(c->stream));
+    b->slices_planned = true;
+    return DNNI_OK;
+}
+
 dnni_status dnni_batch_run(dnni_batch* b, const int32_t* xyz, const uint32_t* gid, int64_t n_rows, float* out_h,
                            uint32_t* out_site, dnni_stats* stats) {
     if (!b) return DNNI_E_INVAL;
@@ -658,25 +751,78 @@ dnni_status dnni_batch_run(dnni_batch* b, const int32_t* xyz, const uint32_t* gi
     dnni_status rs;
     if (n_rows > 0) {
         if ((rs = dnni_ensure(c, b->in_xyz, sizeof(int32_t) * 3 * n_rows))) return rs;
-        CK(cudaMemcpyAsync(b->in_xyz.p, xyz, sizeof(int32_t) * 3 * n_rows, cudaMemcpyHostToDevice, st));
-        if (gid) {
-            if ((rs = dnni_ensure(c, b->in_gid, sizeof(uint32_t) * n_rows))) return rs;
-            CK(cudaMemcpyAsync(b->in_gid.p, gid, sizeof(uint32_t) * n_rows, cudaMemcpyHostToDevice, st));
-        }
+        if (gid && (rs = dnni_ensure(c, b->in_gid, sizeof(uint32_t) * n_rows))) return rs;
     }
     const int64_t nh = std::max<int64_t>(b->hb.out_end, 1), ns = std::max<int64_t>(b->hb.site_end, 1);
     if ((rs = dnni_ensure(c, b->out_h, sizeof(float) * nh))) return rs;
     if (out_site && (rs = dnni_ensure(c, b->out_site, sizeof(uint32_t) * ns))) return rs;
-    rs = dnni_batch_run_device(b, (const int32_t*)b->in_xyz.p, gid ? (const uint32_t*)b->in_gid.p : nullptr,
-                               (float*)b->out_h.p, out_site ? (uint32_t*)b->out_site.p : nullptr, st, stats);
-    if (rs) return rs;
-    CK(cudaMemcpyAsync(out_h, b->out_h.p, sizeof(float) * b->hb.out_end, cudaMemcpyDeviceToHost, st));
-    if (out_site && b->hb.site_end > 0)
-        CK(cudaMemcpyAsync(out_site, b->out_site.p, sizeof(uint32_t) * b->hb.site_end, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(c->h_ctr, b->arr.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (c->h_ctr->err & kErrRange)
-        return set_err(c, DNNI_E_RANGE, "a point lies beyond its tile's declared extent or the coordinate range");
+    if (!b->slices_planned && (rs = plan_slices(b))) return rs;
+    if (!b->sliced) {
+        if (n_rows > 0) {
+            CK(cudaMemcpyAsync(b->in_xyz.p, xyz, sizeof(int32_t) * 3 * n_rows, cudaMemcpyHostToDevice, st));
+            if (gid) CK(cudaMemcpyAsync(b->in_gid.p, gid, sizeof(uint32_t) * n_rows, cudaMemcpyHostToDevice, st));
+        }
+        rs = dnni_batch_run_device(b, (const int32_t*)b->in_xyz.p, gid ? (const uint32_t*)b->in_gid.p : nullptr,
+                                   (float*)b->out_h.p, out_site ? (uint32_t*)b->out_site.p : nullptr, st, stats);
+        if (rs) return rs;
+        CK(cudaMemcpyAsync(out_h, b->out_h.p, sizeof(float) * b->hb.out_end, cudaMemcpyDeviceToHost, st));
+        if (out_site && b->hb.site_end > 0)
+            CK(cudaMemcpyAsync(out_site, b->out_site.p, sizeof(uint32_t) * b->hb.site_end, cudaMemcpyDeviceToHost,
+                               st));
+        CK(cudaMemcpyAsync(c->h_ctr, b->arr.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (c->h_ctr->err & kErrRange)
+            return set_err(c, DNNI_E_RANGE, "a point lies beyond its tile's declared extent or the coordinate range");
+    } else {
+        // pipelined: slice s uploads on s_in while slice s-1 computes on the
+        // context stream and slice s-2 downloads on s_out
+        if (stats) {
+            memset(stats, 0, sizeof(*stats));
+            CK(cudaEventRecord(c->ev[0], st));
+            CK(cudaStreamWaitEvent(b->s_in, c->ev[0], 0));
+        }
+        int32_t* dx = (int32_t*)b->in_xyz.p;
+        uint32_t* dg = gid ? (uint32_t*)b->in_gid.p : nullptr;
+        for (size_t s = 0; s < b->slices.size(); ++s) {
+            const BatchSlice& sl = b->slices[s];
+            const size_t r0 = (size_t)sl.row0, nr = (size_t)(sl.row1 - sl.row0);
+            if (nr) {
+                CK(cudaMemcpyAsync(dx + 3 * r0, xyz + 3 * r0, 12 * nr, cudaMemcpyHostToDevice, b->s_in));
+                if (gid) CK(cudaMemcpyAsync(dg + r0, gid + r0, 4 * nr, cudaMemcpyHostToDevice, b->s_in));
+            }
+            CK(cudaEventRecord(b->ev_in[s], b->s_in));
+            CK(cudaStreamWaitEvent(st, b->ev_in[s], 0));
+            DevArrays a = b->arr;
+            a.tables = (unsigned char*)sl.tables.p;
+            launch_prologue(sl.hb, sl.bt, a, dx, st, false);
+            launch_body(sl.hb, sl.bt, a, dx, dg, (float*)b->out_h.p, out_site ? (uint32_t*)b->out_site.p : nullptr,
+                        c->sm_count, st, nullptr, true);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(&b->h_ctrs[s], a.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+            CK(cudaEventRecord(b->ev_done[s], st));
+            CK(cudaStreamWaitEvent(b->s_out, b->ev_done[s], 0));
+            CK(cudaMemcpyAsync(out_h + sl.out0, (const float*)b->out_h.p + sl.out0, 4 * (size_t)(sl.out1 - sl.out0),
+                               cudaMemcpyDeviceToHost, b->s_out));
+            if (out_site && sl.site1 > sl.site0)
+                CK(cudaMemcpyAsync(out_site + sl.site0, (const uint32_t*)b->out_site.p + sl.site0,
+                                   4 * (size_t)(sl.site1 - sl.site0), cudaMemcpyDeviceToHost, b->s_out));
+        }
+        if (stats) CK(cudaEventRecord(c->ev[1], b->s_out));
+        CK(cudaStreamSynchronize(b->s_out));
+        CK(cudaStreamSynchronize(st));
+        for (size_t s = 0; s < b->slices.size(); ++s)
+            if (b->h_ctrs[s].err & kErrRange)
+                return set_err(c, DNNI_E_RANGE,
+                               "a point lies beyond its tile's declared extent or the coordinate range");
+        if (stats) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+            stats->ms_total = ms;
+            for (const TileParams& t : b->hb.tiles) stats->n_points += t.npts;
+            stats->n_cells = b->hb.n_cells;
+            stats->n_pixels = b->hb.n_pix;
+        }
+    }
     if (stats) {
         stats->h2d_bytes = (int64_t)(sizeof(int32_t) * 3 * n_rows + (gid ? sizeof(uint32_t) * n_rows : 0));
         stats->d2h_bytes =
@@ -693,6 +839,14 @@ dnni_status dnni_batch_destroy(dnni_batch* b) {
         cudaDeviceSynchronize();
         if (b->exec) cudaGraphExecDestroy(b->exec);
         if (b->graph) cudaGraphDestroy(b->graph);
+        for (BatchSlice& sl : b->slices) dnni_release(sl.tables, c);
+        for (cudaEvent_t e : b->ev_in)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : b->ev_done)
+            if (e) cudaEventDestroy(e);
+        if (b->s_in) cudaStreamDestroy(b->s_in);
+        if (b->s_out) cudaStreamDestroy(b->s_out);
+        if (b->h_ctrs) cudaFreeHost(b->h_ctrs);
         release_scratch(c, b->scr);
         dnni_release(b->in_xyz, c);
         dnni_release(b->in_gid, c);

@@ -62,8 +62,25 @@ struct dnni_ctx {
     int64_t calls = 0;
 };
 
+// A slice of a batch for the pipelined host-buffer run: tiles whose point
+// rows form one range, so that the slice's upload, launch sequence and
+// download can overlap those of its neighbours.
+struct BatchSlice {
+    dnni::HostBatch hb;
+    DevBuf tables;
+    dnni::BatchTables bt{};
+    int64_t row0 = 0, row1 = 0, out0 = 0, out1 = 0, site0 = 0, site1 = 0;
+};
+
 struct dnni_batch {
     dnni_ctx* ctx = nullptr;
+    std::vector<dnni_tile> tiles_in;     // the caller's tiles, for slicing
+    dnni_batch_options opt{};
+    std::vector<BatchSlice> slices;      // planned on the first host-buffer run
+    bool sliced = false, slices_planned = false;
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    std::vector<cudaEvent_t> ev_in, ev_done;
+    dnni::BatchCounters* h_ctrs = nullptr;
     dnni::HostBatch hb;
     Scratch scr;
     DevArrays arr;

@@ -207,3 +207,51 @@ def test_autotuned_options_give_the_same_heights(eng):
     with eng.batch(tiles, use_graph=True, **opts) as b:
         h, s, _ = _run_device(b, xyz, nout, nsite)
     _check(meta, ref, h, s)
+
+
+@pytest.mark.parametrize("reverse_out", [False, True])
+def test_pipelined_host_run_matches_device_run(eng, reverse_out):
+    """Batches of 4 Mi point rows or more run their host-buffer form in
+    slices whose upload, launches and download overlap; the result must equal
+    the device-buffer run, also when the tiles' outputs lie in the opposite
+    order to their points."""
+    from terranni_b200 import engine
+    rng = np.random.default_rng(17)
+    rows, tiles, sides = [], [], []
+    pt = 0
+    for k in range(10):
+        side = int(rng.integers(150, 400))
+        n = int(rng.integers(350_000, 600_000))
+        xyz = terrain_case(int(rng.integers(1, 1 << 30)), side, n, lakes=2, lake_r=(0.05 * side, 0.2 * side))
+        xyz[:, 0] += 1_000_000 * k
+        rows.append(xyz)
+        sides.append(side)
+        tiles.append((k, side, pt, n, xyz))
+        pt += n
+    xyz_all = np.concatenate(rows)
+    assert xyz_all.shape[0] >= 4 << 20
+    order = list(range(10))[::-1] if reverse_out else list(range(10))
+    out = {}
+    o = 0
+    for k in order:
+        out[k] = o
+        o += sides[k] * sides[k]
+    site = {}
+    sp = 0
+    for k in range(10):
+        site[k] = sp
+        sp += sides[k] * sides[k]
+    tl = []
+    for k, side, p0, n, xyz in tiles:
+        wp = engine.make_wp(side, side, 100, 1_000_000 * k, 0)
+        ext = (int(xyz[:, 0].min()), int(xyz[:, 1].min()), int(xyz[:, 0].max()), int(xyz[:, 1].max()))
+        tl.append(engine.make_tile(wp, p0, n, out[k], site[k], extent=ext))
+    gid = rng.permutation(xyz_all.shape[0]).astype(np.uint32)
+    with eng.batch(tl, use_graph=True) as b:
+        h_d, s_d, _ = _run_device(b, xyz_all, o, sp, gid)
+        h = np.empty(o, np.float32)
+        s = np.empty(sp, np.uint32)
+        for _ in range(2):
+            st = b.run(xyz_all, h, gid=gid, out_site=s)
+            assert _same(h, h_d[:o]) and np.array_equal(s, s_d[:sp])
+        assert st.n_cells == o and st.ms_total > 0
