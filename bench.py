@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--seg-tile", type=int, default=2048)
     ap.add_argument("--seg-halo", type=int, default=0,
                     help="segment: first raster halo tried (cells); 0 = bound from block occupancy")
-    ap.add_argument("--seg-batch", type=int, default=16, help="segment: tiles per batch")
+    ap.add_argument("--seg-batch", type=int, default=64, help="segment: tiles per batch")
     ap.add_argument("--tiles", type=int, default=4096, help="tiles of the mixed workload")
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="timed passes of the plain per-tile form (0: skip the plain form)")

@@ -238,7 +238,7 @@ typedef struct dnni_segment {
     int32_t halo;                  /* first raster halo tried, cells; 0 = per tile, from an
                                       upper bound of the nearest-site distance computed
                                       from the occupancy of 16-cell blocks */
-    int32_t tiles_per_batch;       /* 0 = 16 */
+    int32_t tiles_per_batch;       /* 0 = 64 */
     double z_scale, z_offset;
     float nodata;
     int32_t small_radius;          /* 0 = the context's setting */

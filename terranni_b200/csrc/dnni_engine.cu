@@ -952,8 +952,15 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
 
 }  // extern "C"
 
+void SegBufs::release(dnni_ctx* c) {
+    DevBuf* all[] = {&xin, &sxyz, &sgid, &rank, &cnt, &start, &bbox, &gxyz, &ggid, &gout, &gsite, &chunks};
+    for (DevBuf* b : all) dnni_release(*b, c);
+}
+
 void dnni_free_all(dnni_ctx* c) {
     release_scratch(c, c->scr);
+    release_scratch(c, c->seg_scr);
+    c->seg.release(c);
     DevBuf* bufs[] = {&c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }

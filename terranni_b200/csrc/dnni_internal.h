@@ -44,12 +44,22 @@ struct DevArrays {
     unsigned char* tables = nullptr;
 };
 
+struct dnni_ctx;
+
+// Device buffers of the segment driver and the server's resident cloud.
+struct SegBufs {
+    DevBuf xin, sxyz, sgid, rank, cnt, start, bbox, gxyz, ggid, gout, gsite, chunks;
+    void release(dnni_ctx* c);
+};
+
 struct dnni_ctx {
     int device = 0;
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     dnni_settings s{};
     Scratch scr;                     // single work packages (grow-only until dnni_clear)
+    SegBufs seg;                     // segment driver buffers (grow-only until dnni_clear)
+    Scratch seg_scr;
     DevBuf in_xyz, in_gid, out_h, out_site;   // staging for the host-buffer entry point
     unsigned char* h_tables = nullptr;        // pinned staging of the tile tables
     size_t h_tables_cap = 0;

@@ -134,14 +134,6 @@ struct SegTile {
     int hr;               // raster halo (cells); the point box is the raster +- hr
 };
 
-struct SegBufs {
-    DevBuf xin, sxyz, sgid, rank, cnt, start, bbox, gxyz, ggid, gout, gsite, chunks;
-    void release(dnni_ctx* c) {
-        DevBuf* all[] = {&xin, &sxyz, &sgid, &rank, &cnt, &start, &bbox, &gxyz, &ggid, &gout, &gsite, &chunks};
-        for (DevBuf* b : all) dnni_release(*b, c);
-    }
-};
-
 long long floor_div_ll(long long a, long long b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 // Uploads n points (chunks of 64 Mi) and buckets them on the device by G:
@@ -161,9 +153,11 @@ dnni_status upload_points(dnni_ctx* c, cudaStream_t st, const int32_t* h_xyz, in
     return DNNI_OK;
 }
 
-// Buckets the n points already uploaded to B.xin (see bucket_points).
+// Buckets the n points already uploaded to B.xin (see bucket_points);
+// keep_staging leaves B.xin and B.rank allocated for the next call.
 dnni_status bucket_uploaded(dnni_ctx* c, cudaStream_t st, const SegGrid& G, int64_t n, SegBufs& B,
-                            std::vector<long long>& start, std::vector<int4>& bbox, float* ms_up, float* ms_bk) {
+                            std::vector<long long>& start, std::vector<int4>& bbox, float* ms_up, float* ms_bk,
+                            bool keep_staging = false) {
     const int nb = G.nbx * G.nby;
     dnni_status rs;
     const size_t npts = (size_t)std::max<int64_t>(n, 1);
@@ -191,16 +185,19 @@ dnni_status bucket_uploaded(dnni_ctx* c, cudaStream_t st, const SegGrid& G, int6
     CK(cudaGetLastError());
     cudaEventElapsedTime(ms_up, c->ev[0], c->ev[1]);
     cudaEventElapsedTime(ms_bk, c->ev[1], c->ev[2]);
-    dnni_release(B.xin, c);
-    dnni_release(B.rank, c);
+    if (!keep_staging) {
+        dnni_release(B.xin, c);
+        dnni_release(B.rank, c);
+    }
     return DNNI_OK;
 }
 
 dnni_status bucket_points(dnni_ctx* c, cudaStream_t st, const SegGrid& G, const int32_t* h_xyz, int64_t n, SegBufs& B,
-                          std::vector<long long>& start, std::vector<int4>& bbox, float* ms_up, float* ms_bk) {
+                          std::vector<long long>& start, std::vector<int4>& bbox, float* ms_up, float* ms_bk,
+                          bool keep_staging = false) {
     dnni_status rs = upload_points(c, st, h_xyz, n, B);
     if (rs) return rs;
-    return bucket_uploaded(c, st, G, n, B, start, bbox, ms_up, ms_bk);
+    return bucket_uploaded(c, st, G, n, B, start, bbox, ms_up, ms_bk, keep_staging);
 }
 
 // Squared distance, in fine blocks (fw LAS units square, nfx x nfy from the
@@ -236,7 +233,7 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     std::vector<long long> start;
     std::vector<int4> bbox;
     float ms_up = 0, ms_bk = 0;
-    if ((rs = bucket_points(c, st, G, h_xyz, n, B, start, bbox, &ms_up, &ms_bk))) return rs;
+    if ((rs = bucket_points(c, st, G, h_xyz, n, B, start, bbox, &ms_up, &ms_bk, true))) return rs;
 
     // 3. first halo of each tile: unless the caller fixed it, an upper bound
     // of the nearest-site distance from the occupancy of fine blocks (fb
@@ -440,7 +437,7 @@ extern "C" dnni_status dnni_segment_run(dnni_ctx* c, const dnni_segment* sp, con
     DeviceGuard g(c->device);
     dnni_segment s = *sp;
     if (!s.tile) s.tile = 2048;
-    if (!s.tiles_per_batch) s.tiles_per_batch = 16;
+    if (!s.tiles_per_batch) s.tiles_per_batch = 64;
     if (!s.small_radius) s.small_radius = c->s.small_radius;
     if (s.ncols <= 0 || s.nrows <= 0 || s.ncols > (1 << 20) || s.nrows > (1 << 20))
         return set_err(c, DNNI_E_INVAL, "grid sides must be in [1, 2^20]");
@@ -452,11 +449,9 @@ extern "C" dnni_status dnni_segment_run(dnni_ctx* c, const dnni_segment* sp, con
     if ((long long)s.ncols * s.cell_size >= (1LL << 30) || (long long)s.nrows * s.cell_size >= (1LL << 30))
         return set_err(c, DNNI_E_RANGE, "grid extent must stay below 2^30 LAS units");
     if ((uint64_t)n >= 0xFFFFFFFFull) return set_err(c, DNNI_E_INVAL, "more points than 32-bit site ids can name");
-    SegBufs B;
-    Scratch scr;
-    const dnni_status rs = segment_run(c, s, h_xyz, n, h_out, h_site, stats, B, scr);
+    // buffers stay with the context (grow-only) for the next call; dnni_clear
+    // and dnni_destroy free them
+    const dnni_status rs = segment_run(c, s, h_xyz, n, h_out, h_site, stats, c->seg, c->seg_scr);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    release_scratch(c, scr);
-    B.release(c);
     return rs;
 }
