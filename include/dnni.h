@@ -247,6 +247,8 @@ typedef struct dnni_segment {
 typedef struct dnni_segment_stats {
     double ms_total;               /* wall time of the call */
     double ms_upload, ms_bucket;   /* host->device copy, device bucketing */
+    double ms_bound;               /* occupancy distance transform and halo planning (host) */
+    double ms_tiles;               /* the tile batches, planning, launches and copies included */
     int64_t points, cells, tiles;
     int64_t tile_runs;             /* tiles + reruns with a larger halo */
     int64_t h2d_bytes, d2h_bytes;

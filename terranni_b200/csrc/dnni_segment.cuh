@@ -109,6 +109,36 @@ __global__ void __launch_bounds__(256) k_seg_extent(const int32_t* __restrict__ 
     }
 }
 
+// Per tile of a batch, the largest R2 over the two outermost pixel columns
+// or rows on each side of its raster: rm[4t + 0..3] = left, right, bottom,
+// top (-1 without sites).
+__global__ void __launch_bounds__(256) k_ring_max(BatchTables bt, const int2* __restrict__ pix, int* __restrict__ rm) {
+    __shared__ int red[4][8];
+    const TileParams& T = bt.tiles[blockIdx.x];
+    const int2* P = pix + T.pix_off;
+    int m[4] = {-1, -1, -1, -1};
+    for (int k = threadIdx.x; k < 2 * T.rh; k += blockDim.x) {
+        const int j = k >> 1, c = min(k & 1, T.rw - 1);
+        m[0] = max(m[0], P[(int64_t)j * T.rw + c].y);
+        m[1] = max(m[1], P[(int64_t)j * T.rw + (T.rw - 1 - c)].y);
+    }
+    for (int k = threadIdx.x; k < 2 * T.rw; k += blockDim.x) {
+        const int i = k >> 1, r = min(k & 1, T.rh - 1);
+        m[2] = max(m[2], P[(int64_t)r * T.rw + i].y);
+        m[3] = max(m[3], P[(int64_t)(T.rh - 1 - r) * T.rw + i].y);
+    }
+    for (int s = 0; s < 4; ++s) {
+        const int v = __reduce_max_sync(0xffffffffu, m[s]);
+        if ((threadIdx.x & 31) == 0) red[s][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        int v = -1;
+        for (int w = 0; w < 8; ++w) v = max(v, red[threadIdx.x][w]);
+        rm[4 * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
 // Gather of bucket ranges into a tile's staging rows: one block per chunk.
 struct SegChunk {
     long long src, dst;
@@ -131,7 +161,8 @@ namespace {
 
 struct SegTile {
     int x0, y0, x1, y1;   // core cells [x0,x1) x [y0,y1)
-    int hr;               // raster halo (cells); the point box is the raster +- hr
+    int h[4];             // raster halo (cells) on the left, right, bottom, top
+    int hp;               // point halo: the point box is the raster +- hp
 };
 
 long long floor_div_ll(long long a, long long b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
@@ -240,6 +271,7 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     // cells square, at most 4096 per side): a pixel in block b has a site
     // within fb * (sqrt(edt2(b)) + sqrt(2)) cells, and a halo of that + 3 over
     // the whole raster passes the exactness check below.
+    const auto t_bound = clk::now();
     const int fb = std::max(16, (std::max(s.ncols, s.nrows) + 4095) / 4096);
     const int nfx = (s.ncols + fb - 1) / fb, nfy = (s.nrows + fb - 1) / fb;
     std::vector<double> edt2;
@@ -252,22 +284,45 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         if (m >= kEdtFar / 2) return hmax;
         return std::min(hmax, (int)std::ceil(fb * (std::sqrt(m) + 1.4143)) + 3);
     };
+    // Halos per side: a pixel outside the raster whose disc reaches a core
+    // cell forces, on the side where the segment to that cell leaves the
+    // raster, a pixel among the two outermost columns (rows) with distance
+    // to its nearest site >= halo - 1.21 (see the check below); so each
+    // side's halo need only exceed the bound over its own two outer lines,
+    // while the point halo must exceed the bound over the whole raster.
+    auto raster_of = [&](const SegTile& T, int& ax0, int& ay0, int& ax1, int& ay1) {
+        ax0 = std::max(0, T.x0 - T.h[0]);
+        ax1 = std::min(s.ncols, T.x1 + T.h[1]);
+        ay0 = std::max(0, T.y0 - T.h[2]);
+        ay1 = std::min(s.nrows, T.y1 + T.h[3]);
+    };
     std::vector<SegTile> queue;
     for (int y = 0; y < s.nrows; y += s.tile)
         for (int x = 0; x < s.ncols; x += s.tile) {
-            SegTile T{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows), s.halo};
+            SegTile T{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows), {s.halo, s.halo, s.halo, s.halo},
+                      s.halo};
             if (s.halo == 0) {
-                T.hr = bound_halo(T.x0, T.y0, T.x1, T.y1);
-                for (int it = 0; it < 16; ++it) {    // the bound over the raster the halo implies
-                    const int h2 = bound_halo(std::max(0, T.x0 - T.hr), std::max(0, T.y0 - T.hr),
-                                              std::min(s.ncols, T.x1 + T.hr), std::min(s.nrows, T.y1 + T.hr));
-                    if (h2 <= T.hr) break;
-                    T.hr = h2;
+                for (int k = 0; k < 4; ++k) T.h[k] = 2;
+                for (int it = 0; it < 32; ++it) {
+                    int ax0, ay0, ax1, ay1;
+                    raster_of(T, ax0, ay0, ax1, ay1);
+                    const int hs[4] = {bound_halo(ax0, ay0, std::min(ax0 + 2, ax1), ay1),
+                                       bound_halo(std::max(ax1 - 2, ax0), ay0, ax1, ay1),
+                                       bound_halo(ax0, ay0, ax1, std::min(ay0 + 2, ay1)),
+                                       bound_halo(ax0, std::max(ay1 - 2, ay0), ax1, ay1)};
+                    bool grew = false;
+                    for (int k = 0; k < 4; ++k)
+                        if (hs[k] > T.h[k]) { T.h[k] = hs[k]; grew = true; }
+                    if (!grew) break;
                 }
+                int ax0, ay0, ax1, ay1;
+                raster_of(T, ax0, ay0, ax1, ay1);
+                T.hp = bound_halo(ax0, ay0, ax1, ay1);
             }
             queue.push_back(T);
         }
     const int64_t ntiles = (int64_t)queue.size();
+    const auto t_tiles = clk::now();
     int64_t runs = 0, d2h = 0;
     int batches = 0;
     int max_halo = 0;
@@ -278,6 +333,7 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     std::vector<SegChunk> chunks;
     std::vector<int> order;
     std::vector<Scalars> hsc;
+    std::vector<int> ring;
     HostBatch hb;
     DevArrays a;
     while (qi < queue.size()) {
@@ -286,21 +342,24 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         tl.assign(ng, dnni_tile{});
         chunks.clear();
         std::vector<int> rx0(ng), ry0(ng), rw(ng);
-        std::vector<char> all_buckets(ng), all_raster(ng);
+        std::vector<char> all_buckets(ng), clipped(4 * ng);
         int64_t pt = 0, out = 0, site = 0;
         for (int k = 0; k < ng; ++k) {
             const SegTile& T = queue[qi + k];
-            const int ax0 = std::max(0, T.x0 - T.hr), ay0 = std::max(0, T.y0 - T.hr);
-            const int ax1 = std::min(s.ncols, T.x1 + T.hr), ay1 = std::min(s.nrows, T.y1 + T.hr);
-            all_raster[k] = ax0 == 0 && ay0 == 0 && ax1 == s.ncols && ay1 == s.nrows;
+            int ax0, ay0, ax1, ay1;
+            raster_of(T, ax0, ay0, ax1, ay1);
+            clipped[4 * k + 0] = ax0 == 0;
+            clipped[4 * k + 1] = ax1 == s.ncols;
+            clipped[4 * k + 2] = ay0 == 0;
+            clipped[4 * k + 3] = ay1 == s.nrows;
             rx0[k] = ax0;
             ry0[k] = ay0;
             rw[k] = ax1 - ax0;
-            // point box: the raster +- hr, as a range of buckets
-            const int bx0 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ax0 - T.hr, kSegBucketCells), 0), nbx - 1);
-            const int bx1 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ax1 + T.hr - 1, kSegBucketCells), 0), nbx - 1);
-            const int by0 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ay0 - T.hr, kSegBucketCells), 0), nby - 1);
-            const int by1 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ay1 + T.hr - 1, kSegBucketCells), 0), nby - 1);
+            // point box: the raster +- hp, as a range of buckets
+            const int bx0 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ax0 - T.hp, kSegBucketCells), 0), nbx - 1);
+            const int bx1 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ax1 + T.hp - 1, kSegBucketCells), 0), nbx - 1);
+            const int by0 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ay0 - T.hp, kSegBucketCells), 0), nby - 1);
+            const int by1 = (int)std::min<long long>(std::max<long long>(floor_div_ll(ay1 + T.hp - 1, kSegBucketCells), 0), nby - 1);
             all_buckets[k] = bx0 == 0 && by0 == 0 && bx1 == nbx - 1 && by1 == nby - 1;
             const int64_t p0 = pt;
             int4 ext = make_int4(INT_MAX, INT_MAX, INT_MIN, INT_MIN);
@@ -365,6 +424,10 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
                     h_site ? (uint32_t*)B.gsite.p : nullptr, c->sm_count, st, nullptr, true);
         CK(cudaGetLastError());
         hsc.resize(ng);
+        ring.resize(4 * (size_t)ng);
+        if ((rs = dnni_ensure(c, B.ring, sizeof(int) * 4 * (size_t)ng))) return rs;
+        k_ring_max<<<ng, 256, 0, st>>>(bt, a.pix, (int*)B.ring.p);
+        CK(cudaMemcpyAsync(ring.data(), B.ring.p, sizeof(int) * 4 * (size_t)ng, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(hsc.data(), a.sc, sizeof(Scalars) * ng, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(c->h_ctr, a.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -378,24 +441,35 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
             int mr2 = -1;
             for (int l = 0; l < kStatSlots; ++l) mr2 = std::max(mr2, hsc[k].max_r2[l]);
             // Every raster pixel's nearest-site distance d is below
-            // R = sqrt(R2 + 1) cells.  (B) With R <= hr no point outside the
-            // point box (the raster +- hr) is as near as the site found, so
-            // the found sites are exact.  (A) A pixel p outside the raster
-            // reaching a core cell q needs d(p) >= |p - q|; on the segment p-q
-            // the point c at L-inf distance hr - 1/2 from the core has a
-            // raster pixel p' within sqrt(2)/2, and d is 1-Lipschitz, so
-            // d(p') >= |c - q| - sqrt(2)/2 > hr - 1.21: R <= hr - 2 rules
-            // that out.
+            // R = sqrt(R2 + 1) cells.  (B) With R <= hp over the whole raster,
+            // no point outside the point box (the raster +- hp) is as near as
+            // the site found, so the found sites are exact.  (A) A pixel p
+            // outside the raster whose disc reaches a core cell q has
+            // d(p) >= |p - q|.  Let the segment p-q leave the raster through
+            // side s, and c be the point of the segment half a pixel inside
+            // that side's outermost line: |c - q| >= h_s - 1/2, and the pixel
+            // p' nearest c lies in the side's two outermost lines, within
+            // sqrt(2)/2 of c.  d is 1-Lipschitz, so d(p') >= |c - q| -
+            // sqrt(2)/2 > h_s - 1.21; R <= h_s - 2 over those two lines rules
+            // p out.  A side on the grid's edge has no pixel beyond it.
             const double R = std::sqrt((double)mr2 + 1.0);
-            const bool okA = all_raster[k] || R <= T.hr - 2;
-            const bool okB = all_buckets[k] || R <= T.hr;
-            if (!(okA && okB)) {
-                SegTile U = T;
-                U.hr = std::max(2 * T.hr, (int)std::ceil(R) + 3);
+            const bool okB = all_buckets[k] || R <= T.hp;
+            SegTile U = T;
+            bool again = !okB;
+            if (!okB) U.hp = std::max(2 * T.hp, (int)std::ceil(R) + 3);
+            for (int sd = 0; sd < 4; ++sd) {
+                if (clipped[4 * k + sd]) continue;
+                const double Rs = std::sqrt((double)ring[4 * k + sd] + 1.0);
+                if (Rs > T.h[sd] - 2) {
+                    U.h[sd] = std::max(2 * T.h[sd], (int)std::ceil(Rs) + 3);
+                    again = true;
+                }
+            }
+            if (again) {
                 queue.push_back(U);
                 continue;
             }
-            max_halo = std::max(max_halo, T.hr);
+            for (int sd = 0; sd < 4; ++sd) max_halo = std::max(max_halo, T.h[sd]);
             const dnni_tile& t = tl[k];
             const size_t w = (size_t)t.wp.ncols, h = (size_t)t.wp.nrows;
             CK(cudaMemcpy2DAsync(h_out + (size_t)T.y0 * s.ncols + T.x0, 4 * (size_t)s.ncols,
@@ -416,6 +490,8 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         stats->ms_total = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         stats->ms_upload = ms_up;
         stats->ms_bucket = ms_bk;
+        stats->ms_bound = std::chrono::duration<double, std::milli>(t_tiles - t_bound).count();
+        stats->ms_tiles = std::chrono::duration<double, std::milli>(clk::now() - t_tiles).count();
         stats->points = n;
         stats->cells = (int64_t)s.ncols * s.nrows;
         stats->tiles = ntiles;

@@ -89,7 +89,7 @@ class Segment(ctypes.Structure):
 
 class SegmentStats(ctypes.Structure):
     _fields_ = [("ms_total", ctypes.c_double), ("ms_upload", ctypes.c_double), ("ms_bucket", ctypes.c_double),
-                ("points", ctypes.c_int64), ("cells", ctypes.c_int64), ("tiles", ctypes.c_int64),
+                ("ms_bound", ctypes.c_double), ("ms_tiles", ctypes.c_double), ("points", ctypes.c_int64), ("cells", ctypes.c_int64), ("tiles", ctypes.c_int64),
                 ("tile_runs", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
                 ("max_halo", ctypes.c_int32), ("batches", ctypes.c_int32)]
 
