@@ -50,7 +50,7 @@ struct BatchTables {
     const int64_t* blk_base;     // blocks (== TileParams::blk_off)
     const int64_t* sup_base;     // superblocks (== TileParams::sup_off)
     const int* row1_base;        // rows of the block grid
-    const int* rt_base;          // 32 x 8 raster tiles
+    const int* rt_base;          // 32 x kTileY raster tiles
     const int* ct_base;          // 32 x 16 cell tiles
     const int* grow_base;        // grid rows
 };
@@ -429,8 +429,9 @@ struct FarSlot {
     int tile, pix, idx, pad;
 };
 
-// Dense pass.  One CTA per 32 x kTileY raster tile of a work package (blockDim
-// 32 x 8; warp w takes pixel rows w, w + 8, ... of the tile): the tile's bin window (bin rings
+// Dense pass.  One CTA per 32 x kTileY raster tile of a work package
+// (blockDim 32 x 8; warp w takes pixel rows w, w + 8, ... of the tile): the
+// tile's bin window (bin rings
 // of every pixel) is staged in shared memory and the rings are searched
 // there; windows too large for shared memory use the global arrays.  A warp
 // with pixels the rings do not settle appends its whole row as one group of
@@ -833,8 +834,9 @@ __device__ __forceinline__ void emit_span(int row, int a, int b, int ncols, int 
 
 // Span path: every pixel with R2 > rs^2 adds its disc as row spans
 // (+v at the first cell, -v after the last) to the per-row difference array.
-// One CTA per 32 x 8 raster tile; warp = 32 consecutive pixels of one row,
-// so one iteration's markers fall on two rows near each other in memory.
+// One CTA (32 x 8 threads) per 32 x kTileY raster tile; a warp takes 32
+// consecutive pixels of one row at a time (rows w, w + 8, ...), so one
+// iteration's markers fall on two rows near each other in memory.
 __global__ void __launch_bounds__(256) k_scatter_spans(BatchTables bt, const int2* __restrict__ pix,
                                                        const Scalars* __restrict__ sc,
                                                        unsigned long long* __restrict__ D_all,

@@ -129,7 +129,7 @@ struct HostBatch {
 };
 
 // Worklist capacity of a tile: every dense warp (32 pixels of a tile row, the
-// raster padded to whole 32 x 8 tiles) may append one group of 32 slots.
+// raster padded to whole 32 x kTileY tiles) may append one group of 32 slots.
 inline int64_t far_slots(const TileParams& t) {
     return (int64_t)((t.rw + kTileX - 1) / kTileX * kTileX) * ((t.rh + kTileY - 1) / kTileY * kTileY);
 }
