@@ -437,7 +437,7 @@ struct FarSlot {
 // with pixels the rings do not settle appends its whole row as one group of
 // 32 slots to the far worklist.  With no points every pixel is settled as
 // "no site".
-__global__ void __launch_bounds__(256, 3) k_near_dense(BatchTables bt, const int4* __restrict__ pts_all,
+__global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int4* __restrict__ pts_all,
                                                        const int* __restrict__ start_all, int2* __restrict__ pix,
                                                        uint32_t* __restrict__ site, FarSlot* __restrict__ far,
                                                        Scalars* __restrict__ sc, BatchCounters* __restrict__ ctr) {

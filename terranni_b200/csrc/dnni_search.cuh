@@ -700,9 +700,9 @@ DNNI_HD void decode_span_word(unsigned long long w, int K, long long zbase, long
     C = cb;
 }
 
-constexpr int kWinMaxBins = 2048;
+constexpr int kWinMaxBins = 1536;
 constexpr int kWinMaxRows = 256;
-constexpr int kWinMaxPts = 3072;
+constexpr int kWinMaxPts = 2560;
 constexpr size_t kDenseSmem = sizeof(int4) * kWinMaxPts + sizeof(int) * (2 * kWinMaxBins + 1);
 
 
