@@ -653,7 +653,7 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
 // batch's scratch (they run one after another on the compute stream).
 static dnni_status plan_slices(dnni_batch* b) {
     dnni_ctx* c = b->ctx;
-    constexpr int kSlices = 4;
+    constexpr int kSlices = 8;
     const int n = (int)b->tiles_in.size();
     const int S = (b->hb.n_rows >= (4 << 20) && n >= kSlices) ? kSlices : 1;
     b->sliced = S > 1;
