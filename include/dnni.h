@@ -353,6 +353,43 @@ dnni_status dnni_batch_autotune(dnni_ctx *ctx, const dnni_tile *tiles, int32_t n
                                 const uint32_t *d_gid, int32_t sample_tiles, dnni_batch_options *options,
                                 dnni_tune_report *report);
 
+/* ---- the reference's default semantics (compatibility mode) ----
+ *
+ * nni::performNNI as the reference computes it by default (timeRadius 0,
+ * plane algorithm; nni.cpp:870-944, cuda_nni.cu:407-503), on the GPU: each
+ * site covers only a square of half-side site_radius/sqrt(2) on a pixel
+ * lattice `scale` times finer than the cells (nni.cpp:183, 879-886); in it
+ * the site's float32 lifted plane competes by depth, the later-drawn site
+ * winning equal depths (GL_LEQUAL, nni.cpp:171-230, 733-737); each cell
+ * collects, over its square of half-side query_radius/sqrt(2), the z-codes
+ * floor((z - point_min + 1) * multiplier) of the pixels where its own plane
+ * is no deeper (nni.cpp:483-534, 538-549), sums them in int32 with
+ * wrap-around and truncates the division (cuda_nni.cu:423-503); heights are
+ * dequantised as nni.cpp:836-848 does (-9999 where no pixel counts).
+ * Planes are evaluated at pixel centres over half-open squares; the GL
+ * rasteriser's fill rule and depth interpolation are not reproduced.  Points
+ * are world coordinates (x, y, z doubles) in draw order; res_out (optional)
+ * receives the int32 division results.  Heights are row-major, row 0 the
+ * lowest y. */
+typedef struct dnni_compat_settings {   /* nni::Settings (nni.h:72-81), the fields used */
+    int32_t scale;
+    float cell_size;
+    float site_radius;
+    int32_t pad0;
+    double query_radius;
+    int32_t point_min;
+    int32_t multiplier;                 /* zMult (terranni.cpp:675-684) */
+    int32_t total_ncols, total_nrows;
+} dnni_compat_settings;
+
+typedef struct dnni_compat_wp {         /* nni::WorkPackage (nni.h:66-70) */
+    float origin_x, origin_y, grid_origin_x, grid_origin_y;
+    int32_t nrows, ncols;
+} dnni_compat_wp;
+
+dnni_status dnni_interpolate_compat(dnni_ctx *ctx, const dnni_compat_settings *settings, const dnni_compat_wp *wp,
+                                    const double *xyz, int64_t n, float *h_out, int32_t *res_out);
+
 /* ---- input: LAS point files ----
  *
  * Replaces the reference's nni_io::las_reader (las_reader.h:34-58,

@@ -1,0 +1,190 @@
+// dnni_compat.cuh -- the reference's own default semantics on the GPU
+// (dnni_interpolate_compat): square site regions, a pixel lattice `scale`
+// times finer than the cells, float32 lifted-plane depths with the
+// later-drawn site winning equal depths, square query regions, int32 z-codes
+// summed with wrap-around and a truncating divide.  Included by
+// dnni_engine.cu.
+//
+// Follows nni::performNNI for timeRadius == 0 with the plane algorithm:
+//   pixel_offset and raster size                   nni.cpp:879-886
+//   site squares, z-code, depth test (LEQUAL)      nni.cpp:171-230, 470-479, 538-549, 733-737
+//   query squares tested against the stored depth  nni.cpp:483-534, 803-807
+//   int32 numer/denom, truncating divide           cuda_nni.cu:423-448, 491-503
+//   dequantisation                                 nni.cpp:836-848
+// evaluating each plane at pixel centres over the half-open square
+// [x - r, x + r) x [y - r, y + r); the GL rasteriser's fill rule and its
+// depth interpolation are not reproduced.  Every floating-point operation is
+// written with an explicit rounding intrinsic, in the order the formulas
+// give, so that no multiply-add is fused and the results are those of the
+// same formulas evaluated in IEEE single and double precision on the host.
+#pragma once
+
+namespace dnni {
+
+struct CompatGeom {
+    double pixel_size, left, bottom, rs, rq, qspacing;
+    float hw;
+    int32_t xp, yp, ncols, nrows, z_offset, z_mult;
+    float ox, oy;
+};
+
+__device__ __forceinline__ float compat_plane_depth(float hw, float sx, float sy, float px, float py) {
+    const float zpx = __fdiv_rn(__fadd_rn(sx, hw), hw);
+    const float zpy = __fdiv_rn(__fadd_rn(sy, hw), hw);
+    const float zoff = __fadd_rn(__fmul_rn(zpx, zpx), __fmul_rn(zpy, zpy));
+    const float a = __fdiv_rn(__fmul_rn(-2.0f, zpx), hw);
+    const float b = __fdiv_rn(__fmul_rn(-2.0f, zpy), hw);
+    const float zx = __fadd_rn(px, hw), zy = __fadd_rn(py, hw);
+    return __fadd_rn(__fadd_rn(__fmul_rn(a, zx), __fmul_rn(b, zy)), zoff);
+}
+
+// Pixel index range [i0, i1] whose centres fall in [x0, x1) (one axis).
+__device__ __forceinline__ void compat_span(float x0, float x1, double left, double ps, long long n, long long& i0,
+                                            long long& i1) {
+    i0 = (long long)ceil(__dsub_rn(__ddiv_rn(__dsub_rn((double)x0, left), ps), 0.5));
+    i1 = (long long)ceil(__dsub_rn(__ddiv_rn(__dsub_rn((double)x1, left), ps), 0.5)) - 1;
+    if (i0 < 0) i0 = 0;
+    if (i1 > n - 1) i1 = n - 1;
+}
+
+__device__ __forceinline__ float compat_centre(long long p, double base, double ps) {
+    return __double2float_rn(__dadd_rn(base, __dmul_rn((double)p + 0.5, ps)));
+}
+
+// Order-preserving map of a float's bits to an unsigned integer.
+__device__ __forceinline__ uint32_t compat_order(float d) {
+    const uint32_t u = __float_as_uint(d);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float compat_unorder(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+// Site pass: one thread per point (draw order k); every pixel of its square
+// keeps the smallest depth, the largest k among equal depths (the depth
+// test's later-draw-wins), as the 64-bit key order(d) << 32 | ~k.
+__global__ void __launch_bounds__(256) k_compat_sites(CompatGeom G, const double* __restrict__ xyz, int64_t n,
+                                                      unsigned long long* __restrict__ key) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const float sx = __double2float_rn(__dsub_rn(xyz[3 * k], (double)G.ox));
+        const float sy = __double2float_rn(__dsub_rn(xyz[3 * k + 1], (double)G.oy));
+        const float x0 = __double2float_rn(__dsub_rn((double)sx, G.rs)), x1 = __double2float_rn(__dadd_rn((double)sx, G.rs));
+        const float y0 = __double2float_rn(__dsub_rn((double)sy, G.rs)), y1 = __double2float_rn(__dadd_rn((double)sy, G.rs));
+        long long i0, i1, j0, j1;
+        compat_span(x0, x1, G.left, G.pixel_size, G.xp, i0, i1);
+        compat_span(y0, y1, G.bottom, G.pixel_size, G.yp, j0, j1);
+        const unsigned long long low = 0xFFFFFFFFull - (unsigned long long)k;
+        for (long long pj = j0; pj <= j1; ++pj) {
+            const float cy = compat_centre(pj, G.bottom, G.pixel_size);
+            for (long long pi = i0; pi <= i1; ++pi) {
+                const float cx = compat_centre(pi, G.left, G.pixel_size);
+                const float d = compat_plane_depth(G.hw, sx, sy, cx, cy);
+                atomicMin(&key[pj * G.xp + pi], ((unsigned long long)compat_order(d) << 32) | low);
+            }
+        }
+    }
+}
+
+// z-code of a point: floor((z + zOffset + 1) * zMult) (nni.cpp:538-549).
+__device__ __forceinline__ uint32_t compat_zcode(double z, int z_offset, int z_mult) {
+    return (uint32_t)(long long)floor(__dmul_rn(__dadd_rn(__dadd_rn(z, (double)z_offset), 1.0), (double)z_mult));
+}
+
+// Query pass and divide: one thread per cell, over the pixels of its square;
+// a pixel counts when it holds a site with a non-zero z-code and the cell's
+// own plane is no deeper there (cuda_nni.cu:423-448).
+__global__ void __launch_bounds__(256) k_compat_cells(CompatGeom G, const double* __restrict__ xyz,
+                                                      const unsigned long long* __restrict__ key,
+                                                      float* __restrict__ h, int32_t* __restrict__ res) {
+    const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (w >= (int64_t)G.ncols * G.nrows) return;
+    const int i = (int)(w % G.ncols), j = (int)(w / G.ncols);
+    const float qx = __double2float_rn(__dmul_rn((double)i, G.qspacing));
+    const float qy = __double2float_rn(__dmul_rn((double)j, G.qspacing));
+    const float x0 = __double2float_rn(__dsub_rn((double)qx, G.rq)), x1 = __double2float_rn(__dadd_rn((double)qx, G.rq));
+    const float y0 = __double2float_rn(__dsub_rn((double)qy, G.rq)), y1 = __double2float_rn(__dadd_rn((double)qy, G.rq));
+    long long i0, i1, j0, j1;
+    compat_span(x0, x1, G.left, G.pixel_size, G.xp, i0, i1);
+    compat_span(y0, y1, G.bottom, G.pixel_size, G.yp, j0, j1);
+    uint32_t numer = 0;
+    int32_t denom = 0;
+    for (long long pj = j0; pj <= j1; ++pj) {
+        const float cy = compat_centre(pj, G.bottom, G.pixel_size);
+        for (long long pi = i0; pi <= i1; ++pi) {
+            const unsigned long long kk = key[pj * G.xp + pi];
+            if (kk == ~0ull) continue;                        // no site drew here
+            const int64_t k = (int64_t)(0xFFFFFFFFull - (kk & 0xFFFFFFFFull));
+            const uint32_t zc = compat_zcode(xyz[3 * k + 2], G.z_offset, G.z_mult);
+            if (zc == 0) continue;
+            const float cx = compat_centre(pi, G.left, G.pixel_size);
+            const float d = compat_plane_depth(G.hw, qx, qy, cx, cy);
+            if (d <= compat_unorder((uint32_t)(kk >> 32))) {
+                numer += zc;                                  // int32 sum with wrap, as the atomicAdd
+                denom += 1;
+            }
+        }
+    }
+    const int32_t r = denom == 0 ? -9999 * G.z_mult : (int32_t)numer / denom;
+    if (res) res[w] = r;
+    double z = __ddiv_rn((double)r, (double)G.z_mult);
+    if (z != -9999.0) z = __dsub_rn(__dsub_rn(z, (double)G.z_offset), 1.0);
+    h[w] = __double2float_rn(z);
+}
+
+}  // namespace dnni
+
+extern "C" dnni_status dnni_interpolate_compat(dnni_ctx* c, const dnni_compat_settings* s, const dnni_compat_wp* wp,
+                                               const double* xyz, int64_t n, float* h_out, int32_t* res_out) {
+    if (!c || !s || !wp || !h_out || n < 0 || (n > 0 && !xyz)) return DNNI_E_INVAL;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    if (s->scale <= 0 || !(s->cell_size > 0) || wp->nrows <= 0 || wp->ncols <= 0 || s->multiplier <= 0)
+        return set_err(c, DNNI_E_INVAL, "scale, cell size, grid sides and multiplier must be positive");
+    if ((uint64_t)n >= 0xFFFFFFFFull) return set_err(c, DNNI_E_INVAL, "too many points for 32-bit draw order");
+    // geometry as nni::performNNI derives it (nni.cpp:879-886, 186-189)
+    CompatGeom G;
+    G.qspacing = s->cell_size;
+    G.pixel_size = G.qspacing / s->scale;
+    const float qr = (float)s->query_radius;
+    const int pixel_offset = (int)std::ceil((qr - std::floor(s->scale / 2.0) * G.pixel_size) / G.pixel_size) + 1;
+    const long long xp = (long long)wp->ncols * s->scale + 2LL * pixel_offset;
+    const long long yp = (long long)wp->nrows * s->scale + 2LL * pixel_offset;
+    if (xp <= 0 || yp <= 0 || xp > 65535 || yp > 65535 || xp * yp > (1LL << 31))
+        return set_err(c, DNNI_E_INVAL, "raster of the work package too large");
+    G.xp = (int32_t)xp;
+    G.yp = (int32_t)yp;
+    G.left = 0 - (G.qspacing / 2.0) - (pixel_offset * G.pixel_size);
+    G.bottom = G.left;
+    G.hw = (float)(((wp->nrows - 1) * G.qspacing) / 2.0);
+    G.rs = s->site_radius / std::sqrt(2.0);
+    G.rq = qr / std::sqrt(2.0);
+    G.ncols = wp->ncols;
+    G.nrows = wp->nrows;
+    G.z_offset = -1 * s->point_min;
+    G.z_mult = s->multiplier;
+    G.ox = wp->origin_x;
+    G.oy = wp->origin_y;
+    const int64_t cells = (int64_t)wp->ncols * wp->nrows;
+    dnni_status rs;
+    // scratch: the pixel keys in the context's span-word buffer, points and
+    // outputs in its staging buffers
+    if ((rs = dnni_ensure(c, c->scr.D, sizeof(unsigned long long) * (size_t)(xp * yp))) ||
+        (rs = dnni_ensure(c, c->in_xyz, sizeof(double) * 3 * (size_t)std::max<int64_t>(n, 1))) ||
+        (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)) ||
+        (res_out && (rs = dnni_ensure(c, c->out_site, sizeof(int32_t) * (size_t)cells))))
+        return rs;
+    cudaStream_t st = c->stream;
+    unsigned long long* key = (unsigned long long*)c->scr.D.p;
+    CK(cudaMemsetAsync(key, 0xFF, sizeof(unsigned long long) * (size_t)(xp * yp), st));
+    if (n > 0) {
+        CK(cudaMemcpyAsync(c->in_xyz.p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
+        k_compat_sites<<<c->sm_count * 8, 256, 0, st>>>(G, (const double*)c->in_xyz.p, n, key);
+    }
+    k_compat_cells<<<(int)((cells + 255) / 256), 256, 0, st>>>(G, (const double*)c->in_xyz.p, key, (float*)c->out_h.p,
+                                                               res_out ? (int32_t*)c->out_site.p : nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_out, c->out_h.p, sizeof(float) * (size_t)cells, cudaMemcpyDeviceToHost, st));
+    if (res_out) CK(cudaMemcpyAsync(res_out, c->out_site.p, sizeof(int32_t) * (size_t)cells, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return DNNI_OK;
+}

@@ -1103,3 +1103,4 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
 
 #include "dnni_segment.cuh"
 #include "dnni_server.cuh"
+#include "dnni_compat.cuh"

@@ -142,6 +142,17 @@ class LasHeader(ctypes.Structure):
         return d
 
 
+class CompatSettings(ctypes.Structure):
+    _fields_ = [("scale", ctypes.c_int32), ("cell_size", ctypes.c_float), ("site_radius", ctypes.c_float),
+                ("pad0", ctypes.c_int32), ("query_radius", ctypes.c_double), ("point_min", ctypes.c_int32),
+                ("multiplier", ctypes.c_int32), ("total_ncols", ctypes.c_int32), ("total_nrows", ctypes.c_int32)]
+
+
+class CompatWP(ctypes.Structure):
+    _fields_ = [("origin_x", ctypes.c_float), ("origin_y", ctypes.c_float), ("grid_origin_x", ctypes.c_float),
+                ("grid_origin_y", ctypes.c_float), ("nrows", ctypes.c_int32), ("ncols", ctypes.c_int32)]
+
+
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("pad", ctypes.c_int32)]
@@ -195,6 +206,8 @@ _SIGS = {
                         ctypes.c_double, ctypes.c_float, ctypes.c_int32], ctypes.c_int),
     "dnni_write_grid_bin": ([ctypes.c_char_p, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                              ctypes.c_double, ctypes.c_float], ctypes.c_int),
+    "dnni_interpolate_compat": ([_P, ctypes.POINTER(CompatSettings), ctypes.POINTER(CompatWP), _P, ctypes.c_int64,
+                                 _P, _P], ctypes.c_int),
     "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
                              ctypes.POINTER(BatchOptions), ctypes.POINTER(TuneReport)], ctypes.c_int),
 }
@@ -341,6 +354,16 @@ class Engine:
     def server(self, xyz, **options):
         """dnni_server_create over host points (absolute LAS xyz) -> Server."""
         return Server(self, xyz, **options)
+
+    def interpolate_compat(self, settings: CompatSettings, wp: CompatWP, pts_world):
+        """dnni_interpolate_compat (the reference's default semantics) ->
+        (heights, int32 division results)."""
+        pts = np.ascontiguousarray(pts_world, dtype=np.float64).reshape(-1, 3)
+        h = np.empty((wp.nrows, wp.ncols), np.float32)
+        res = np.empty((wp.nrows, wp.ncols), np.int32)
+        self._check(lib().dnni_interpolate_compat(self._h, ctypes.byref(settings), ctypes.byref(wp), _ptr(pts),
+                                                  pts.shape[0], _ptr(h), _ptr(res)))
+        return h, res
 
     def clear(self):
         self._check(lib().dnni_clear(self._h))
