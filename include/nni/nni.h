@@ -23,6 +23,13 @@
  * (nni.cpp:310-316); here every failure throws nni::Error carrying the
  * engine's status and message.
  *
+ * setCompatMode(true) switches performNNI to the reference's own default
+ * semantics instead (dnni_interpolate_compat): square site and query regions,
+ * a pixel lattice Settings::scale times finer than the cells, float32 plane
+ * depths with the later-drawn site winning ties, int32 z-codes quantised by
+ * Settings::pointMin and Settings::multiplier, truncating divide.  Points are
+ * then taken as world doubles, without the LAS quantisation.
+ *
  * Not implemented: space-time interpolation (timeRadius > 0, nni.cpp:117-157,
  * 902-933) throws nni::Error with DNNI_E_INVAL.
  */
@@ -104,9 +111,11 @@ struct State {
     Settings s{};
     double xy_scale = 0.01, z_scale = 0.01;
     int device = 0;
+    bool compat = false;
     double ms_points = 0, ms_engine = 0, ms_write = 0;
     long long calls = 0;
     std::vector<int32_t> xyz;
+    std::vector<double> world;
     std::vector<uint32_t> gid;
     std::vector<float> h;
 };
@@ -154,6 +163,10 @@ inline void setCoordinateScale(double xy_scale, double z_scale) {
     detail::state().xy_scale = xy_scale;
     detail::state().z_scale = z_scale;
 }
+
+/* Reference-default semantics for the following performNNI calls
+ * (extension; the reference's behaviour with its default build options). */
+inline void setCompatMode(bool on) { detail::state().compat = on; }
 
 /* Device used by the next init() (extension; the reference uses device 0,
  * cuda_nni.cu:659). */
@@ -226,6 +239,7 @@ inline void performNNI(const WorkPackage& wp, tpie::ami::stream<OutPoint>& out, 
     bool foundSeek = false;
     st.xyz.clear();
     st.gid.clear();
+    st.world.clear();
     Point4D* pp;
     uint32_t order = 0;
     while (vec.read_item(&pp) == tpie::ami::NO_ERROR) {
@@ -235,7 +249,9 @@ inline void performNNI(const WorkPackage& wp, tpie::ami::stream<OutPoint>& out, 
             finalSeekTo = seekto;
             foundSeek = true;
         }
-        if (std::fabs(t - p.t) <= timeRadius + 0.000001) {
+        if (std::fabs(t - p.t) <= timeRadius + 0.000001 && st.compat) {
+            st.world.insert(st.world.end(), p.p, p.p + 3);
+        } else if (std::fabs(t - p.t) <= timeRadius + 0.000001) {
             const double X = std::llround((p.p[0] - wp.origin_x) / st.xy_scale);
             const double Y = std::llround((p.p[1] - wp.origin_y) / st.xy_scale);
             const double Z = std::llround(p.p[2] / st.z_scale);
@@ -253,14 +269,31 @@ inline void performNNI(const WorkPackage& wp, tpie::ami::stream<OutPoint>& out, 
     if (!useDelta) vec.seek(finalSeekTo);
     else vec.seek(seekto);
 
-    dnni_workpackage d = detail::to_dnni(wp, -1);
     st.h.resize((size_t)wp.ncols * wp.nrows);
-    dnni_stats stats{};
-    const int64_t n = (int64_t)st.gid.size();
-    detail::check(dnni_interpolate_segment(st.ctx, &d, n ? st.xyz.data() : nullptr, n ? st.gid.data() : nullptr, n,
-                                           st.h.data(), nullptr, &stats),
-                  "performNNI");
-    st.ms_engine += stats.ms_total;
+    if (st.compat) {
+        dnni_compat_settings cs{};
+        cs.scale = st.s.scale;
+        cs.cell_size = st.s.cell_size;
+        cs.site_radius = st.s.site_radius;
+        cs.query_radius = st.s.query_radius;
+        cs.point_min = st.s.pointMin;
+        cs.multiplier = st.s.multiplier;
+        cs.total_ncols = st.s.ncols;
+        cs.total_nrows = st.s.nrows;
+        const dnni_compat_wp cw{wp.origin_x, wp.origin_y, wp.grid_origin_x, wp.grid_origin_y, wp.nrows, wp.ncols};
+        const int64_t n = (int64_t)st.world.size() / 3;
+        detail::check(dnni_interpolate_compat(st.ctx, &cs, &cw, n ? st.world.data() : nullptr, n, st.h.data(),
+                                              nullptr),
+                      "performNNI");
+    } else {
+        dnni_workpackage d = detail::to_dnni(wp, -1);
+        dnni_stats stats{};
+        const int64_t n = (int64_t)st.gid.size();
+        detail::check(dnni_interpolate_segment(st.ctx, &d, n ? st.xyz.data() : nullptr, n ? st.gid.data() : nullptr,
+                                               n, st.h.data(), nullptr, &stats),
+                      "performNNI");
+        st.ms_engine += stats.ms_total;
+    }
     st.calls++;
     for (int i = 0; i < wp.ncols; i++) {
         for (int j = 0; j < wp.nrows; j++) {

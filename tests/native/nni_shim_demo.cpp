@@ -4,15 +4,18 @@
 //
 // usage: nni_shim_demo <points.bin> <out.bin> <ncols> <nrows> <cell_m> <origin_x> <origin_y>
 //                      <grid_origin_x> <grid_origin_y> <total_ncols> <total_nrows> <query_radius_m>
-// points.bin holds raw nni::Point4D records; out.bin receives raw nni::OutPoint
-// records.  Exit status: 0, or the engine status of an nni::Error.
+//                      [<scale> <site_radius_m> <pointMin> <multiplier>]
+// The four optional arguments switch the shim to the reference's default
+// semantics (nni::setCompatMode) with those settings.  points.bin holds raw
+// nni::Point4D records; out.bin receives raw nni::OutPoint records.  Exit
+// status: 0, or the engine status of an nni::Error.
 #include <cstdio>
 #include <cstdlib>
 
 #include <nni/nni.h>
 
 int main(int argc, char** argv) {
-    if (argc != 13) {
+    if (argc != 13 && argc != 17) {
         std::fprintf(stderr, "usage: %s points.bin out.bin ncols nrows cell_m ox oy gox goy total_ncols total_nrows qr\n",
                      argv[0]);
         return 64;
@@ -24,6 +27,13 @@ int main(int argc, char** argv) {
     s.nrows = std::atoi(argv[11]);
     s.query_radius = std::atof(argv[12]);
     s.site_radius = (float)s.query_radius;
+    if (argc == 17) {
+        s.scale = std::atoi(argv[13]);
+        s.site_radius = (float)std::atof(argv[14]);
+        s.pointMin = std::atoi(argv[15]);
+        s.multiplier = std::atoi(argv[16]);
+        nni::setCompatMode(true);
+    }
     nni::WorkPackage wp{};
     wp.ncols = std::atoi(argv[3]);
     wp.nrows = std::atoi(argv[4]);

@@ -64,3 +64,36 @@ def test_reference_caller_matches_oracle(tmp_path, oracle):
     assert np.array_equal(got["i"], np.array([w[0] for w in want], np.int32))
     assert np.array_equal(got["j"], np.array([w[1] for w in want], np.int32))
     assert np.array_equal(got["h"].view(np.uint32), np.array([w[2] for w in want], np.float32).view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_reference_caller_compat_mode_matches_oracle(tmp_path, oracle):
+    """nni::setCompatMode: the same caller, the reference's default semantics
+    (scaling 5, site radius 5 m, pointMin/multiplier quantisation)."""
+    exe = build_demo()
+    ncols, nrows, cell_m, qr, scale, sr, pmin = 40, 30, 2.0, 4.99, 5, 5.0, 0
+    ox, oy, gox, goy, tot_c, tot_r = 500.0, 700.0, 3, 4, 40, 32
+    rng = np.random.default_rng(9)
+    n = 3000
+    pts = np.zeros(n, POINT4D)
+    pts["x"] = ox + rng.uniform(-4, 84, n)
+    pts["y"] = oy + rng.uniform(-4, 64, n)
+    pts["z"] = rng.uniform(10, 20, n)
+    mult = oracle.compat_multiplier(sr, scale, cell_m, float(pts["z"].max()), pmin)
+    pin, pout = tmp_path / "pts.bin", tmp_path / "out.bin"
+    pts.tofile(pin)
+    r = subprocess.run([exe, str(pin), str(pout), str(ncols), str(nrows), str(cell_m), str(ox), str(oy), str(gox),
+                        str(goy), str(tot_c), str(tot_r), str(qr), str(scale), str(sr), str(pmin), str(mult)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(pout, OUTPOINT)
+    s = oracle.CompatSettings(scale=scale, cell_size=cell_m, site_radius=sr, query_radius=qr, point_min=pmin,
+                              multiplier=mult, total_ncols=tot_c, total_nrows=tot_r)
+    cwp = oracle.CompatWP(origin_x=ox, origin_y=oy, grid_origin_x=gox, grid_origin_y=goy, nrows=nrows, ncols=ncols)
+    ref, _ = oracle.compat(s, cwp, np.stack([pts["x"], pts["y"], pts["z"]], 1))
+    want = [(i + gox, j + goy, ref[j, i]) for i in range(ncols) for j in range(nrows)
+            if i + gox < tot_c and j + goy < tot_r]
+    assert got.shape[0] == len(want)
+    assert np.array_equal(got["i"], np.array([w[0] for w in want], np.int32))
+    assert np.array_equal(got["h"].view(np.uint32), np.array([w[2] for w in want], np.float32).view(np.uint32))
+    assert (ref != np.float32(-9999.0)).mean() > 0.9
