@@ -390,6 +390,39 @@ typedef struct dnni_compat_wp {         /* nni::WorkPackage (nni.h:66-70) */
 dnni_status dnni_interpolate_compat(dnni_ctx *ctx, const dnni_compat_settings *settings, const dnni_compat_wp *wp,
                                     const double *xyz, int64_t n, float *h_out, int32_t *res_out);
 
+/* ---- space-time interpolation: nni::performNNI with timeRadius > 0 ----
+ *
+ * Replaces the slice loop of nni::performNNI (nni.cpp:902-933) with its
+ * per-slice site drawing (nni.cpp:722-790; drawPlane's time term,
+ * nni.cpp:171-230) and query drawing lifted by the slice offset
+ * (nni.cpp:483-493), in the canonical semantics of the 2-D path:
+ *   slices ts = cur_time + j, j = -time_radius .. time_radius;
+ *   the sites of slice ts are the points whose time t has |ts - t| <=
+ *   time_radius (nni.cpp:770), each at lifted squared distance
+ *   dx^2 + dy^2 + ((ts - t) * time_scale)^2 from a pixel (time_scale = LAS
+ *   units per time step; the reference's GL units make one time step one
+ *   metre); a pixel's site is the lifted-nearest one, ties to the lower
+ *   input index (the earlier point of the stream);
+ *   cell q (at cur_time) takes pixel p of slice ts iff
+ *   |q - p|^2 * cell^2 + (j * time_scale)^2 <= that lifted distance;
+ *   Z and C are summed over every slice; h as in the 2-D path.
+ * time_radius = 0 gives exactly dnni_interpolate_segment over the points
+ * with t == cur_time.  Points whose time is farther than 2 * time_radius from
+ * cur_time take part in no slice and may be passed or left out.
+ * Limits: 0 <= time_radius <= 16, time_scale > 0,
+ * time_radius * time_scale <= 2^30; (2 * time_radius + 1) x raster pixels
+ * < 2^31. */
+typedef struct dnni_st_options {
+    int32_t cur_time;       /* curTime of nni::performNNI (integer times) */
+    int32_t time_radius;    /* timeRadius (terranni --time-radius) */
+    int32_t time_scale;     /* LAS units per time step in the lifted distance */
+    int32_t pad;
+} dnni_st_options;
+
+dnni_status dnni_interpolate_spacetime(dnni_ctx *ctx, const dnni_workpackage *wp, const dnni_st_options *opt,
+                                       const int32_t *xyz, const int32_t *t, int64_t n, float *h_out,
+                                       dnni_stats *stats);
+
 /* ---- input: LAS point files ----
  *
  * Replaces the reference's nni_io::las_reader (las_reader.h:34-58,

@@ -651,3 +651,144 @@ int32_t orc_compat_multiplier(float site_radius, int32_t scale, float cell_size,
     }
     return m;
 }
+
+/* ------------------------------------------------------------------ */
+/* space-time (3-D) interpolation, timeRadius > 0                       */
+/* ------------------------------------------------------------------ */
+
+/* Canonical restatement of nni::performNNI with a time radius
+ * (nni.cpp:902-933 slice loop, nni.cpp:722-790 site selection per slice,
+ * nni.cpp:171-230 drawPlane's time term timeOffset^2 in the plane offset,
+ * nni.cpp:483-493 query planes lifted by the slice offset):
+ *   slices ts = cur + j, j = -rt..rt;
+ *   the sites of slice ts are the points with |ts - t| <= rt, each at lifted
+ *   squared distance d_l^2 = dx^2 + dy^2 + ((ts - t) * tau)^2 from a pixel
+ *   (tau = LAS units per time step); s(p) = min (d_l^2, index, z);
+ *   cell q (at time cur) takes pixel p of slice ts iff
+ *   |q - p|^2 * cell^2 + (j * tau)^2 <= d_l^2, i.e. |q - p|^2 <= R2 =
+ *   floor((d_l^2 - (j tau)^2) / cell^2), none when negative (capped as 2-D);
+ *   Z and C are summed over all slices, h as orc_height.
+ * Ties go to the lower input index (the earlier point of the stream).
+ * brute = 1: every point for every (slice, pixel); brute = 0: one k-d tree
+ * per time value, whose 2-D nearest site plus the value's constant time term
+ * is that value's best -- the minimum over the values is s(p). */
+static int st_scatter_layer(const orc_wp *wp, const int32_t r[4], const int32_t *sz, const int32_t *r2,
+                            int64_t *Z, int64_t *C) {
+    int64_t rw = r[2] - r[0], rh = r[3] - r[1];
+    int64_t nc = wp->ncols, nr = wp->nrows;
+    for (int64_t j = 0; j < rh; j++)
+        for (int64_t i = 0; i < rw; i++) {
+            int64_t R2 = r2[j * rw + i];
+            if (R2 < 0) continue;
+            int64_t px = r[0] + i, py = r[1] + j, z = sz[j * rw + i];
+            int64_t rr = (int64_t)isqrt_u64((uint64_t)R2);
+            for (int64_t dy = -rr; dy <= rr; dy++) {
+                int64_t row = py + dy;
+                if (row < 0 || row >= nr) continue;
+                int64_t w = (int64_t)isqrt_u64((uint64_t)(R2 - dy * dy));
+                int64_t a = px - w, b = px + w;
+                if (a < 0) a = 0;
+                if (b > nc - 1) b = nc - 1;
+                if (a > b) continue;
+                Z[row * nc + a] += z; C[row * nc + a] += 1;
+                if (b + 1 < nc) { Z[row * nc + b + 1] -= z; C[row * nc + b + 1] -= 1; }
+            }
+        }
+    return ORC_OK;
+}
+
+static int32_t st_r2(uint64_t dl2, int64_t jt, int64_t cs2, int64_t cap) {
+    uint64_t q2 = (uint64_t)(jt * jt);
+    if (dl2 < q2) return -1;
+    uint64_t v = (dl2 - q2) / (uint64_t)cs2;
+    return (int32_t)(v > (uint64_t)cap ? (uint64_t)cap : v);
+}
+
+int orc_interpolate_st(const orc_wp *wp, const int32_t *xyz, const int32_t *tt, int64_t n, int32_t cur,
+                       int32_t rt, int32_t tau, int brute, float *h, int64_t *Zout, int64_t *Cout) {
+    int32_t r[4];
+    if (check_wp(wp, r) || rt < 0 || rt > 16 || tau <= 0 || (int64_t)rt * tau > (1LL << 30)) return ORC_E_INVAL;
+    int64_t rw = r[2] - r[0], rh = r[3] - r[1], npix = rw * rh;
+    int64_t cells = (int64_t)wp->ncols * wp->nrows;
+    int64_t cap = r2_cap(wp, r), cs2 = (int64_t)wp->cell_size * wp->cell_size;
+    int nv = 4 * rt + 1;
+    int64_t *Z = Zout ? Zout : (int64_t *)malloc(sizeof(int64_t) * (size_t)cells);
+    int64_t *C = Cout ? Cout : (int64_t *)malloc(sizeof(int64_t) * (size_t)cells);
+    int32_t *sz = (int32_t *)malloc(sizeof(int32_t) * (size_t)npix);
+    int32_t *r2 = (int32_t *)malloc(sizeof(int32_t) * (size_t)npix);
+    kdtree *kd = (kdtree *)calloc((size_t)nv, sizeof(kdtree));
+    int64_t *cnt = (int64_t *)calloc((size_t)nv, sizeof(int64_t));
+    int rc = ORC_E_NOMEM;
+    if (!Z || !C || !sz || !r2 || !kd || !cnt) goto out;
+    memset(Z, 0, sizeof(int64_t) * (size_t)cells);
+    memset(C, 0, sizeof(int64_t) * (size_t)cells);
+    if (!brute) {
+        /* per time value: the points with that time, in input order */
+        int32_t *sx = (int32_t *)malloc(sizeof(int32_t) * 3 * (size_t)(n > 0 ? n : 1));
+        uint32_t *sg = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+        if (!sx || !sg) { free(sx); free(sg); goto out; }
+        for (int v = 0; v < nv; v++) {
+            int64_t m = 0;
+            for (int64_t k = 0; k < n; k++)
+                if ((int64_t)tt[k] == (int64_t)cur - 2 * rt + v) {
+                    sx[3 * m] = xyz[3 * k]; sx[3 * m + 1] = xyz[3 * k + 1]; sx[3 * m + 2] = xyz[3 * k + 2];
+                    sg[m++] = (uint32_t)k;
+                }
+            cnt[v] = m;
+            if (m > 0 && kd_build(&kd[v], sx, sg, m)) { free(sx); free(sg); goto out; }
+        }
+        free(sx); free(sg);
+    }
+    for (int s = 0; s <= 2 * rt; s++) {
+        int64_t ts = (int64_t)cur - rt + s, jt = (int64_t)(s - rt) * tau;
+        for (int64_t j = 0; j < rh; j++)
+            for (int64_t i = 0; i < rw; i++) {
+                int64_t qx = (int64_t)wp->origin_x + (r[0] + i) * (int64_t)wp->cell_size;
+                int64_t qy = (int64_t)wp->origin_y + (r[1] + j) * (int64_t)wp->cell_size;
+                uint64_t bd = UINT64_MAX;
+                uint32_t bg = 0xFFFFFFFFu;
+                int32_t bz = INT32_MAX;
+                if (brute) {
+                    for (int64_t k = 0; k < n; k++) {
+                        int64_t dt = ts - tt[k];
+                        if (dt < -rt || dt > rt) continue;
+                        int64_t dx = xyz[3 * k] - qx, dy = xyz[3 * k + 1] - qy;
+                        uint64_t d2 = (uint64_t)(dx * dx) + (uint64_t)(dy * dy) + (uint64_t)(dt * tau * dt * tau);
+                        int32_t z = xyz[3 * k + 2];
+                        if (d2 < bd || (d2 == bd && ((uint32_t)k < bg || ((uint32_t)k == bg && z < bz)))) {
+                            bd = d2; bg = (uint32_t)k; bz = z;
+                        }
+                    }
+                } else {
+                    for (int v = s; v <= s + 2 * rt; v++) {
+                        if (!cnt[v]) continue;
+                        int64_t dt = ts - ((int64_t)cur - 2 * rt + v);
+                        nn_best b = { INT64_MAX, 0xFFFFFFFFu, INT32_MAX };
+                        kd_query_rec(&kd[v], 0, 0, cnt[v], qx, qy, &b);
+                        uint64_t d2 = (uint64_t)b.d2 + (uint64_t)(dt * tau * dt * tau);
+                        if (d2 < bd || (d2 == bd && (b.gid < bg || (b.gid == bg && b.z < bz)))) {
+                            bd = d2; bg = b.gid; bz = b.z;
+                        }
+                    }
+                }
+                sz[j * rw + i] = bz;
+                r2[j * rw + i] = bg == 0xFFFFFFFFu ? -1 : st_r2(bd, jt, cs2, cap);
+            }
+        st_scatter_layer(wp, r, sz, r2, Z, C);
+    }
+    for (int64_t row = 0; row < wp->nrows; row++) {
+        int64_t a = 0, b = 0;
+        for (int64_t x = 0; x < wp->ncols; x++) {
+            a += Z[row * wp->ncols + x]; b += C[row * wp->ncols + x];
+            Z[row * wp->ncols + x] = a; C[row * wp->ncols + x] = b;
+        }
+    }
+    if (h) finalize_grid(wp, Z, C, h);
+    rc = ORC_OK;
+out:
+    if (kd) for (int v = 0; v < nv; v++) if (cnt && cnt[v]) kd_free(&kd[v]);
+    free(kd); free(cnt); free(sz); free(r2);
+    if (!Zout) free(Z);
+    if (!Cout) free(C);
+    return rc;
+}

@@ -87,6 +87,9 @@ def lib():
         L.orc_compat_multiplier.argtypes = [ctypes.c_float, ctypes.c_int32, ctypes.c_float,
                                             ctypes.c_double, ctypes.c_int32]
         L.orc_compat_multiplier.restype = ctypes.c_int32
+        L.orc_interpolate_st.argtypes = [ctypes.POINTER(WorkPackage), P, P, i64, ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.c_int32, ctypes.c_int, P, P, P]
+        L.orc_interpolate_st.restype = ctypes.c_int
         L.orc_height.argtypes = [i64, i64, ctypes.c_double, ctypes.c_double, ctypes.c_float]
         L.orc_height.restype = ctypes.c_float
         _lib = L
@@ -151,6 +154,23 @@ def interpolate(wp, xyz, gid=None, brute=False):
     if rc:
         raise ValueError(f"oracle interpolate failed: {rc}")
     return {"h": h, "site": site, "Z": Z, "C": C}
+
+
+def interpolate_spacetime(wp, xyz, t, cur_time, time_radius, time_scale, brute=False):
+    """Space-time canonical NNI (slices cur - rt .. cur + rt, lifted time
+    distance, time_scale LAS units per time step) -> dict(h, Z, C)."""
+    xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
+    t = np.ascontiguousarray(t, np.int32).reshape(-1)
+    if t.shape[0] != xyz.shape[0]:
+        raise ValueError("one time per point")
+    h = np.empty((wp.nrows, wp.ncols), np.float32)
+    Z = np.empty((wp.nrows, wp.ncols), np.int64)
+    C = np.empty((wp.nrows, wp.ncols), np.int64)
+    rc = lib().orc_interpolate_st(ctypes.byref(wp), _ptr(xyz), _ptr(t), xyz.shape[0], int(cur_time),
+                                  int(time_radius), int(time_scale), 1 if brute else 0, _ptr(h), _ptr(Z), _ptr(C))
+    if rc:
+        raise ValueError(f"oracle interpolate_spacetime failed: {rc}")
+    return {"h": h, "Z": Z, "C": C}
 
 
 def work_stats(wp, r2):

@@ -961,7 +961,8 @@ void dnni_free_all(dnni_ctx* c) {
     release_scratch(c, c->scr);
     release_scratch(c, c->seg_scr);
     c->seg.release(c);
-    DevBuf* bufs[] = {&c->in_xyz, &c->in_gid, &c->out_h, &c->out_site};
+    DevBuf* bufs[] = {&c->in_xyz, &c->in_gid, &c->out_h, &c->out_site, &c->st.xyz, &c->st.idx, &c->st.site,
+                      &c->st.hv, &c->st.pix};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
 
@@ -1104,3 +1105,4 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
 #include "dnni_segment.cuh"
 #include "dnni_server.cuh"
 #include "dnni_compat.cuh"
+#include "dnni_spacetime.cuh"

@@ -52,6 +52,11 @@ struct SegBufs {
     void release(dnni_ctx* c);
 };
 
+// Device buffers of the space-time driver (grow-only until dnni_clear).
+struct StBufs {
+    DevBuf xyz, idx, site, hv, pix;
+};
+
 struct dnni_ctx {
     int device = 0;
     int sm_count = 148;
@@ -60,6 +65,7 @@ struct dnni_ctx {
     Scratch scr;                     // single work packages (grow-only until dnni_clear)
     SegBufs seg;                     // segment driver buffers (grow-only until dnni_clear)
     Scratch seg_scr;
+    StBufs st;
     DevBuf in_xyz, in_gid, out_h, out_site;   // staging for the host-buffer entry point
     unsigned char* h_tables = nullptr;        // pinned staging of the tile tables
     size_t h_tables_cap = 0;

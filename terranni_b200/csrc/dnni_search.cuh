@@ -671,12 +671,13 @@ DNNI_HD int64_t point_bin(const BinGrid& g, int xr, int yr) {
 // so |Zrel| <= C * zabs.  Packed: word = (Zrel << K) + C with C < 2^K and
 // |Zrel| < 2^(62-K); otherwise separate int64 Z and int32 C.
 DNNI_HD void decide_packing(int max_r2, long long npix, long long zmin, long long zmax, int& packed, int& K,
-                            long long& zbase) {
+                            long long& zbase, int layers = 1) {
     long long cb = 0;
     if (max_r2 >= 0) {
         const long long r = isqrt_i32(max_r2);
         cb = (2 * r + 1) * (2 * r + 1);
         if (cb > npix) cb = npix;
+        cb *= layers;          // stacked rasters (space-time slices) add up per cell
     }
     K = 1;
     while (K < 62 && (1LL << K) <= cb) ++K;

@@ -148,6 +148,12 @@ class CompatSettings(ctypes.Structure):
                 ("multiplier", ctypes.c_int32), ("total_ncols", ctypes.c_int32), ("total_nrows", ctypes.c_int32)]
 
 
+class StOptions(ctypes.Structure):
+    """dnni_st_options: space-time interpolation settings."""
+    _fields_ = [("cur_time", ctypes.c_int32), ("time_radius", ctypes.c_int32), ("time_scale", ctypes.c_int32),
+                ("pad", ctypes.c_int32)]
+
+
 class CompatWP(ctypes.Structure):
     _fields_ = [("origin_x", ctypes.c_float), ("origin_y", ctypes.c_float), ("grid_origin_x", ctypes.c_float),
                 ("grid_origin_y", ctypes.c_float), ("nrows", ctypes.c_int32), ("ncols", ctypes.c_int32)]
@@ -206,6 +212,8 @@ _SIGS = {
                         ctypes.c_double, ctypes.c_float, ctypes.c_int32], ctypes.c_int),
     "dnni_write_grid_bin": ([ctypes.c_char_p, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                              ctypes.c_double, ctypes.c_float], ctypes.c_int),
+    "dnni_interpolate_spacetime": ([_P, ctypes.POINTER(WorkPackage), ctypes.POINTER(StOptions), _P, _P,
+                                    ctypes.c_int64, _P, _P], ctypes.c_int),
     "dnni_interpolate_compat": ([_P, ctypes.POINTER(CompatSettings), ctypes.POINTER(CompatWP), _P, ctypes.c_int64,
                                  _P, _P], ctypes.c_int),
     "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
@@ -312,6 +320,19 @@ class Engine:
         self._check(lib().dnni_interpolate_segment(self._h, ctypes.byref(wp), _ptr(xyz), _ptr(gid),
                                                    xyz.shape[0], _ptr(h), _ptr(sm), ctypes.byref(st)))
         return h, sm, st
+
+    def interpolate_spacetime(self, wp: WorkPackage, xyz, t, cur_time, time_radius, time_scale, out_h=None):
+        """dnni_interpolate_spacetime (timeRadius > 0) -> (h, stats)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1, 3)
+        t = np.ascontiguousarray(t, dtype=np.int32).reshape(-1)
+        if t.shape[0] != xyz.shape[0]:
+            raise ValueError("one time per point")
+        h = out_h if out_h is not None else np.empty((wp.nrows, wp.ncols), np.float32)
+        st = Stats()
+        opt = StOptions(int(cur_time), int(time_radius), int(time_scale), 0)
+        self._check(lib().dnni_interpolate_spacetime(self._h, ctypes.byref(wp), ctypes.byref(opt), _ptr(xyz), _ptr(t),
+                                                     xyz.shape[0], _ptr(h), ctypes.byref(st)))
+        return h, st
 
     def interpolate_device(self, wp: WorkPackage, d_xyz, n, d_h, d_gid=None, d_site=None, stream=None,
                            stats=True):

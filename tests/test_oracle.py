@@ -109,3 +109,60 @@ def test_gl_disagreement_is_a_fraction(oracle):
     d = oracle.gl_disagreement(oracle.make_wp(64, 64, 100), xyz)
     assert d["pixels"] == 64 * 64
     assert 0.0 <= d["site_frac"] <= 1.0 and d["z_differs"] <= d["site_differs"]
+
+
+def _st_case(rng, n, nc, nr, cs, cur, rt):
+    xyz = np.stack([rng.integers(-3 * cs, (nc + 3) * cs, n), rng.integers(-3 * cs, (nr + 3) * cs, n),
+                    rng.integers(-500, 500, n)], 1).astype(np.int32)
+    t = rng.integers(cur - 3 * rt - 1, cur + 3 * rt + 2, n).astype(np.int32)
+    return xyz, t
+
+
+def test_spacetime_kd_matches_brute(oracle):
+    # the per-time-value k-d form against every point for every (slice, pixel)
+    rng = np.random.default_rng(1)
+    for trial in range(40):
+        nc, nr = (int(v) for v in rng.integers(1, 20, 2))
+        cs = int(rng.choice([1, 7, 100]))
+        rt, tau, cur = int(rng.integers(0, 4)), int(rng.choice([1, 50, 100, 1000])), int(rng.integers(-3, 10))
+        xyz, t = _st_case(rng, int(rng.integers(0, 50)), nc, nr, cs, cur, rt)
+        if xyz.shape[0] > 3:
+            xyz[1, :2] = xyz[0, :2]
+            t[1] = t[0]
+        wp = oracle.make_wp(nc, nr, cs, raster=(-2, -1, nc + 3, nr + 2) if trial % 2 else None)
+        a = oracle.interpolate_spacetime(wp, xyz, t, cur, rt, tau)
+        b = oracle.interpolate_spacetime(wp, xyz, t, cur, rt, tau, brute=True)
+        assert np.array_equal(a["Z"], b["Z"]) and np.array_equal(a["C"], b["C"])
+        assert np.array_equal(a["h"].view(np.uint32), b["h"].view(np.uint32))
+
+
+def test_spacetime_radius_zero_is_the_2d_slice(oracle):
+    rng = np.random.default_rng(2)
+    xyz, t = _st_case(rng, 400, 30, 25, 100, 5, 2)
+    wp = oracle.make_wp(30, 25, 100, raster=(-3, -3, 33, 28))
+    a = oracle.interpolate_spacetime(wp, xyz, t, 5, 0, 100)
+    sel = t == 5
+    b = oracle.interpolate(wp, xyz[sel], np.nonzero(sel)[0].astype(np.uint32))
+    assert np.array_equal(a["Z"], b["Z"]) and np.array_equal(a["C"], b["C"])
+
+
+def test_spacetime_known_answers(oracle):
+    rng = np.random.default_rng(3)
+    wp = oracle.make_wp(24, 18, 100)
+    # a constant field stays constant whatever the times
+    xyz = np.stack([rng.integers(0, 2400, 300), rng.integers(0, 1800, 300), np.full(300, 4321)], 1)
+    t = rng.integers(0, 9, 300)
+    assert np.all(oracle.interpolate_spacetime(wp, xyz, t, 4, 2, 100)["h"] == np.float32(43.21))
+    # one site: every slice within reach sees it; the slice it is in covers every cell
+    r = oracle.interpolate_spacetime(wp, np.array([[1200, 900, 777]]), np.array([5]), 4, 2, 100)
+    assert np.all(r["h"] == np.float32(7.77)) and np.all(r["C"] >= 1)
+    # points farther than 2 rt from the current time take part in no slice
+    far = np.concatenate([xyz, [[1200, 900, 99999]]])
+    tf = np.concatenate([t, [4 + 5]])
+    assert np.array_equal(oracle.interpolate_spacetime(wp, far, tf, 4, 2, 100)["Z"],
+                          oracle.interpolate_spacetime(wp, xyz, t, 4, 2, 100)["Z"])
+    # a slice with no site leaves nothing; no points at all: nodata
+    e = oracle.interpolate_spacetime(wp, np.zeros((0, 3), np.int32), np.zeros(0, np.int32), 0, 1, 100)
+    assert np.all(e["h"] == np.float32(-9999.0)) and np.all(e["C"] == 0)
+    with pytest.raises(ValueError):
+        oracle.interpolate_spacetime(wp, xyz, t, 4, 17, 100)
