@@ -30,15 +30,23 @@
  * Settings::pointMin and Settings::multiplier, truncating divide.  Points are
  * then taken as world doubles, without the LAS quantisation.
  *
- * Not implemented: space-time interpolation (timeRadius > 0, nni.cpp:117-157,
- * 902-933) throws nni::Error with DNNI_E_INVAL.
+ * Space-time (timeRadius > 0, nni.cpp:902-933) runs dnni_interpolate_spacetime
+ * on the points the reference's slice loop reads (nni.cpp:722-790, with its
+ * renderbuffer reuse across calls in the Delta mode, nni.cpp:325-359, and its
+ * stream seeks); the stream must be sorted by time, as the reference's
+ * binning leaves it (terranni.cpp:120-126).  timeRadius and curTime must be
+ * whole numbers; one time step counts as one world unit of distance, as in
+ * drawPlane (nni.cpp:198), unless setTimeScale says otherwise.  Not with
+ * setCompatMode.
  */
 #ifndef DNNI_NNI_SHIM_H
 #define DNNI_NNI_SHIM_H
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -112,10 +120,18 @@ struct State {
     double xy_scale = 0.01, z_scale = 0.01;
     int device = 0;
     bool compat = false;
+    double time_scale = 1.0;                 // world units per time step
+    // space-time: slice times whose sites were read (the reference's rbTimes),
+    // the renderbuffer shape they belong to, and every point read for them,
+    // by stream position
+    std::vector<int> rb_times;
+    long long rb_key[3] = {-1, -1, -1};
+    std::map<long long, Point4D> st_points;
     double ms_points = 0, ms_engine = 0, ms_write = 0;
     long long calls = 0;
     std::vector<int32_t> xyz;
     std::vector<double> world;
+    std::vector<int32_t> times;
     std::vector<uint32_t> gid;
     std::vector<float> h;
 };
@@ -167,6 +183,10 @@ inline void setCoordinateScale(double xy_scale, double z_scale) {
 /* Reference-default semantics for the following performNNI calls
  * (extension; the reference's behaviour with its default build options). */
 inline void setCompatMode(bool on) { detail::state().compat = on; }
+
+/* World units of distance per time step in space-time interpolation
+ * (extension; the reference's planes count one step as one unit). */
+inline void setTimeScale(double world_units_per_step) { detail::state().time_scale = world_units_per_step; }
 
 /* Device used by the next init() (extension; the reference uses device 0,
  * cuda_nni.cu:659). */
@@ -223,6 +243,103 @@ inline void setupRun(const WorkPackage& wp, int pixel_offset = -1, int timeCount
     detail::check(dnni_setup_run(st.ctx, &d, 0), "setupRun");
 }
 
+namespace detail {
+inline void emit_outpoints(const WorkPackage& wp, tpie::ami::stream<OutPoint>& out) {
+    State& st = state();
+    for (int i = 0; i < wp.ncols; i++) {
+        for (int j = 0; j < wp.nrows; j++) {
+            OutPoint o((int)(i + wp.grid_origin_x), (int)(j + wp.grid_origin_y), st.h[(size_t)j * wp.ncols + i]);
+            if (o.i < st.s.ncols && o.j < st.s.nrows) out.write_item(o);
+        }
+    }
+}
+
+// nni.cpp:902-933 for timeRadius > 0: the slice loop's reads and seeks
+// (renderInputPoints, nni.cpp:722-790) and, in the Delta mode, the reuse of
+// slices already drawn (switchRenderbuffers, nni.cpp:325-359); the points
+// read feed dnni_interpolate_spacetime.
+inline void performNNISpaceTime(const WorkPackage& wp, tpie::ami::stream<OutPoint>& out,
+                                tpie::ami::stream<Point4D>& vec, float timeRadius, float curTime, bool useDelta) {
+    State& st = state();
+    if (st.compat) throw Error(DNNI_E_INVAL, "space-time interpolation has no reference-compatible mode");
+    if (timeRadius < 0 || timeRadius != std::floor(timeRadius) || curTime != std::floor(curTime))
+        throw Error(DNNI_E_INVAL, "timeRadius and curTime must be whole, timeRadius >= 0");
+    const int rt = (int)timeRadius, cur = (int)curTime;
+    const int numRB = useDelta ? 2 * rt + 1 : 1;
+    const int po = default_pixel_offset(st.s);
+    const long long key[3] = {(long long)wp.ncols + 2 * po, (long long)wp.nrows + 2 * po, numRB};
+    if (key[0] != st.rb_key[0] || key[1] != st.rb_key[1] || key[2] != st.rb_key[2]) {
+        st.rb_times.assign((size_t)numRB, -1);        // new renderbuffers (nni.cpp:381-410)
+        st.st_points.clear();
+        for (int k = 0; k < 3; ++k) st.rb_key[k] = key[k];
+    }
+    TPIE_OS_OFFSET finalSeekTo = vec.tell();
+    bool firstSeek = true;
+    Point4D* pp;
+    for (int j = -rt; j <= rt; j++) {
+        const float t = curTime + j;
+        bool found = false;
+        if (useDelta) {
+            for (int v : st.rb_times) found = found || v == (int)t;
+            if (!found) {
+                size_t mi = 0;
+                for (size_t k = 1; k < st.rb_times.size(); ++k)
+                    if (st.rb_times[k] < st.rb_times[mi]) mi = k;
+                st.rb_times[mi] = (int)t;
+            }
+        }
+        if (useDelta && found) continue;
+        TPIE_OS_OFFSET seekto = vec.tell();
+        bool foundSeek = false;
+        while (vec.read_item(&pp) == tpie::ami::NO_ERROR) {
+            const Point4D& p = *pp;
+            const TPIE_OS_OFFSET at = vec.tell() - 1;
+            if (!foundSeek && p.t >= t + 1 - timeRadius) {
+                seekto = at;
+                foundSeek = true;
+                if (firstSeek) {
+                    firstSeek = false;
+                    finalSeekTo = at;
+                }
+            }
+            if (std::fabs(t - p.t) <= timeRadius + 0.000001) st.st_points[(long long)at] = p;
+            else if (p.t > t + timeRadius) break;
+        }
+        if (!useDelta && j + 1 > timeRadius) vec.seek(finalSeekTo);
+        else vec.seek(seekto);
+    }
+    st.xyz.clear();
+    st.times.clear();
+    for (const auto& kv : st.st_points) {
+        const Point4D& p = kv.second;
+        if (std::abs((long long)p.t - cur) > 2LL * rt) continue;
+        const double X = std::llround((p.p[0] - wp.origin_x) / st.xy_scale);
+        const double Y = std::llround((p.p[1] - wp.origin_y) / st.xy_scale);
+        const double Z = std::llround(p.p[2] / st.z_scale);
+        if (std::fabs(X) >= 1073741824.0 || std::fabs(Y) >= 1073741824.0 || std::fabs(Z) >= 1073741824.0)
+            throw Error(DNNI_E_RANGE, "point beyond +-2^30 LAS units of the work-package origin");
+        st.xyz.push_back((int32_t)X);
+        st.xyz.push_back((int32_t)Y);
+        st.xyz.push_back((int32_t)Z);
+        st.times.push_back(p.t);
+    }
+    dnni_workpackage d = to_dnni(wp, -1);
+    dnni_st_options o{};
+    o.cur_time = cur;
+    o.time_radius = rt;
+    o.time_scale = (int32_t)std::llround(st.time_scale / st.xy_scale);
+    st.h.resize((size_t)wp.ncols * wp.nrows);
+    dnni_stats stats{};
+    const int64_t n = (int64_t)st.times.size();
+    check(dnni_interpolate_spacetime(st.ctx, &d, &o, n ? st.xyz.data() : nullptr, n ? st.times.data() : nullptr, n,
+                                     st.h.data(), &stats),
+          "performNNI");
+    st.ms_engine += stats.ms_total;
+    st.calls++;
+    emit_outpoints(wp, out);
+}
+}  // namespace detail
+
 /* nni.cpp:870-944.  Reads the points of time slice curTime from `vec` at its
  * current position (2-D: the reference's renderInputPoints loop,
  * nni.cpp:750-788, including where it leaves the stream), interpolates the
@@ -233,7 +350,10 @@ inline void performNNI(const WorkPackage& wp, tpie::ami::stream<OutPoint>& out, 
     (void)debug;
     detail::State& st = detail::state();
     if (!st.ctx) throw Error(DNNI_E_STATE, "performNNI before init");
-    if (timeRadius != 0.0f) throw Error(DNNI_E_INVAL, "space-time interpolation (timeRadius > 0) is not supported");
+    if (timeRadius != 0.0f) {
+        detail::performNNISpaceTime(wp, out, vec, timeRadius, curTime, useDelta);
+        return;
+    }
     const float t = curTime;
     TPIE_OS_OFFSET seekto = vec.tell(), finalSeekTo = vec.tell();
     bool foundSeek = false;
@@ -295,19 +415,19 @@ inline void performNNI(const WorkPackage& wp, tpie::ami::stream<OutPoint>& out, 
         st.ms_engine += stats.ms_total;
     }
     st.calls++;
-    for (int i = 0; i < wp.ncols; i++) {
-        for (int j = 0; j < wp.nrows; j++) {
-            OutPoint o((int)(i + wp.grid_origin_x), (int)(j + wp.grid_origin_y), st.h[(size_t)j * wp.ncols + i]);
-            if (o.i < st.s.ncols && o.j < st.s.nrows) out.write_item(o);
-        }
-    }
+    detail::emit_outpoints(wp, out);
 }
 
 /* nni.cpp:362-379 cleared the renderbuffers between work packages.  The
- * engine keeps no per-package state (each call starts from cleared scratch),
- * so nothing needs clearing; the scratch stays allocated for the next work
- * package and is released by cleanup(). */
-inline void clearRenderbuffers() {}
+ * engine keeps no per-package device state (each call starts from cleared
+ * scratch), so this only forgets the space-time slices read so far; the
+ * scratch stays allocated for the next work package and is released by
+ * cleanup(). */
+inline void clearRenderbuffers() {
+    detail::State& st = detail::state();
+    std::fill(st.rb_times.begin(), st.rb_times.end(), -1);
+    st.st_points.clear();
+}
 
 }  // namespace nni
 

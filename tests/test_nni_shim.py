@@ -20,19 +20,24 @@ POINT4D = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("t", "<i4"), ("pa
 OUTPOINT = np.dtype([("i", "<i4"), ("j", "<i4"), ("h", "<f4")])
 
 
-def build_demo():
-    deps = [SRC, os.path.join(ROOT, "include", "nni", "nni.h"), os.path.join(ROOT, "include", "tpie", "stream.h"),
+TSRC = os.path.join(ROOT, "tests", "native", "nni_shim_time_demo.cpp")
+TEXE = os.path.join(ROOT, "tests", "native", "nni_shim_time_demo")
+
+
+def build_demo(src=SRC, exe=EXE):
+    deps = [src, os.path.join(ROOT, "include", "nni", "nni.h"), os.path.join(ROOT, "include", "tpie", "stream.h"),
             os.path.join(ROOT, "include", "dnni.h"), os.path.join(LIBDIR, "libdnni.so")]
-    if not os.path.exists(EXE) or any(os.path.getmtime(d) > os.path.getmtime(EXE) for d in deps):
-        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), SRC, "-o", EXE,
+    if not os.path.exists(exe) or any(os.path.getmtime(d) > os.path.getmtime(exe) for d in deps):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), src, "-o", exe,
                "-L", LIBDIR, "-ldnni", f"-Wl,-rpath,{LIBDIR}"]
         subprocess.run(cmd, check=True, capture_output=True, text=True)
-    return EXE
+    return exe
 
 
 def test_reference_caller_compiles_and_links_against_the_shim():
     exe = build_demo()
     assert os.access(exe, os.X_OK)
+    assert os.access(build_demo(TSRC, TEXE), os.X_OK)
     assert POINT4D.itemsize == 32 and OUTPOINT.itemsize == 12     # nni.h:34-64 layouts
 
 
@@ -97,3 +102,35 @@ def test_reference_caller_compat_mode_matches_oracle(tmp_path, oracle):
     assert np.array_equal(got["i"], np.array([w[0] for w in want], np.int32))
     assert np.array_equal(got["h"].view(np.uint32), np.array([w[2] for w in want], np.float32).view(np.uint32))
     assert (ref != np.float32(-9999.0)).mean() > 0.9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rt,delta", [(1, 1), (1, 0), (2, 1), (2, 0)])
+def test_space_time_caller_matches_oracle(tmp_path, oracle, rt, delta):
+    """binRun's time loop (terranni.cpp:408-420) over one work package: every
+    curTime's OutPoints equal the oracle's space-time interpolation of the
+    whole time-sorted stream, and the stream is left where the reference's
+    seeks leave it (Delta: the first point of time cur + 1; Delta^2: of time
+    cur + 1 - 2 rt, nni.cpp:782-788)."""
+    from conftest import terrain_case
+    exe = build_demo(TSRC, TEXE)
+    side, cell_m, qr, t0, t1 = 60, 1.0, 3.0, 3, 7
+    xyz = terrain_case(23, side, 5000, lakes=1, lake_r=(5.0, 15.0))
+    times = np.sort(np.random.default_rng(4).integers(0, 11, xyz.shape[0])).astype(np.int32)
+    pts = np.zeros(xyz.shape[0], POINT4D)
+    pts["x"], pts["y"], pts["z"], pts["t"] = xyz[:, 0] * 0.01, xyz[:, 1] * 0.01, xyz[:, 2] * 0.01, times
+    pin = tmp_path / "pts.bin"
+    pts.tofile(pin)
+    r = subprocess.run([exe, str(pin), str(tmp_path / "out_"), str(side), str(side), str(cell_m), str(qr), str(rt),
+                        str(t0), str(t1), str(delta)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    pos = {int(a[1]): int(a[3]) for a in (ln.split() for ln in r.stdout.splitlines()) if a[0] == "t"}
+    po = int(np.ceil(qr / cell_m)) + 1
+    wp = oracle.make_wp(side, side, 100, raster=(-po, -po, side + po, side + po))
+    for cur in range(t0, t1 + 1):
+        got = np.fromfile(tmp_path / f"out_{cur}.bin", OUTPOINT)
+        ref = oracle.interpolate_spacetime(wp, xyz, times, cur, rt, 100)["h"]
+        want = np.array([ref[j, i] for i in range(side) for j in range(side)], np.float32)
+        assert np.array_equal(got["h"].view(np.uint32), want.view(np.uint32))
+        first = cur + 1 if delta else cur + 1 - 2 * rt
+        assert pos[cur] == int(np.searchsorted(times, first))
