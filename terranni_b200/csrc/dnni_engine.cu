@@ -155,9 +155,10 @@ void launch_prologue(const HostBatch& hb, const BatchTables& bt, const DevArrays
 // Launch sequence, part 2: binning, nearest sites, spans, stencil, finalize.
 // Needs no host synchronisation (a batch's whole sequence can be captured).
 // ev[0..2] (optional) mark the ends of binning, nearest sites and spans.
+// sites_only: stop after the nearest-site kernels (the site map is the result).
 void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a, const int32_t* d_xyz,
                  const uint32_t* d_gid, float* d_h, uint32_t* d_site, int sms, cudaStream_t st,
-                 const cudaEvent_t* ev, bool bbox_in_count = false) {
+                 const cudaEvent_t* ev, bool bbox_in_count = false, bool sites_only = false) {
     const int nchunk = hb.chunk_base.back();
     const int64_t nblk = hb.blk_base.back(), nsup = hb.sup_base.back();
     if (nchunk > 0) {
@@ -180,6 +181,7 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     if (nchunk > 0)
         k_near_far<<<sms * 6, 256, 0, st>>>(bt, a.sorted, a.start, a.bmask, a.smask, a.near, a.far, a.pix, d_site,
                                             a.sc, a.ctr);
+    if (sites_only) return;
     k_decide<<<(int)hb.tiles.size(), 32, 0, st>>>(bt, a.sc);
     if (ev) cudaEventRecord(ev[1], st);
     cudaMemsetAsync(a.D, 0, sizeof(unsigned long long) * hb.n_cells, st);
@@ -961,8 +963,9 @@ void dnni_free_all(dnni_ctx* c) {
     release_scratch(c, c->scr);
     release_scratch(c, c->seg_scr);
     c->seg.release(c);
-    DevBuf* bufs[] = {&c->in_xyz, &c->in_gid, &c->out_h, &c->out_site, &c->st.xyz, &c->st.idx, &c->st.site,
-                      &c->st.hv, &c->st.pix};
+    release_scratch(c, c->st.scr);
+    DevBuf* bufs[] = {&c->in_xyz, &c->in_gid, &c->out_h, &c->out_site, &c->st.xin, &c->st.tin, &c->st.xyz,
+                      &c->st.idx, &c->st.gs, &c->st.site, &c->st.pix};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
 

@@ -54,7 +54,8 @@ struct SegBufs {
 
 // Device buffers of the space-time driver (grow-only until dnni_clear).
 struct StBufs {
-    DevBuf xyz, idx, site, hv, pix;
+    DevBuf xin, tin, xyz, idx, gs, site, pix;
+    Scratch scr;                     // the per-time-value batch
 };
 
 struct dnni_ctx {

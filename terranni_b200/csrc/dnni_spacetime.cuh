@@ -9,10 +9,12 @@
 // numer/denom buffers over all slices (cuda_nni.cu:516-548 clears them once per
 // call).  Here, in the engine's exact form:
 //
-//   1. the points are grouped by time value v in [cur - 2rt, cur + 2rt]
-//      (stable, so each group keeps the input order);
-//   2. one batch of the 2-D engine, one tile per time value, gives every
-//      raster pixel its nearest site among that value's points (the site map);
+//   1. the points are grouped by time value v in [cur - 2rt, cur + 2rt] on
+//      the device, each keeping its input index as its gid (ties go to the
+//      lower index, the earlier point of the stream);
+//   2. one batch of the 2-D engine's nearest-site kernels, one tile per time
+//      value, gives every raster pixel its nearest site among that value's
+//      points (the site map; the batch stops there);
 //   3. k_st_lift: for slice s and pixel p the lifted-nearest site is the
 //      minimum over the 2rt + 1 values v within rt of ts of
 //      (2-D distance^2 to v's nearest site + ((ts - v) * tau)^2, input index,
@@ -29,16 +31,141 @@ namespace dnni {
 constexpr int kStMaxRadius = 16;
 constexpr int kStMaxValues = 4 * kStMaxRadius + 1;
 
+constexpr int kStChunk = 4096;          // points per block in the grouping passes
+
 struct StParams {
-    int32_t rt, tau;
+    int32_t rt, tau, nv, pad;
     int64_t npix;                        // raster pixels of one slice
+    int64_t t0;                          // time of value 0 (cur - 2 rt)
     int64_t off[kStMaxValues + 1];       // first grouped row of each time value
 };
 
+// Per time value: point count, box (absolute x0, y0, x1, y1, then z0, z1) and
+// the scatter cursors; err: a point beyond the coordinate range.
+struct StGroupStats {
+    int cnt[kStMaxValues];
+    int cursor[kStMaxValues];
+    int bb[kStMaxValues][6];
+    int err;
+};
+
+__global__ void k_st_init(StGroupStats* gs) {
+    for (int v = threadIdx.x; v < kStMaxValues; v += blockDim.x) {
+        gs->cnt[v] = 0;
+        gs->cursor[v] = 0;
+        gs->bb[v][0] = INT_MAX; gs->bb[v][1] = INT_MAX; gs->bb[v][2] = INT_MIN;
+        gs->bb[v][3] = INT_MIN; gs->bb[v][4] = INT_MAX; gs->bb[v][5] = INT_MIN;
+    }
+    if (threadIdx.x == 0) gs->err = 0;
+}
+
+// Time value of point i (-1: in no slice's reach or past the end).
+__device__ __forceinline__ int st_value(const int32_t* __restrict__ tt, int64_t i, int64_t n, int64_t t0, int nv) {
+    if (i >= n) return -1;
+    const int64_t dv = (int64_t)__ldg(&tt[i]) - t0;
+    return (dv >= 0 && dv < nv) ? (int)dv : -1;
+}
+
+// Grouping pass 1: counts and boxes per time value.  The lanes of a warp
+// that hold the same value reduce together; their leader updates the block's
+// shared copy, and each block folds its copy into the global one.
+__global__ void __launch_bounds__(256) k_st_count(const int32_t* __restrict__ xyz, const int32_t* __restrict__ tt,
+                                                  int64_t n, int64_t t0, int nv, int32_t ox, int32_t oy,
+                                                  StGroupStats* gs) {
+    __shared__ int cnt[kStMaxValues];
+    __shared__ int bb[kStMaxValues][6];
+    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+        cnt[v] = 0;
+        bb[v][0] = INT_MAX; bb[v][1] = INT_MAX; bb[v][2] = INT_MIN;
+        bb[v][3] = INT_MIN; bb[v][4] = INT_MAX; bb[v][5] = INT_MIN;
+    }
+    __syncthreads();
+    const int64_t c0 = (int64_t)blockIdx.x * kStChunk;
+    const int64_t c1 = c0 + kStChunk < n ? c0 + kStChunk : n;
+    const unsigned lane = threadIdx.x & 31;
+    unsigned bad = 0;
+    for (int64_t b = c0; b < c1; b += blockDim.x) {
+        const int64_t i = b + threadIdx.x;
+        const int v = st_value(tt, i, c1, t0, nv);
+        int x = 0, y = 0, z = 0;
+        if (v >= 0) {
+            x = __ldg(&xyz[3 * i]);
+            y = __ldg(&xyz[3 * i + 1]);
+            z = __ldg(&xyz[3 * i + 2]);
+            const int64_t rx = (int64_t)x - ox, ry = (int64_t)y - oy;
+            if (rx <= -kCoordLimit || rx >= kCoordLimit || ry <= -kCoordLimit || ry >= kCoordLimit) bad = 1;
+        }
+        const unsigned grp = __match_any_sync(0xffffffffu, v);
+        if (v >= 0) {
+            const int x0 = __reduce_min_sync(grp, x), x1 = __reduce_max_sync(grp, x);
+            const int y0 = __reduce_min_sync(grp, y), y1 = __reduce_max_sync(grp, y);
+            const int z0 = __reduce_min_sync(grp, z), z1 = __reduce_max_sync(grp, z);
+            if (lane == (unsigned)(__ffs(grp) - 1)) {
+                atomicAdd(&cnt[v], __popc(grp));
+                atomicMin(&bb[v][0], x0); atomicMin(&bb[v][1], y0); atomicMax(&bb[v][2], x1);
+                atomicMax(&bb[v][3], y1); atomicMin(&bb[v][4], z0); atomicMax(&bb[v][5], z1);
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&gs->err, 1);
+    __syncthreads();
+    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+        if (!cnt[v]) continue;
+        atomicAdd(&gs->cnt[v], cnt[v]);
+        atomicMin(&gs->bb[v][0], bb[v][0]); atomicMin(&gs->bb[v][1], bb[v][1]);
+        atomicMax(&gs->bb[v][2], bb[v][2]); atomicMax(&gs->bb[v][3], bb[v][3]);
+        atomicMin(&gs->bb[v][4], bb[v][4]); atomicMax(&gs->bb[v][5], bb[v][5]);
+    }
+}
+
+// Grouping pass 2: every point of a value to its group (rows off[v] ..),
+// with its input index as the gid that breaks ties.  A block counts its
+// points per value, reserves one range per value with a global cursor, then
+// places them (order inside a group is free: the gid carries the input order).
+__global__ void __launch_bounds__(256) k_st_scatter(const int32_t* __restrict__ xyz, const int32_t* __restrict__ tt,
+                                                    int64_t n, StParams P, StGroupStats* gs,
+                                                    int32_t* __restrict__ gxyz, uint32_t* __restrict__ gidx) {
+    __shared__ int cnt[kStMaxValues];
+    __shared__ int base[kStMaxValues];
+    for (int v = threadIdx.x; v < P.nv; v += blockDim.x) cnt[v] = 0;
+    __syncthreads();
+    const int64_t c0 = (int64_t)blockIdx.x * kStChunk;
+    const int64_t c1 = c0 + kStChunk < n ? c0 + kStChunk : n;
+    const unsigned lane = threadIdx.x & 31, below = (1u << lane) - 1u;
+    for (int64_t b = c0; b < c1; b += blockDim.x) {
+        const int v = st_value(tt, b + threadIdx.x, c1, P.t0, P.nv);
+        const unsigned grp = __match_any_sync(0xffffffffu, v);
+        if (v >= 0 && lane == (unsigned)(__ffs(grp) - 1)) atomicAdd(&cnt[v], __popc(grp));
+    }
+    __syncthreads();
+    for (int v = threadIdx.x; v < P.nv; v += blockDim.x) {
+        base[v] = cnt[v] ? atomicAdd(&gs->cursor[v], cnt[v]) : 0;
+        cnt[v] = 0;
+    }
+    __syncthreads();
+    for (int64_t b = c0; b < c1; b += blockDim.x) {
+        const int64_t i = b + threadIdx.x;
+        const int v = st_value(tt, i, c1, P.t0, P.nv);
+        const unsigned grp = __match_any_sync(0xffffffffu, v);
+        const int leader = __ffs(grp) - 1;
+        int first = 0;
+        if (v >= 0 && (int)lane == leader) first = atomicAdd(&cnt[v], __popc(grp));
+        first = __shfl_sync(0xffffffffu, first, leader);
+        if (v >= 0) {
+            const int64_t q = P.off[v] + base[v] + first + __popc(grp & below);
+            gxyz[3 * q] = __ldg(&xyz[3 * i]);
+            gxyz[3 * q + 1] = __ldg(&xyz[3 * i + 1]);
+            gxyz[3 * q + 2] = __ldg(&xyz[3 * i + 2]);
+            gidx[q] = (uint32_t)i;
+        }
+    }
+}
+
 // One thread per (slice, raster pixel); see step 3 above.
+// The site maps hold input indices (the batch's gids); xyz is the input.
 __global__ void __launch_bounds__(256) k_st_lift(TileParams T, StParams P, const uint32_t* __restrict__ site,
-                                                 const int32_t* __restrict__ gxyz, const int32_t* __restrict__ gidx,
-                                                 int2* __restrict__ pix, Scalars* __restrict__ sc) {
+                                                 const int32_t* __restrict__ xyz, int2* __restrict__ pix,
+                                                 Scalars* __restrict__ sc) {
     const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int R2 = -1;
     if (w < (2LL * P.rt + 1) * P.npix) {
@@ -51,16 +178,15 @@ __global__ void __launch_bounds__(256) k_st_lift(TileParams T, StParams P, const
         int bz = INT_MAX;
         for (int k = 0; k <= 2 * P.rt; ++k) {
             const int vi = s + k;                        // time value cur - 2rt + vi, ts - v = rt - k
-            const uint32_t loc = __ldg(&site[(int64_t)vi * P.npix + p]);
-            if (loc == 0xFFFFFFFFu) continue;
-            const int64_t q = P.off[vi] + loc;
-            const long long dx = (long long)rel_coord(__ldg(&gxyz[3 * q]), T.ox) - px;
-            const long long dy = (long long)rel_coord(__ldg(&gxyz[3 * q + 1]), T.oy) - py;
+            const uint32_t g = __ldg(&site[(int64_t)vi * P.npix + p]);
+            if (g == 0xFFFFFFFFu) continue;
+            const int64_t q = g;
+            const long long dx = (long long)rel_coord(__ldg(&xyz[3 * q]), T.ox) - px;
+            const long long dy = (long long)rel_coord(__ldg(&xyz[3 * q + 1]), T.oy) - py;
             const long long dt = (long long)(P.rt - k) * P.tau;
             const unsigned long long d2 =
                 (unsigned long long)(dx * dx) + (unsigned long long)(dy * dy) + (unsigned long long)(dt * dt);
-            const uint32_t g = (uint32_t)__ldg(&gidx[q]);
-            const int z = __ldg(&gxyz[3 * q + 2]);
+            const int z = __ldg(&xyz[3 * q + 2]);
             if (d2 < bd || (d2 == bd && (g < bg || (g == bg && z < bz)))) {
                 bd = d2;
                 bg = g;
@@ -193,54 +319,54 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
     const int64_t npix = (int64_t)T.rw * T.rh, cells = (int64_t)T.ncols * T.nrows;
     if (npix * V >= (int64_t)INT32_MAX) return set_err(c, DNNI_E_INVAL, "raster pixels x time values exceed 2^31");
 
-    // 1. group the points of the 4rt + 1 time values, input order kept
-    const int64_t t0 = (int64_t)o->cur_time - 2 * rt;
-    std::vector<int64_t> off(V + 1, 0);
-    for (int64_t k = 0; k < n; ++k) {
-        const int64_t dv = (int64_t)tt[k] - t0;
-        if (dv >= 0 && dv < V) off[dv + 1]++;
-    }
-    for (int v = 0; v < V; ++v) off[v + 1] += off[v];
-    const int64_t m = off[V];
-    if (m > (int64_t)INT32_MAX - 1) return set_err(c, DNNI_E_INVAL, "too many points in the time window");
-    std::vector<int32_t> gx(3 * (size_t)std::max<int64_t>(m, 1)), gi((size_t)std::max<int64_t>(m, 1));
-    std::vector<int64_t> pos(off.begin(), off.end() - 1);
-    std::vector<int32_t> bb((size_t)V * 4);
-    for (int v = 0; v < V; ++v) {
-        bb[4 * v] = INT32_MAX; bb[4 * v + 1] = INT32_MAX; bb[4 * v + 2] = INT32_MIN; bb[4 * v + 3] = INT32_MIN;
-    }
-    int zmin = INT_MAX, zmax = INT_MIN;
-    for (int64_t k = 0; k < n; ++k) {
-        const int64_t dv = (int64_t)tt[k] - t0;
-        if (dv < 0 || dv >= V) continue;
-        const int64_t q = pos[dv]++;
-        const int32_t x = xyz[3 * k], y = xyz[3 * k + 1], z = xyz[3 * k + 2];
-        const int64_t rx = (int64_t)x - wp->origin_x, ry = (int64_t)y - wp->origin_y;
-        if (rx <= -kCoordLimit || rx >= kCoordLimit || ry <= -kCoordLimit || ry >= kCoordLimit)
-            return set_err(c, DNNI_E_RANGE, "a point lies beyond +-2^30 LAS units of the work-package origin");
-        gx[3 * q] = x;
-        gx[3 * q + 1] = y;
-        gx[3 * q + 2] = z;
-        gi[q] = (int32_t)k;
-        int32_t* b = &bb[4 * dv];
-        b[0] = std::min(b[0], x); b[1] = std::min(b[1], y); b[2] = std::max(b[2], x); b[3] = std::max(b[3], y);
-        zmin = std::min(zmin, (int)z);
-        zmax = std::max(zmax, (int)z);
-    }
+    if (n > (int64_t)INT32_MAX - 1) return set_err(c, DNNI_E_INVAL, "more than 2^31 - 2 points");
     cudaStream_t st = c->stream;
-    if ((rs = dnni_ensure(c, c->st.xyz, sizeof(int32_t) * gx.size())) ||
-        (rs = dnni_ensure(c, c->st.idx, sizeof(int32_t) * gi.size())) ||
+    const int64_t t0 = (int64_t)o->cur_time - 2 * rt;
+    const int64_t nb = std::max<int64_t>(n, 1);
+    if ((rs = dnni_ensure(c, c->st.xin, sizeof(int32_t) * 3 * (size_t)nb)) ||
+        (rs = dnni_ensure(c, c->st.tin, sizeof(int32_t) * (size_t)nb)) ||
+        (rs = dnni_ensure(c, c->st.xyz, sizeof(int32_t) * 3 * (size_t)nb)) ||
+        (rs = dnni_ensure(c, c->st.idx, sizeof(uint32_t) * (size_t)nb)) ||
+        (rs = dnni_ensure(c, c->st.gs, sizeof(StGroupStats))) ||
         (rs = dnni_ensure(c, c->st.site, sizeof(uint32_t) * (size_t)(V * npix))) ||
-        (rs = dnni_ensure(c, c->st.hv, sizeof(float) * (size_t)(V * cells))) ||
         (rs = dnni_ensure(c, c->st.pix, sizeof(int2) * (size_t)(S * npix))) ||
         (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)))
         return rs;
     const bool timing = stats || (c->s.flags & DNNI_F_TIMING);
     if (timing) CK(cudaEventRecord(c->ev[0], st));
-    if (m > 0) {
-        CK(cudaMemcpyAsync(c->st.xyz.p, gx.data(), sizeof(int32_t) * 3 * (size_t)m, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(c->st.idx.p, gi.data(), sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, st));
+
+    // 1. upload, then group the points of the 4rt + 1 time values on the device
+    StGroupStats* gs = (StGroupStats*)c->st.gs.p;
+    k_st_init<<<1, 128, 0, st>>>(gs);
+    const int nchunk = (int)((n + kStChunk - 1) / kStChunk);
+    if (n > 0) {
+        CK(cudaMemcpyAsync(c->st.xin.p, xyz, sizeof(int32_t) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->st.tin.p, tt, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+        k_st_count<<<nchunk, 256, 0, st>>>((const int32_t*)c->st.xin.p, (const int32_t*)c->st.tin.p, n, t0, V,
+                                           wp->origin_x, wp->origin_y, gs);
     }
+    StGroupStats hg;
+    CK(cudaMemcpyAsync(&hg, gs, sizeof(StGroupStats), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hg.err) return set_err(c, DNNI_E_RANGE, "a point lies beyond +-2^30 LAS units of the work-package origin");
+    StParams P;
+    memset(&P, 0, sizeof(P));
+    P.rt = rt;
+    P.tau = tau;
+    P.nv = V;
+    P.npix = npix;
+    P.t0 = t0;
+    for (int v = 0; v < V; ++v) P.off[v + 1] = P.off[v] + hg.cnt[v];
+    const int64_t m = P.off[V];
+    int zmin = INT_MAX, zmax = INT_MIN;
+    for (int v = 0; v < V; ++v)
+        if (hg.cnt[v]) {
+            zmin = std::min(zmin, hg.bb[v][4]);
+            zmax = std::max(zmax, hg.bb[v][5]);
+        }
+    if (m > 0)
+        k_st_scatter<<<nchunk, 256, 0, st>>>((const int32_t*)c->st.xin.p, (const int32_t*)c->st.tin.p, n, P, gs,
+                                             (int32_t*)c->st.xyz.p, (uint32_t*)c->st.idx.p);
 
     // 2. nearest site per time value: one 2-D batch, one tile per value
     std::vector<dnni_tile> tiles((size_t)V);
@@ -248,25 +374,33 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
         dnni_tile& d = tiles[v];
         memset(&d, 0, sizeof(d));
         d.wp = *wp;
-        d.pt_offset = off[v];
-        d.pt_count = off[v + 1] - off[v];
+        d.pt_offset = P.off[v];
+        d.pt_count = P.off[v + 1] - P.off[v];
         d.out_offset = (int64_t)v * cells;
         d.site_offset = (int64_t)v * npix;
         if (d.pt_count > 0) {
-            d.ext_x0 = bb[4 * v];
-            d.ext_y0 = bb[4 * v + 1];
-            d.ext_x1 = bb[4 * v + 2];
-            d.ext_y1 = bb[4 * v + 3];
+            d.ext_x0 = hg.bb[v][0];
+            d.ext_y0 = hg.bb[v][1];
+            d.ext_x1 = hg.bb[v][2];
+            d.ext_y1 = hg.bb[v][3];
             if (!(d.ext_x0 || d.ext_y0 || d.ext_x1 || d.ext_y1)) d.ext_x1 = 1;   // all zero reads as "the raster"
         }
     }
-    dnni_batch_options bo{};
-    dnni_batch* b = nullptr;
-    if ((rs = dnni_batch_create(c, tiles.data(), V, &bo, &b))) return rs;
-    rs = dnni_batch_run_device(b, m > 0 ? (const int32_t*)c->st.xyz.p : nullptr, nullptr, (float*)c->st.hv.p,
-                               (uint32_t*)c->st.site.p, st, nullptr);
-    dnni_batch_destroy(b);
-    if (rs) return rs;
+    {
+        dnni_batch_options bo{};
+        HostBatch vb;
+        std::vector<int> order;
+        if ((rs = plan_batch(c, tiles.data(), V, bo, vb, order))) return rs;
+        DevArrays va;
+        if ((rs = ensure_scratch(c, c->st.scr, scratch_sizes(vb), va))) return rs;
+        const BatchTables vbt = device_tables(va.tables, V);
+        if ((rs = stage_tables(c, vb, va.tables, st))) return rs;
+        const int32_t* dx = m > 0 ? (const int32_t*)c->st.xyz.p : nullptr;
+        launch_prologue(vb, vbt, va, dx, st, false);
+        launch_body(vb, vbt, va, dx, (const uint32_t*)c->st.idx.p, nullptr, (uint32_t*)c->st.site.p, c->sm_count, st,
+                    nullptr, true, true);
+        CK(cudaGetLastError());
+    }
     if (timing) CK(cudaEventRecord(c->ev[1], st));
 
     // 3-4. lift the site maps into per-slice pixel records, scatter, finalize
@@ -280,17 +414,10 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
     BatchTables bt = device_tables(a.tables, 1);
     if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
     k_init_scalars<<<1, 32, 0, st>>>(bt, a.sc, a.ctr);
-    StParams P;
-    memset(&P, 0, sizeof(P));
-    P.rt = rt;
-    P.tau = tau;
-    P.npix = npix;
-    for (int v = 0; v <= V; ++v) P.off[v] = off[v];
     int2* pix = (int2*)c->st.pix.p;
     const int64_t lifts = (int64_t)S * npix;
     k_st_lift<<<(unsigned)((lifts + 255) / 256), 256, 0, st>>>(T, P, (const uint32_t*)c->st.site.p,
-                                                               (const int32_t*)c->st.xyz.p,
-                                                               (const int32_t*)c->st.idx.p, pix, a.sc);
+                                                               (const int32_t*)c->st.xin.p, pix, a.sc);
     k_st_decide<<<1, 32, 0, st>>>(a.sc, m > 0 ? zmin : 1, m > 0 ? zmax : 0, npix, S);
     if (timing) CK(cudaEventRecord(c->ev[2], st));
     CK(cudaMemsetAsync(a.D, 0, sizeof(unsigned long long) * (size_t)cells, st));
@@ -326,7 +453,7 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
         stats->n_cells = cells;
         stats->n_pixels = npix * S;
         fold_stats(c->h_sc, 1, stats);
-        stats->h2d_bytes = (int64_t)(16 * m);
+        stats->h2d_bytes = (int64_t)(16 * n);
         stats->d2h_bytes = (int64_t)(sizeof(float) * cells);
     }
     return DNNI_OK;
