@@ -52,7 +52,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["mixed", "tile4096", "segment", "served", "spacetime"], default="mixed")
+    ap.add_argument("--workload", choices=["mixed", "tile4096", "segment", "served", "spacetime", "compat"], default="mixed")
+    ap.add_argument("--cp-side", type=int, default=2000, help="compat: work-package side in cells (2 m)")
+    ap.add_argument("--cp-points", type=int, default=16_000_000, help="compat: points")
     ap.add_argument("--st-side", type=int, default=4096, help="spacetime: grid side in cells (1 m)")
     ap.add_argument("--st-points", type=int, default=36_000_000, help="spacetime: points over all time values")
     ap.add_argument("--st-radius", type=int, default=2, help="spacetime: time radius (slices 2r+1)")
@@ -797,6 +799,86 @@ def run_engine_spacetime(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------
+# compat: one work package in the reference's default semantics
+# ---------------------------------------------------------------------------
+
+def run_engine_compat(args, world, rank, local):
+    """terranni's defaults (scaling 5, 2 m cells, site radius 5 m, query
+    radius 4.99 m, pointMin 0, zMultiplier from the z range) on one side x side
+    work package, through dnni_interpolate_compat from pinned host buffers.
+    cpu_baseline: the oracle's compat restatement on one thread over a window
+    of the same cloud, checked bit-exact against the engine there."""
+    import numpy as np
+    import torch
+    from oracle import oracle
+    from terranni_b200 import engine, synth
+
+    torch.cuda.set_device(local)
+    side, n = args.cp_side, args.cp_points
+    cell, scale, sr, qr = 2.0, 5, 5.0, 5 * 2.0 / 2.0 - 0.01
+    t0 = time.perf_counter()
+    raw = synth.config3(seed=BASE_SEED + 9 + 1000 * rank, n=n, side=int(side * cell))["xyz"]
+    pts = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    pts[:] = raw * 0.01
+    h = torch.empty((side, side), dtype=torch.float32, pin_memory=True).numpy()
+    gen_s = time.perf_counter() - t0
+    mult = oracle.compat_multiplier(sr, scale, cell, float(pts[:, 2].max()), 0)
+    kw = dict(scale=scale, cell_size=cell, site_radius=sr, query_radius=qr, point_min=0, multiplier=mult)
+    se = engine.CompatSettings(total_ncols=side, total_nrows=side, **kw)
+    we = engine.CompatWP(nrows=side, ncols=side)
+    eng = engine.Engine(device=local)
+    for _ in range(args.warmup):
+        eng.interpolate_compat(se, we, pts)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        clk.mark("t_start")
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            h[:], _ = eng.interpolate_compat(se, we, pts)
+        dt = time.perf_counter() - t1
+        clk.mark("t_end")
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        win = 250
+        sel = (pts[:, 0] < (win + 8) * cell) & (pts[:, 1] < (win + 8) * cell)
+        so = oracle.CompatSettings(total_ncols=win, total_nrows=win, **kw)
+        wo = oracle.CompatWP(origin_x=0.0, origin_y=0.0, grid_origin_x=0.0, grid_origin_y=0.0, nrows=win, ncols=win)
+        tc = time.perf_counter()
+        ref, _ = oracle.compat(so, wo, pts[sel])
+        cpu_s = time.perf_counter() - tc
+        got, _ = eng.interpolate_compat(engine.CompatSettings(total_ncols=win, total_nrows=win, **kw),
+                                        engine.CompatWP(nrows=win, ncols=win), pts[sel])
+        cpu = {"value": win * win / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"oracle compat restatement, one {win}x{win} window of the same cloud "
+                         f"({int(sel.sum())} points), {cpu_s:.1f} s",
+               "bit_exact_vs_engine": bool(np.array_equal(got.view(np.uint32), ref.view(np.uint32)))}
+    if rank == 0:
+        peak, peak_kind = peaks()
+        cells = side * side
+        ms_step = 1000 * dt / args.steps
+        po = int(np.ceil((qr - 2 * cell / scale) / (cell / scale))) + 1
+        pix = (side * scale + 2 * po) ** 2
+        alg = 24 * n + 8 * pix + 4 * cells
+        print(json.dumps({
+            "metric": METRIC, "value": cells * 1000.0 / ms_step, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32/f64/int32", "data": "synthetic (seeded fBm terrain, clusters, lakes)",
+            "config": {"workload": f"compat{side}", "side": side, "cell_m": cell, "scale": scale, "points": n,
+                       "site_radius_m": sr, "query_radius_m": qr, "multiplier": mult, "raster_pixels": pix,
+                       "form": "dnni_interpolate_compat from pinned host buffers, timed host to host",
+                       "generate_s": round(gen_s, 1)},
+            "roofline": {"bound": "hbm", "kernel": "whole compat call, host to host", "achieved":
+                         alg / (ms_step / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms_step / 1000) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes": alg},
+            "e2e": {"value": cells * 1000.0 / ms_step, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+                    "d2h_bytes_per_step": 4 * cells, "note": "the call is host to host"},
+            "gpu_launches": 2 * args.steps, "cpu_baseline": cpu, "clocks": clk.summary(),
+        }), flush=True)
+    eng.close()
+
+
+# ---------------------------------------------------------------------------
 # served: DEM requests against a resident cloud
 # ---------------------------------------------------------------------------
 
@@ -919,6 +1001,15 @@ def main():
                               "note": "the CPU reference arm is measured on the mixed workload"}))
             return
         run_engine_served(args, world, rank, local)
+        return
+    if args.workload == "compat":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "metric": METRIC, "unit": UNIT, "workload": "compat",
+                              "note": "the CPU reference arm is measured on the mixed workload"}))
+            return
+        if world > 1:
+            raise SystemExit("the compat workload runs on one GPU")
+        run_engine_compat(args, world, rank, local)
         return
     if args.workload == "spacetime":
         if args.impl == "reference":
