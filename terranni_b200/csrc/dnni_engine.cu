@@ -650,12 +650,18 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
     return DNNI_OK;
 }
 
-// Cuts a batch into up to kSlices slices of consecutive point rows with
-// about equal work, plans each and uploads its tables; the slices share the
-// batch's scratch (they run one after another on the compute stream).
+// Cuts a batch into up to kSlices slices of consecutive point rows, with work
+// in the proportions of kSliceWeight, plans each and uploads its tables; the
+// slices share the batch's scratch (they run one after another on the
+// compute stream).
 static dnni_status plan_slices(dnni_batch* b) {
     dnni_ctx* c = b->ctx;
-    constexpr int kSlices = 8;
+    // slice sizes: a small first slice shortens the wait for the first upload,
+    // the next ones grow by 1.5x (each upload, at about two thirds of the
+    // compute rate, then ends before the compute of its predecessor), and a
+    // small last slice shortens the final download
+    constexpr int kSlices = 12;
+    constexpr double kSliceWeight[kSlices] = {0.1, 0.15, 0.225, 0.34, 0.5, 0.75, 1.0, 1.0, 1.0, 1.0, 0.5, 0.25};
     const int n = (int)b->tiles_in.size();
     const int S = (b->hb.n_rows >= (4 << 20) && n >= kSlices) ? kSlices : 1;
     b->sliced = S > 1;
@@ -674,13 +680,16 @@ static dnni_status plan_slices(dnni_batch* b) {
     };
     double total = 0;
     for (int k : idx) total += cost(k);
+    double wsum = 0;
+    for (int s = 0; s < S; ++s) wsum += kSliceWeight[s];
     dnni_batch_options o = b->opt;
     o.order_by_cost = 0;
-    double run = 0;
+    double run = 0, wrun = 0;
     size_t k0 = 0;
     for (int s = 0; s < S; ++s) {
         size_t k1 = k0;
-        const double goal = total * (s + 1) / S;
+        wrun += kSliceWeight[s];
+        const double goal = total * wrun / wsum;
         while (k1 < idx.size() && (s == S - 1 || run + cost(idx[k1]) <= goal || k1 == k0)) run += cost(idx[k1++]);
         if (k1 == k0) break;
         std::vector<dnni_tile> part;
