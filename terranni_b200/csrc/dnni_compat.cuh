@@ -60,28 +60,120 @@ __device__ __forceinline__ float compat_unorder(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
 }
 
-// Site pass: one thread per point (draw order k); every pixel of its square
-// keeps the smallest depth, the largest k among equal depths (the depth
-// test's later-draw-wins), as the 64-bit key order(d) << 32 | ~k.
-__global__ void __launch_bounds__(256) k_compat_sites(CompatGeom G, const double* __restrict__ xyz, int64_t n,
-                                                      unsigned long long* __restrict__ key) {
+// A point's square of site influence: its position relative to the work
+// package (float, as drawPlane has it) and the pixels [i0,i1] x [j0,j1]
+// whose centres the square covers (empty when i0 > i1 or j0 > j1).
+struct CompatSquare {
+    float sx, sy;
+    long long i0, i1, j0, j1;
+};
+
+__device__ __forceinline__ CompatSquare compat_square(const CompatGeom& G, const double* __restrict__ xyz, int64_t k) {
+    CompatSquare q;
+    q.sx = __double2float_rn(__dsub_rn(xyz[3 * k], (double)G.ox));
+    q.sy = __double2float_rn(__dsub_rn(xyz[3 * k + 1], (double)G.oy));
+    const float x0 = __double2float_rn(__dsub_rn((double)q.sx, G.rs)), x1 = __double2float_rn(__dadd_rn((double)q.sx, G.rs));
+    const float y0 = __double2float_rn(__dsub_rn((double)q.sy, G.rs)), y1 = __double2float_rn(__dadd_rn((double)q.sy, G.rs));
+    compat_span(x0, x1, G.left, G.pixel_size, G.xp, q.i0, q.i1);
+    compat_span(y0, y1, G.bottom, G.pixel_size, G.yp, q.j0, q.j1);
+    return q;
+}
+
+// The site pass runs per raster tile of kCpTile x kCpTile pixels whose keys
+// sit in shared memory: the points are first listed per tile they reach
+// (k_compat_count, k_compat_offsets, k_compat_fill), then one CTA per tile
+// takes the minimum key of its points per pixel and writes the tile out once.
+constexpr int kCpTile = 96;
+constexpr size_t kCpTileSmem = sizeof(unsigned long long) * kCpTile * kCpTile;
+
+__global__ void __launch_bounds__(256) k_compat_count(CompatGeom G, const double* __restrict__ xyz, int64_t n,
+                                                      int ntx, int* __restrict__ tcnt) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const float sx = __double2float_rn(__dsub_rn(xyz[3 * k], (double)G.ox));
-        const float sy = __double2float_rn(__dsub_rn(xyz[3 * k + 1], (double)G.oy));
-        const float x0 = __double2float_rn(__dsub_rn((double)sx, G.rs)), x1 = __double2float_rn(__dadd_rn((double)sx, G.rs));
-        const float y0 = __double2float_rn(__dsub_rn((double)sy, G.rs)), y1 = __double2float_rn(__dadd_rn((double)sy, G.rs));
-        long long i0, i1, j0, j1;
-        compat_span(x0, x1, G.left, G.pixel_size, G.xp, i0, i1);
-        compat_span(y0, y1, G.bottom, G.pixel_size, G.yp, j0, j1);
+        const CompatSquare q = compat_square(G, xyz, k);
+        if (q.i0 > q.i1 || q.j0 > q.j1) continue;
+        for (long long ty = q.j0 / kCpTile; ty <= q.j1 / kCpTile; ++ty)
+            for (long long tx = q.i0 / kCpTile; tx <= q.i1 / kCpTile; ++tx) atomicAdd(&tcnt[ty * ntx + tx], 1);
+    }
+}
+
+// One CTA of 1024 threads: exclusive prefix of the nt tile counts into
+// toff[0..nt] and zeroed fill cursors.
+__global__ void __launch_bounds__(1024) k_compat_offsets(const int* __restrict__ tcnt, int nt, long long* __restrict__ toff,
+                                                         int* __restrict__ tcur) {
+    __shared__ long long wsum[32];
+    const int per = (nt + 1023) / 1024;
+    const int b0 = threadIdx.x * per;
+    long long s = 0;
+    for (int k = 0; k < per; ++k) if (b0 + k < nt) s += tcnt[b0 + k];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long x = s;
+    for (int o = 1; o < 32; o <<= 1) { const long long y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) { const long long y = __shfl_up_sync(0xffffffffu, w, o); if (lane >= o) w += y; }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    long long run = x - s + (warp ? wsum[warp - 1] : 0);
+    for (int k = 0; k < per; ++k)
+        if (b0 + k < nt) { toff[b0 + k] = run; run += tcnt[b0 + k]; tcur[b0 + k] = 0; }
+    if (threadIdx.x == 1023) toff[nt] = run;
+}
+
+// (cap: the list's capacity, a bound on the squares' tile counts that the
+// host derives from the site radius; entries past it are dropped, never written)
+__global__ void __launch_bounds__(256) k_compat_fill(CompatGeom G, const double* __restrict__ xyz, int64_t n, int ntx,
+                                                     const long long* __restrict__ toff, int* __restrict__ tcur,
+                                                     uint32_t* __restrict__ list, int64_t cap) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const CompatSquare q = compat_square(G, xyz, k);
+        if (q.i0 > q.i1 || q.j0 > q.j1) continue;
+        for (long long ty = q.j0 / kCpTile; ty <= q.j1 / kCpTile; ++ty)
+            for (long long tx = q.i0 / kCpTile; tx <= q.i1 / kCpTile; ++tx) {
+                const long long t = ty * ntx + tx;
+                const long long e = toff[t] + atomicAdd(&tcur[t], 1);
+                if (e < cap) list[e] = (uint32_t)k;
+            }
+    }
+}
+
+// Site pass, one CTA per tile: every pixel keeps the smallest depth of the
+// points whose squares cover it, the largest draw order k among equal depths
+// (the depth test's later-draw-wins), as the 64-bit key order(d) << 32 | ~k;
+// ~0 where no square reaches.
+__global__ void __launch_bounds__(256) k_compat_sites(CompatGeom G, const double* __restrict__ xyz, int ntx,
+                                                      const long long* __restrict__ toff,
+                                                      const uint32_t* __restrict__ list, int64_t cap,
+                                                      unsigned long long* __restrict__ key) {
+    extern __shared__ unsigned long long sk[];
+    const int t = blockIdx.x;
+    const long long px0 = (long long)(t % ntx) * kCpTile, py0 = (long long)(t / ntx) * kCpTile;
+    const int pw = (int)min((long long)kCpTile, (long long)G.xp - px0);
+    const int ph = (int)min((long long)kCpTile, (long long)G.yp - py0);
+    for (int e = threadIdx.x; e < kCpTile * kCpTile; e += blockDim.x) sk[e] = ~0ull;
+    __syncthreads();
+    const long long e1 = toff[t + 1] < cap ? toff[t + 1] : (long long)cap;
+    for (long long e = toff[t] + threadIdx.x; e < e1; e += blockDim.x) {
+        const int64_t k = list[e];
+        const CompatSquare q = compat_square(G, xyz, k);
+        const long long i0 = max(q.i0, px0), i1 = min(q.i1, px0 + pw - 1);
+        const long long j0 = max(q.j0, py0), j1 = min(q.j1, py0 + ph - 1);
         const unsigned long long low = 0xFFFFFFFFull - (unsigned long long)k;
         for (long long pj = j0; pj <= j1; ++pj) {
             const float cy = compat_centre(pj, G.bottom, G.pixel_size);
             for (long long pi = i0; pi <= i1; ++pi) {
                 const float cx = compat_centre(pi, G.left, G.pixel_size);
-                const float d = compat_plane_depth(G.hw, sx, sy, cx, cy);
-                atomicMin(&key[pj * G.xp + pi], ((unsigned long long)compat_order(d) << 32) | low);
+                const float d = compat_plane_depth(G.hw, q.sx, q.sy, cx, cy);
+                atomicMin(&sk[(pj - py0) * kCpTile + (pi - px0)], ((unsigned long long)compat_order(d) << 32) | low);
             }
         }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kCpTile * kCpTile; e += blockDim.x) {
+        const int r = e / kCpTile, c = e - r * kCpTile;
+        if (r < ph && c < pw) key[(py0 + r) * G.xp + px0 + c] = sk[e];
     }
 }
 
@@ -165,21 +257,42 @@ extern "C" dnni_status dnni_interpolate_compat(dnni_ctx* c, const dnni_compat_se
     G.ox = wp->origin_x;
     G.oy = wp->origin_y;
     const int64_t cells = (int64_t)wp->ncols * wp->nrows;
+    const int ntx = (int)((xp + kCpTile - 1) / kCpTile), nty = (int)((yp + kCpTile - 1) / kCpTile);
+    const int nt = ntx * nty;
+    // tiles one square can reach: its pixel span is at most 2 rs / ps + 1
+    // (plus rounding) wide
+    const long long span = (long long)std::ceil(2.0 * G.rs / G.pixel_size) + 3;
+    const long long per = (span / kCpTile + 2) * (span / kCpTile + 2);
+    const int64_t list_n = std::max<int64_t>(n * per, 1);
     dnni_status rs;
-    // scratch: the pixel keys in the context's span-word buffer, points and
-    // outputs in its staging buffers
+    // scratch: the pixel keys in the context's span-word buffer, the tile
+    // counts, offsets and cursors in its bin-count buffer, the per-tile point
+    // lists in its rank buffer; points and outputs in its staging buffers
+    const size_t tbytes = sizeof(long long) * (size_t)(nt + 1) + 2 * sizeof(int) * (size_t)nt;
     if ((rs = dnni_ensure(c, c->scr.D, sizeof(unsigned long long) * (size_t)(xp * yp))) ||
+        (rs = dnni_ensure(c, c->scr.cnt, tbytes)) ||
+        (rs = dnni_ensure(c, c->scr.rank, sizeof(uint32_t) * (size_t)list_n)) ||
         (rs = dnni_ensure(c, c->in_xyz, sizeof(double) * 3 * (size_t)std::max<int64_t>(n, 1))) ||
         (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)) ||
         (res_out && (rs = dnni_ensure(c, c->out_site, sizeof(int32_t) * (size_t)cells))))
         return rs;
     cudaStream_t st = c->stream;
     unsigned long long* key = (unsigned long long*)c->scr.D.p;
-    CK(cudaMemsetAsync(key, 0xFF, sizeof(unsigned long long) * (size_t)(xp * yp), st));
+    long long* toff = (long long*)c->scr.cnt.p;
+    int* tcnt = (int*)(toff + nt + 1);
+    int* tcur = tcnt + nt;
+    CK(cudaMemsetAsync(tcnt, 0, sizeof(int) * (size_t)nt, st));
     if (n > 0) {
         CK(cudaMemcpyAsync(c->in_xyz.p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
-        k_compat_sites<<<c->sm_count * 8, 256, 0, st>>>(G, (const double*)c->in_xyz.p, n, key);
+        k_compat_count<<<c->sm_count * 8, 256, 0, st>>>(G, (const double*)c->in_xyz.p, n, ntx, tcnt);
     }
+    k_compat_offsets<<<1, 1024, 0, st>>>(tcnt, nt, toff, tcur);
+    if (n > 0)
+        k_compat_fill<<<c->sm_count * 8, 256, 0, st>>>(G, (const double*)c->in_xyz.p, n, ntx, toff, tcur,
+                                                       (uint32_t*)c->scr.rank.p, list_n);
+    CK(cudaFuncSetAttribute(k_compat_sites, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCpTileSmem));
+    k_compat_sites<<<nt, 256, kCpTileSmem, st>>>(G, (const double*)c->in_xyz.p, ntx, toff,
+                                                 (const uint32_t*)c->scr.rank.p, list_n, key);
     k_compat_cells<<<(int)((cells + 255) / 256), 256, 0, st>>>(G, (const double*)c->in_xyz.p, key, (float*)c->out_h.p,
                                                                res_out ? (int32_t*)c->out_site.p : nullptr);
     CK(cudaGetLastError());

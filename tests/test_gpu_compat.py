@@ -33,10 +33,16 @@ def _cases():
     # scaling 2, wide site squares, few points
     pts = np.stack([rng.uniform(0, 30, 120), rng.uniform(0, 30, 120), rng.uniform(100, 130, 120)], 1)
     out.append(dict(scale=2, cell=1.5, sr=8.0, qr=6.0, pmin=99, ncols=20, nrows=20, origin=(0.0, 0.0), pts=pts))
+    # UTM-scale world coordinates: the float32 work-package origin and the
+    # double points meet in the subtraction, as in the reference
+    pts = np.stack([rng.uniform(500100, 500180, 2500), rng.uniform(4100200, 4100260, 2500),
+                    rng.uniform(200, 230, 2500)], 1)
+    out.append(dict(scale=5, cell=2.0, sr=5.0, qr=4.99, pmin=150, ncols=40, nrows=30, origin=(500100.0, 4100200.0),
+                    pts=pts))
     return out
 
 
-@pytest.mark.parametrize("k", range(3))
+@pytest.mark.parametrize("k", range(4))
 def test_compat_matches_oracle(eng, oracle, k):
     from terranni_b200 import engine
     c = _cases()[k]

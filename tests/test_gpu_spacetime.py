@@ -86,3 +86,17 @@ def test_spacetime_constant_field_at_size(eng):
     t = rng.integers(96, 105, n).astype(np.int32)
     h, st = eng.interpolate_spacetime(engine.make_wp(2048, 2048, 100), xyz, t, 100, 2, 100)
     assert np.all(h == np.float32(12.34)) and st.nodata_cells == 0
+
+
+def test_spacetime_negative_times_and_origin(eng, oracle):
+    # times below zero, the current time negative, a work package away from
+    # the LAS origin with a raster halo
+    from terranni_b200 import engine
+    xyz, t = _terrain(31, 72, 3000, 100, -3, 1, 4)
+    xyz[:, 0] += 123400
+    xyz[:, 1] -= 56700
+    args = dict(origin_x=123400, origin_y=-56700, raster=(-3, -3, 75, 75))
+    ref = oracle.interpolate_spacetime(oracle.make_wp(72, 72, 100, **args), xyz, t, -3, 1, 100)
+    h, _ = eng.interpolate_spacetime(engine.make_wp(72, 72, 100, **args), xyz, t, -3, 1, 100)
+    assert np.array_equal(h.view(np.uint32), ref["h"].view(np.uint32))
+    assert (ref["h"] != np.float32(-9999.0)).mean() > 0.9
