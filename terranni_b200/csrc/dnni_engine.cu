@@ -733,8 +733,47 @@ static dnni_status plan_slices(dnni_batch* b) {
     }
     b->arr = full;
     const int ns = (int)b->slices.size();
+    // each slice works in its own part of the batch's scratch (the parts add
+    // up to the whole batch's sizes), so that consecutive slices can compute
+    // on two streams at once
+    if ((rs = dnni_ensure(c, b->slice_ctrs, sizeof(BatchCounters) * (size_t)ns))) return rs;
+    {
+        int64_t pts = 0, bins = 0, scan = 0, blk = 0, sup = 0, pix = 0, far = 0, cells = 0, tiles = 0;
+        for (int s = 0; s < ns; ++s) {
+            BatchSlice& sl = b->slices[s];
+            const HostBatch& h = sl.hb;
+            DevArrays v = full;
+            v.sorted += pts;
+            v.rank += pts;
+            v.cnt += bins;
+            v.start += bins;
+            v.bsum += scan;
+            v.bmask += blk;
+            v.smask += sup;
+            v.rownear += blk;
+            v.near += blk;
+            v.pix += pix;
+            v.far += far;
+            v.D += cells;
+            v.Dc += cells;
+            v.sc += tiles;
+            v.ctr = (BatchCounters*)b->slice_ctrs.p + s;
+            v.tables = (unsigned char*)sl.tables.p;
+            sl.arr = v;
+            pts += h.n_pts;
+            bins += h.n_bins;
+            scan += h.scan_base.back();
+            blk += h.blk_base.back();
+            sup += h.sup_base.back();
+            pix += h.n_pix;
+            far += h.n_far;
+            cells += h.n_cells;
+            tiles += (int64_t)h.tiles.size();
+        }
+    }
     if (cudaStreamCreateWithFlags(&b->s_in, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->s_cmp, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost((void**)&b->h_ctrs, sizeof(BatchCounters) * ns) != cudaSuccess) {
         cudaGetLastError();
         return set_err(c, DNNI_E_CUDA, "slice streams");
@@ -785,8 +824,10 @@ dnni_status dnni_batch_run(dnni_batch* b, const int32_t* xyz, const uint32_t* gi
         if (c->h_ctr->err & kErrRange)
             return set_err(c, DNNI_E_RANGE, "a point lies beyond its tile's declared extent or the coordinate range");
     } else {
-        // pipelined: slice s uploads on s_in while slice s-1 computes on the
-        // context stream and slice s-2 downloads on s_out
+        // pipelined: slice s uploads on s_in while the slices before it
+        // compute, alternately on the context stream and on s_cmp (each in its
+        // own part of the scratch, so one slice's kernels fill the SMs that
+        // the other's leave idle), and finished slices download on s_out
         if (stats) {
             memset(stats, 0, sizeof(*stats));
             CK(cudaEventRecord(c->ev[0], st));
@@ -802,15 +843,15 @@ dnni_status dnni_batch_run(dnni_batch* b, const int32_t* xyz, const uint32_t* gi
                 if (gid) CK(cudaMemcpyAsync(dg + r0, gid + r0, 4 * nr, cudaMemcpyHostToDevice, b->s_in));
             }
             CK(cudaEventRecord(b->ev_in[s], b->s_in));
-            CK(cudaStreamWaitEvent(st, b->ev_in[s], 0));
-            DevArrays a = b->arr;
-            a.tables = (unsigned char*)sl.tables.p;
-            launch_prologue(sl.hb, sl.bt, a, dx, st, false);
+            cudaStream_t cs = (s & 1) ? b->s_cmp : st;
+            CK(cudaStreamWaitEvent(cs, b->ev_in[s], 0));
+            const DevArrays& a = sl.arr;
+            launch_prologue(sl.hb, sl.bt, a, dx, cs, false);
             launch_body(sl.hb, sl.bt, a, dx, dg, (float*)b->out_h.p, out_site ? (uint32_t*)b->out_site.p : nullptr,
-                        c->sm_count, st, nullptr, true);
+                        c->sm_count, cs, nullptr, true);
             CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(&b->h_ctrs[s], a.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
-            CK(cudaEventRecord(b->ev_done[s], st));
+            CK(cudaMemcpyAsync(&b->h_ctrs[s], a.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, cs));
+            CK(cudaEventRecord(b->ev_done[s], cs));
             CK(cudaStreamWaitEvent(b->s_out, b->ev_done[s], 0));
             CK(cudaMemcpyAsync(out_h + sl.out0, (const float*)b->out_h.p + sl.out0, 4 * (size_t)(sl.out1 - sl.out0),
                                cudaMemcpyDeviceToHost, b->s_out));
@@ -821,6 +862,7 @@ dnni_status dnni_batch_run(dnni_batch* b, const int32_t* xyz, const uint32_t* gi
         if (stats) CK(cudaEventRecord(c->ev[1], b->s_out));
         CK(cudaStreamSynchronize(b->s_out));
         CK(cudaStreamSynchronize(st));
+        CK(cudaStreamSynchronize(b->s_cmp));
         for (size_t s = 0; s < b->slices.size(); ++s)
             if (b->h_ctrs[s].err & kErrRange)
                 return set_err(c, DNNI_E_RANGE,
@@ -857,6 +899,8 @@ dnni_status dnni_batch_destroy(dnni_batch* b) {
             if (e) cudaEventDestroy(e);
         if (b->s_in) cudaStreamDestroy(b->s_in);
         if (b->s_out) cudaStreamDestroy(b->s_out);
+        if (b->s_cmp) cudaStreamDestroy(b->s_cmp);
+        dnni_release(b->slice_ctrs, c);
         if (b->h_ctrs) cudaFreeHost(b->h_ctrs);
         release_scratch(c, b->scr);
         dnni_release(b->in_xyz, c);

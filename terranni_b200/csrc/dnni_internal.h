@@ -86,6 +86,7 @@ struct BatchSlice {
     dnni::HostBatch hb;
     DevBuf tables;
     dnni::BatchTables bt{};
+    DevArrays arr;                       // the slice's own part of the batch's scratch
     int64_t row0 = 0, row1 = 0, out0 = 0, out1 = 0, site0 = 0, site1 = 0;
 };
 
@@ -95,7 +96,8 @@ struct dnni_batch {
     dnni_batch_options opt{};
     std::vector<BatchSlice> slices;      // planned on the first host-buffer run
     bool sliced = false, slices_planned = false;
-    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaStream_t s_in = nullptr, s_out = nullptr, s_cmp = nullptr;   // s_cmp: the second compute stream
+    DevBuf slice_ctrs;                   // one BatchCounters per slice
     std::vector<cudaEvent_t> ev_in, ev_done;
     dnni::BatchCounters* h_ctrs = nullptr;
     dnni::HostBatch hb;
