@@ -34,22 +34,155 @@ __device__ __forceinline__ int seg_bucket(const SegGrid& g, int x, int y) {
 }
 
 __global__ void __launch_bounds__(256) k_seg_count(SegGrid g, const int32_t* __restrict__ xyz, int64_t n,
-                                                   unsigned* __restrict__ cnt, unsigned* __restrict__ rank) {
+                                                   unsigned* __restrict__ cnt) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        rank[i] = atomicAdd(&cnt[seg_bucket(g, xyz[3 * i], xyz[3 * i + 1])], 1u);
+        atomicAdd(&cnt[seg_bucket(g, xyz[3 * i], xyz[3 * i + 1])], 1u);
 }
 
-__global__ void __launch_bounds__(256) k_seg_scatter(SegGrid g, const int32_t* __restrict__ xyz, int64_t n,
-                                                     const long long* __restrict__ start,
-                                                     const unsigned* __restrict__ rank, int32_t* __restrict__ oxyz,
-                                                     uint32_t* __restrict__ ogid) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
-        const long long pos = start[seg_bucket(g, x, y)] + rank[i];
-        oxyz[3 * pos] = x;
-        oxyz[3 * pos + 1] = y;
-        oxyz[3 * pos + 2] = z;
-        ogid[pos] = (uint32_t)i;
+// Bucketing by partition in two passes, each staged in shared memory: a CTA
+// takes kSegPart points, counts them per key, places them in key order in
+// shared memory, reserves one range per key with a global cursor and writes
+// each key's points as one contiguous run (the input order is random in
+// space, so writing point by point would scatter every store).  Pass 1 keys
+// by group of rstep bucket rows into `part` ({x, y, z, input index}); pass 2,
+// over part, keys by bucket within the rows a CTA's points span (point by
+// point with global cursors when they span more than kSegKeys buckets).  The
+// order of points inside a bucket is free: the input index travels with
+// each point.
+constexpr int kSegPart = 2048;              // points per CTA
+constexpr int kSegPer = kSegPart / 256;     // per thread
+constexpr int kSegKeys = 2048;              // most keys one pass-2 CTA stages
+constexpr int kSegRowKeys = 4096;           // most row groups of pass 1
+
+__device__ __forceinline__ int seg_row(const SegGrid& g, int x, int y) { return seg_bucket(g, x, y) / g.nbx; }
+
+// Exclusive prefix of cnt[0..nk) into off[] by 256 threads (each sums a run
+// of consecutive keys); reserves each non-empty key's range from cur[key0 +
+// k] into base[k].
+__device__ __forceinline__ void seg_part_offsets(const int* cnt, int* off, unsigned long long* base, int nk,
+                                                 unsigned long long* __restrict__ cur, long long key0) {
+    __shared__ int wsum[8];
+    const int per = (nk + 255) / 256, k0 = threadIdx.x * per;
+    int s = 0;
+    for (int k = k0; k < k0 + per && k < nk; ++k) s += cnt[k];
+    int total;
+    int run = block_exclusive_sum(s, wsum, total, (int)threadIdx.x);
+    for (int k = k0; k < k0 + per && k < nk; ++k) {
+        off[k] = run;
+        run += cnt[k];
+        base[k] = cnt[k] ? atomicAdd(&cur[key0 + k], (unsigned long long)cnt[k]) : 0ull;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_seg_part_rows(SegGrid g, int rstep, int ngrp,
+                                                       const int32_t* __restrict__ xyz, int64_t n,
+                                                       unsigned long long* __restrict__ rowcur,
+                                                       int4* __restrict__ part) {
+    extern __shared__ int4 stage[];                        // kSegPart points, then the per-group tables
+    unsigned long long* base = (unsigned long long*)(stage + kSegPart);
+    int* cnt = (int*)(base + ngrp);
+    int* off = cnt + ngrp;
+    const int64_t c0 = (int64_t)blockIdx.x * kSegPart;
+    const int m = (int)(n - c0 < kSegPart ? n - c0 : kSegPart);
+    for (int r = threadIdx.x; r < ngrp; r += blockDim.x) cnt[r] = 0;
+    __syncthreads();
+    int4 p[kSegPer];
+    int key[kSegPer], lr[kSegPer];
+#pragma unroll
+    for (int k = 0; k < kSegPer; ++k) {
+        const int j = k * 256 + threadIdx.x;
+        if (j < m) {
+            const int64_t i = c0 + j;
+            p[k] = make_int4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], (int)i);
+            key[k] = seg_row(g, p[k].x, p[k].y) / rstep;
+            lr[k] = atomicAdd(&cnt[key[k]], 1);
+        }
+    }
+    __syncthreads();
+    seg_part_offsets(cnt, off, base, ngrp, rowcur, 0);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSegPer; ++k)
+        if (k * 256 + (int)threadIdx.x < m) stage[off[key[k]] + lr[k]] = p[k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+        const int4 q = stage[j];
+        const int r = seg_row(g, q.x, q.y) / rstep;
+        part[base[r] + (unsigned long long)(j - off[r])] = q;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_seg_part_buckets(SegGrid g, const int4* __restrict__ part, int64_t n,
+                                                          unsigned long long* __restrict__ bcur,
+                                                          int32_t* __restrict__ oxyz, uint32_t* __restrict__ ogid) {
+    extern __shared__ int4 stage[];                        // kSegPart points, then the per-bucket tables
+    unsigned long long* base = (unsigned long long*)(stage + kSegPart);
+    int* cnt = (int*)(base + kSegKeys);
+    int* off = cnt + kSegKeys;
+    const int64_t c0 = (int64_t)blockIdx.x * kSegPart;
+    const int m = (int)(n - c0 < kSegPart ? n - c0 : kSegPart);
+    // the rows r0 .. r1 that the CTA's points span
+    __shared__ int rmin, rmax;
+    if (threadIdx.x == 0) {
+        rmin = INT_MAX;
+        rmax = INT_MIN;
+    }
+    __syncthreads();
+    {
+        int lo = INT_MAX, hi = INT_MIN;
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            const int4 q = part[c0 + j];
+            const int r = seg_row(g, q.x, q.y);
+            lo = r < lo ? r : lo;
+            hi = r > hi ? r : hi;
+        }
+        atomicMin(&rmin, lo);
+        atomicMax(&rmax, hi);
+    }
+    __syncthreads();
+    const int r0 = rmin, r1 = rmax;
+    const long long key0 = (long long)r0 * g.nbx;
+    const long long nk = (long long)(r1 - r0 + 1) * g.nbx;
+    if (nk > kSegKeys) {
+        // sparse rows: too many buckets to stage, place point by point
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            const int4 q = part[c0 + j];
+            const unsigned long long pos = atomicAdd(&bcur[seg_bucket(g, q.x, q.y)], 1ull);
+            oxyz[3 * pos] = q.x;
+            oxyz[3 * pos + 1] = q.y;
+            oxyz[3 * pos + 2] = q.z;
+            ogid[pos] = (uint32_t)q.w;
+        }
+        return;
+    }
+    for (int k = threadIdx.x; k < (int)nk; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    int4 p[kSegPer];
+    int key[kSegPer], lr[kSegPer];
+#pragma unroll
+    for (int k = 0; k < kSegPer; ++k) {
+        const int j = k * 256 + threadIdx.x;
+        if (j < m) {
+            p[k] = part[c0 + j];
+            key[k] = (int)(seg_bucket(g, p[k].x, p[k].y) - key0);
+            lr[k] = atomicAdd(&cnt[key[k]], 1);
+        }
+    }
+    __syncthreads();
+    seg_part_offsets(cnt, off, base, (int)nk, bcur, key0);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSegPer; ++k)
+        if (k * 256 + (int)threadIdx.x < m) stage[off[key[k]] + lr[k]] = p[k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+        const int4 q = stage[j];
+        const int b = (int)(seg_bucket(g, q.x, q.y) - key0);
+        const unsigned long long pos = base[b] + (unsigned long long)(j - off[b]);
+        oxyz[3 * pos] = q.x;
+        oxyz[3 * pos + 1] = q.y;
+        oxyz[3 * pos + 2] = q.z;
+        ogid[pos] = (uint32_t)q.w;
     }
 }
 
@@ -170,7 +303,7 @@ long long floor_div_ll(long long a, long long b) { return a >= 0 ? a / b : -((-a
 // Uploads n points (chunks of 64 Mi) and buckets them on the device by G:
 // afterwards B.sxyz / B.sgid hold the points in bucket order (gid = input
 // index), start / bbox the bucket ranges and bounding boxes; B.xin and
-// B.rank are released again.
+// B.part are released again.
 dnni_status upload_points(dnni_ctx* c, cudaStream_t st, const int32_t* h_xyz, int64_t n, SegBufs& B) {
     dnni_status rs;
     if ((rs = dnni_ensure(c, B.xin, 12 * (size_t)std::max<int64_t>(n, 1)))) return rs;
@@ -185,7 +318,7 @@ dnni_status upload_points(dnni_ctx* c, cudaStream_t st, const int32_t* h_xyz, in
 }
 
 // Buckets the n points already uploaded to B.xin (see bucket_points);
-// keep_staging leaves B.xin and B.rank allocated for the next call.
+// keep_staging leaves B.xin and B.part allocated for the next call.
 dnni_status bucket_uploaded(dnni_ctx* c, cudaStream_t st, const SegGrid& G, int64_t n, SegBufs& B,
                             std::vector<long long>& start, std::vector<int4>& bbox, float* ms_up, float* ms_bk,
                             bool keep_staging = false) {
@@ -193,21 +326,38 @@ dnni_status bucket_uploaded(dnni_ctx* c, cudaStream_t st, const SegGrid& G, int6
     dnni_status rs;
     const size_t npts = (size_t)std::max<int64_t>(n, 1);
     if ((rs = dnni_ensure(c, B.sxyz, 12 * npts)) || (rs = dnni_ensure(c, B.sgid, 4 * npts)) ||
-        (rs = dnni_ensure(c, B.rank, 4 * npts)) || (rs = dnni_ensure(c, B.cnt, 4 * (size_t)nb)) ||
-        (rs = dnni_ensure(c, B.start, 8 * (size_t)(nb + 1))) || (rs = dnni_ensure(c, B.bbox, 16 * (size_t)nb)))
+        (rs = dnni_ensure(c, B.part, 16 * npts)) || (rs = dnni_ensure(c, B.cnt, 4 * (size_t)nb)) ||
+        (rs = dnni_ensure(c, B.cur, 8 * (size_t)nb)) || (rs = dnni_ensure(c, B.start, 8 * (size_t)(nb + 1))) ||
+        (rs = dnni_ensure(c, B.bbox, 16 * (size_t)nb)))
         return rs;
     CK(cudaMemsetAsync(B.cnt.p, 0, 4 * (size_t)nb, st));
     const int grid = c->sm_count * 8;
-    if (n > 0) k_seg_count<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (unsigned*)B.cnt.p, (unsigned*)B.rank.p);
+    if (n > 0) k_seg_count<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (unsigned*)B.cnt.p);
     std::vector<unsigned> cnt(nb);
     start.assign(nb + 1, 0);
     CK(cudaMemcpyAsync(cnt.data(), B.cnt.p, 4 * (size_t)nb, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     for (int b = 0; b < nb; ++b) start[b + 1] = start[b] + cnt[b];
     CK(cudaMemcpyAsync(B.start.p, start.data(), 8 * (size_t)(nb + 1), cudaMemcpyHostToDevice, st));
-    if (n > 0)
-        k_seg_scatter<<<grid, 256, 0, st>>>(G, (const int32_t*)B.xin.p, n, (const long long*)B.start.p,
-                                            (const unsigned*)B.rank.p, (int32_t*)B.sxyz.p, (uint32_t*)B.sgid.p);
+    if (n > 0) {
+        // pass 1 by bucket row (cursors: the rows' first positions), pass 2
+        // by bucket (cursors: the buckets' first positions)
+        const int rstep = (G.nby + kSegRowKeys - 1) / kSegRowKeys;
+        const int ngrp = (G.nby + rstep - 1) / rstep;
+        std::vector<long long> rowcur(ngrp);
+        for (int r = 0; r < ngrp; ++r) rowcur[r] = start[(size_t)r * rstep * G.nbx];
+        CK(cudaMemcpyAsync(B.cur.p, rowcur.data(), 8 * (size_t)ngrp, cudaMemcpyHostToDevice, st));
+        const int nblk = (int)((n + kSegPart - 1) / kSegPart);
+        const size_t sm1 = sizeof(int4) * kSegPart + 16 * (size_t)ngrp;
+        const size_t sm2 = sizeof(int4) * kSegPart + 16 * (size_t)kSegKeys;
+        CK(cudaFuncSetAttribute(k_seg_part_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+        CK(cudaFuncSetAttribute(k_seg_part_buckets, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        k_seg_part_rows<<<nblk, 256, sm1, st>>>(G, rstep, ngrp, (const int32_t*)B.xin.p, n,
+                                                (unsigned long long*)B.cur.p, (int4*)B.part.p);
+        CK(cudaMemcpyAsync(B.cur.p, B.start.p, 8 * (size_t)nb, cudaMemcpyDeviceToDevice, st));
+        k_seg_part_buckets<<<nblk, 256, sm2, st>>>(G, (const int4*)B.part.p, n, (unsigned long long*)B.cur.p,
+                                                   (int32_t*)B.sxyz.p, (uint32_t*)B.sgid.p);
+    }
     k_seg_bbox<<<nb, 256, 0, st>>>((const int32_t*)B.sxyz.p, (const long long*)B.start.p, (int4*)B.bbox.p);
     bbox.resize(nb);
     CK(cudaMemcpyAsync(bbox.data(), B.bbox.p, 16 * (size_t)nb, cudaMemcpyDeviceToHost, st));
@@ -218,7 +368,7 @@ dnni_status bucket_uploaded(dnni_ctx* c, cudaStream_t st, const SegGrid& G, int6
     cudaEventElapsedTime(ms_bk, c->ev[1], c->ev[2]);
     if (!keep_staging) {
         dnni_release(B.xin, c);
-        dnni_release(B.rank, c);
+        dnni_release(B.part, c);
     }
     return DNNI_OK;
 }
