@@ -1008,8 +1008,8 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
 }  // extern "C"
 
 void SegBufs::release(dnni_ctx* c) {
-    DevBuf* all[] = {&xin, &sxyz, &sgid, &part, &cur, &cnt, &start, &bbox, &gxyz, &ggid, &gout, &gsite, &chunks,
-                     &ring};
+    DevBuf* all[] = {&xin, &sxyz, &sgid, &part, &cur, &cnt, &start, &bbox, &occ, &gxyz, &ggid, &gout[0], &gout[1],
+                     &gsite[0], &gsite[1], &chunks, &ring};
     for (DevBuf* b : all) dnni_release(*b, c);
 }
 

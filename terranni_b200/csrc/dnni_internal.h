@@ -48,7 +48,7 @@ struct dnni_ctx;
 
 // Device buffers of the segment driver and the server's resident cloud.
 struct SegBufs {
-    DevBuf xin, sxyz, sgid, part, cur, cnt, start, bbox, gxyz, ggid, gout, gsite, chunks, ring;
+    DevBuf xin, sxyz, sgid, part, cur, cnt, start, bbox, occ, gxyz, ggid, gout[2], gsite[2], chunks, ring;
     void release(dnni_ctx* c);
 };
 

@@ -384,8 +384,8 @@ dnni_status bucket_points(dnni_ctx* c, cudaStream_t st, const SegGrid& G, const 
 // Squared distance, in fine blocks (fw LAS units square, nfx x nfy from the
 // grid origin), from every fine block to the nearest one holding a point.
 dnni_status occupancy_edt(dnni_ctx* c, cudaStream_t st, const SegGrid& G, long long fw, int nfx, int nfy,
-                          const SegBufs& B, int64_t n, std::vector<double>& edt2) {
-    DevBuf occ_d;
+                          SegBufs& B, int64_t n, std::vector<double>& edt2) {
+    DevBuf& occ_d = B.occ;                   // kept between calls: no allocation, no implicit synchronisation
     dnni_status rs;
     if ((rs = dnni_ensure(c, occ_d, (size_t)nfx * nfy))) return rs;
     std::vector<unsigned char> occ((size_t)nfx * nfy);
@@ -395,7 +395,6 @@ dnni_status occupancy_edt(dnni_ctx* c, cudaStream_t st, const SegGrid& G, long l
                                                    (unsigned char*)occ_d.p);
     if (e == cudaSuccess) e = cudaMemcpyAsync(occ.data(), occ_d.p, occ.size(), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    dnni_release(occ_d, c);
     if (e != cudaSuccess) return cuda_err(c, e, "occupancy");
     edt2 = edt_2d(occ.data(), nfx, nfy);
     return DNNI_OK;
@@ -486,6 +485,23 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     std::vector<int> ring;
     HostBatch hb;
     DevArrays a;
+    // a batch's accepted tiles download on so while the next batch computes
+    // into the other of two output buffers (done[b]: buffer b's downloads)
+    cudaStream_t so = nullptr;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    struct Release {
+        cudaStream_t& so;
+        cudaEvent_t* done;
+        ~Release() {
+            if (so) { cudaStreamSynchronize(so); cudaStreamDestroy(so); }
+            for (int b = 0; b < 2; ++b) if (done[b]) cudaEventDestroy(done[b]);
+        }
+    } release_on_exit{so, done};
+    if (cudaStreamCreateWithFlags(&so, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming) != cudaSuccess)
+        return cuda_err(c, cudaGetLastError(), "segment download stream");
+    int ob = 0;
     while (qi < queue.size()) {
         const size_t q1 = std::min(queue.size(), qi + (size_t)s.tiles_per_batch);
         const int ng = (int)(q1 - qi);
@@ -554,11 +570,16 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
             site += (int64_t)(ax1 - ax0) * (ay1 - ay0);
         }
         const size_t gp = (size_t)std::max<int64_t>(pt, 1);
+        // this buffer's downloads from two batches ago must be over before
+        // it is written (or reallocated) again
+        CK(cudaEventSynchronize(done[ob]));
         if ((rs = dnni_ensure(c, B.gxyz, 12 * gp)) || (rs = dnni_ensure(c, B.ggid, 4 * gp)) ||
-            (rs = dnni_ensure(c, B.gout, 4 * (size_t)std::max<int64_t>(out, 1))) ||
-            (h_site && (rs = dnni_ensure(c, B.gsite, 4 * (size_t)std::max<int64_t>(site, 1)))) ||
+            (rs = dnni_ensure(c, B.gout[ob], 4 * (size_t)std::max<int64_t>(out, 1))) ||
+            (h_site && (rs = dnni_ensure(c, B.gsite[ob], 4 * (size_t)std::max<int64_t>(site, 1)))) ||
             (rs = dnni_ensure(c, B.chunks, sizeof(SegChunk) * std::max<size_t>(chunks.size(), 1))))
             return rs;
+        float* gout = (float*)B.gout[ob].p;
+        uint32_t* gsite = h_site ? (uint32_t*)B.gsite[ob].p : nullptr;
         if (!chunks.empty()) {
             CK(cudaMemcpyAsync(B.chunks.p, chunks.data(), sizeof(SegChunk) * chunks.size(), cudaMemcpyHostToDevice, st));
             k_seg_gather<<<(int)chunks.size(), 256, 0, st>>>((const SegChunk*)B.chunks.p, (const int32_t*)B.sxyz.p,
@@ -570,8 +591,8 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         const BatchTables bt = device_tables(a.tables, ng);
         if ((rs = stage_tables(c, hb, a.tables, st))) return rs;
         launch_prologue(hb, bt, a, (const int32_t*)B.gxyz.p, st, false);
-        launch_body(hb, bt, a, (const int32_t*)B.gxyz.p, (const uint32_t*)B.ggid.p, (float*)B.gout.p,
-                    h_site ? (uint32_t*)B.gsite.p : nullptr, c->sm_count, st, nullptr, true);
+        launch_body(hb, bt, a, (const int32_t*)B.gxyz.p, (const uint32_t*)B.ggid.p, gout, gsite, c->sm_count, st,
+                    nullptr, true);
         CK(cudaGetLastError());
         hsc.resize(ng);
         ring.resize(4 * (size_t)ng);
@@ -622,20 +643,21 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
             for (int sd = 0; sd < 4; ++sd) max_halo = std::max(max_halo, T.h[sd]);
             const dnni_tile& t = tl[k];
             const size_t w = (size_t)t.wp.ncols, h = (size_t)t.wp.nrows;
-            CK(cudaMemcpy2DAsync(h_out + (size_t)T.y0 * s.ncols + T.x0, 4 * (size_t)s.ncols,
-                                 (const float*)B.gout.p + t.out_offset, 4 * w, 4 * w, h, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpy2DAsync(h_out + (size_t)T.y0 * s.ncols + T.x0, 4 * (size_t)s.ncols, gout + t.out_offset,
+                                 4 * w, 4 * w, h, cudaMemcpyDeviceToHost, so));
             d2h += (int64_t)(4 * w * h);
             if (h_site) {
-                const uint32_t* src = (const uint32_t*)B.gsite.p + t.site_offset +
-                                      (size_t)(T.y0 - ry0[k]) * rw[k] + (T.x0 - rx0[k]);
+                const uint32_t* src = gsite + t.site_offset + (size_t)(T.y0 - ry0[k]) * rw[k] + (T.x0 - rx0[k]);
                 CK(cudaMemcpy2DAsync(h_site + (size_t)T.y0 * s.ncols + T.x0, 4 * (size_t)s.ncols, src,
-                                     4 * (size_t)rw[k], 4 * w, h, cudaMemcpyDeviceToHost, st));
+                                     4 * (size_t)rw[k], 4 * w, h, cudaMemcpyDeviceToHost, so));
                 d2h += (int64_t)(4 * w * h);
             }
         }
-        CK(cudaStreamSynchronize(st));
+        CK(cudaEventRecord(done[ob], so));
+        ob ^= 1;
         qi = q1;
     }
+    CK(cudaStreamSynchronize(so));
     if (stats) {
         stats->ms_total = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         stats->ms_upload = ms_up;
