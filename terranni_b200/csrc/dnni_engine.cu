@@ -660,8 +660,9 @@ static dnni_status plan_slices(dnni_batch* b) {
     // the next ones grow by 1.5x (each upload, at about two thirds of the
     // compute rate, then ends before the compute of its predecessor), and a
     // small last slice shortens the final download
-    constexpr int kSlices = 12;
-    constexpr double kSliceWeight[kSlices] = {0.1, 0.15, 0.225, 0.34, 0.5, 0.75, 1.0, 1.0, 1.0, 1.0, 0.5, 0.25};
+    constexpr int kSlices = 16;
+    constexpr double kSliceWeight[kSlices] = {0.05, 0.075, 0.11, 0.17, 0.25, 0.38, 0.57, 0.85,
+                                              1.0, 1.0, 1.0, 1.0, 1.0, 0.5, 0.25, 0.12};
     const int n = (int)b->tiles_in.size();
     const int S = (b->hb.n_rows >= (4 << 20) && n >= kSlices) ? kSlices : 1;
     b->sliced = S > 1;
