@@ -717,13 +717,11 @@ static dnni_status plan_slices(dnni_batch* b) {
         if ((rs = dnni_ensure(c, sl.tables, TableLayout((int)part.size()).total))) return rs;
         sl.bt = device_tables((const unsigned char*)sl.tables.p, (int)part.size());
         if ((rs = stage_tables(c, sl.hb, (unsigned char*)sl.tables.p, c->stream))) return rs;
-        DevArrays tmp;
-        if ((rs = ensure_scratch(c, b->scr, scratch_sizes(sl.hb), tmp))) return rs;
         b->slices.push_back(std::move(sl));
         k0 = k1;
     }
-    // the shared scratch may have moved while it grew: the full batch's view
-    // and its captured graph are rebuilt
+    // the full batch's view of its scratch (the graph captured for it is
+    // rebuilt if the arrays moved)
     DevArrays full;
     dnni_status rs = ensure_scratch(c, b->scr, scratch_sizes(b->hb), full);
     if (rs) return rs;
