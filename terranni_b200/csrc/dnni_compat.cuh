@@ -28,14 +28,26 @@ struct CompatGeom {
     float ox, oy;
 };
 
-__device__ __forceinline__ float compat_plane_depth(float hw, float sx, float sy, float px, float py) {
+// A site's (or query's) lifted plane: its slopes and offset depend on the
+// point only, so they are formed once per point (drawPlane, nni.cpp:186-212).
+struct CompatPlane {
+    float a, b, zoff;
+};
+
+__device__ __forceinline__ CompatPlane compat_plane(float hw, float sx, float sy) {
     const float zpx = __fdiv_rn(__fadd_rn(sx, hw), hw);
     const float zpy = __fdiv_rn(__fadd_rn(sy, hw), hw);
-    const float zoff = __fadd_rn(__fmul_rn(zpx, zpx), __fmul_rn(zpy, zpy));
-    const float a = __fdiv_rn(__fmul_rn(-2.0f, zpx), hw);
-    const float b = __fdiv_rn(__fmul_rn(-2.0f, zpy), hw);
+    CompatPlane P;
+    P.zoff = __fadd_rn(__fmul_rn(zpx, zpx), __fmul_rn(zpy, zpy));
+    P.a = __fdiv_rn(__fmul_rn(-2.0f, zpx), hw);
+    P.b = __fdiv_rn(__fmul_rn(-2.0f, zpy), hw);
+    return P;
+}
+
+// The plane's depth at a pixel centre (px, py).
+__device__ __forceinline__ float compat_depth(const CompatPlane& P, float hw, float px, float py) {
     const float zx = __fadd_rn(px, hw), zy = __fadd_rn(py, hw);
-    return __fadd_rn(__fadd_rn(__fmul_rn(a, zx), __fmul_rn(b, zy)), zoff);
+    return __fadd_rn(__fadd_rn(__fmul_rn(P.a, zx), __fmul_rn(P.b, zy)), P.zoff);
 }
 
 // Pixel index range [i0, i1] whose centres fall in [x0, x1) (one axis).
@@ -161,11 +173,12 @@ __global__ void __launch_bounds__(256) k_compat_sites(CompatGeom G, const double
         const long long i0 = max(q.i0, px0), i1 = min(q.i1, px0 + pw - 1);
         const long long j0 = max(q.j0, py0), j1 = min(q.j1, py0 + ph - 1);
         const unsigned long long low = 0xFFFFFFFFull - (unsigned long long)k;
+        const CompatPlane P = compat_plane(G.hw, q.sx, q.sy);
         for (long long pj = j0; pj <= j1; ++pj) {
             const float cy = compat_centre(pj, G.bottom, G.pixel_size);
             for (long long pi = i0; pi <= i1; ++pi) {
                 const float cx = compat_centre(pi, G.left, G.pixel_size);
-                const float d = compat_plane_depth(G.hw, q.sx, q.sy, cx, cy);
+                const float d = compat_depth(P, G.hw, cx, cy);
                 atomicMin(&sk[(pj - py0) * kCpTile + (pi - px0)], ((unsigned long long)compat_order(d) << 32) | low);
             }
         }
@@ -200,6 +213,7 @@ __global__ void __launch_bounds__(256) k_compat_cells(CompatGeom G, const double
     compat_span(y0, y1, G.bottom, G.pixel_size, G.yp, j0, j1);
     uint32_t numer = 0;
     int32_t denom = 0;
+    const CompatPlane Q = compat_plane(G.hw, qx, qy);
     for (long long pj = j0; pj <= j1; ++pj) {
         const float cy = compat_centre(pj, G.bottom, G.pixel_size);
         for (long long pi = i0; pi <= i1; ++pi) {
@@ -209,7 +223,7 @@ __global__ void __launch_bounds__(256) k_compat_cells(CompatGeom G, const double
             const uint32_t zc = compat_zcode(xyz[3 * k + 2], G.z_offset, G.z_mult);
             if (zc == 0) continue;
             const float cx = compat_centre(pi, G.left, G.pixel_size);
-            const float d = compat_plane_depth(G.hw, qx, qy, cx, cy);
+            const float d = compat_depth(Q, G.hw, cx, cy);
             if (d <= compat_unorder((uint32_t)(kk >> 32))) {
                 numer += zc;                                  // int32 sum with wrap, as the atomicAdd
                 denom += 1;
