@@ -219,9 +219,10 @@ def test_pipelined_host_run_matches_device_run(eng, reverse_out):
     rng = np.random.default_rng(17)
     rows, tiles, sides = [], [], []
     pt = 0
-    for k in range(10):
+    ntiles = 20                     # at least the slice count, with 4 Mi rows or more: sliced
+    for k in range(ntiles):
         side = int(rng.integers(150, 400))
-        n = int(rng.integers(350_000, 600_000))
+        n = int(rng.integers(220_000, 400_000))
         xyz = terrain_case(int(rng.integers(1, 1 << 30)), side, n, lakes=2, lake_r=(0.05 * side, 0.2 * side))
         xyz[:, 0] += 1_000_000 * k
         rows.append(xyz)
@@ -230,7 +231,7 @@ def test_pipelined_host_run_matches_device_run(eng, reverse_out):
         pt += n
     xyz_all = np.concatenate(rows)
     assert xyz_all.shape[0] >= 4 << 20
-    order = list(range(10))[::-1] if reverse_out else list(range(10))
+    order = list(range(ntiles))[::-1] if reverse_out else list(range(ntiles))
     out = {}
     o = 0
     for k in order:
@@ -238,7 +239,7 @@ def test_pipelined_host_run_matches_device_run(eng, reverse_out):
         o += sides[k] * sides[k]
     site = {}
     sp = 0
-    for k in range(10):
+    for k in range(ntiles):
         site[k] = sp
         sp += sides[k] * sides[k]
     tl = []
