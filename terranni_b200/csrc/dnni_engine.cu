@@ -664,7 +664,9 @@ static dnni_status plan_slices(dnni_batch* b) {
     constexpr double kSliceWeight[kSlices] = {0.05, 0.075, 0.11, 0.17, 0.25, 0.38, 0.57, 0.85,
                                               1.0, 1.0, 1.0, 1.0, 1.0, 0.5, 0.25, 0.12};
     const int n = (int)b->tiles_in.size();
-    const int S = (b->hb.n_rows >= (4 << 20) && n >= kSlices) ? kSlices : 1;
+    // fewer tiles than slices: one tile per slice, equal weights
+    const int S = b->hb.n_rows >= (4 << 20) ? std::min(n, kSlices) : 1;
+    const bool ramp = S == kSlices;
     b->sliced = S > 1;
     b->slices.clear();
     if (!b->sliced) {
@@ -681,15 +683,16 @@ static dnni_status plan_slices(dnni_batch* b) {
     };
     double total = 0;
     for (int k : idx) total += cost(k);
+    auto weight = [&](int s) { return ramp ? kSliceWeight[s] : 1.0; };
     double wsum = 0;
-    for (int s = 0; s < S; ++s) wsum += kSliceWeight[s];
+    for (int s = 0; s < S; ++s) wsum += weight(s);
     dnni_batch_options o = b->opt;
     o.order_by_cost = 0;
     double run = 0, wrun = 0;
     size_t k0 = 0;
     for (int s = 0; s < S; ++s) {
         size_t k1 = k0;
-        wrun += kSliceWeight[s];
+        wrun += weight(s);
         const double goal = total * wrun / wsum;
         while (k1 < idx.size() && (s == S - 1 || run + cost(idx[k1]) <= goal || k1 == k0)) run += cost(idx[k1++]);
         if (k1 == k0) break;

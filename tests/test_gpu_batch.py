@@ -209,20 +209,21 @@ def test_autotuned_options_give_the_same_heights(eng):
     _check(meta, ref, h, s)
 
 
-@pytest.mark.parametrize("reverse_out", [False, True])
-def test_pipelined_host_run_matches_device_run(eng, reverse_out):
+@pytest.mark.parametrize("reverse_out,ntiles", [(False, 20), (True, 20), (False, 6)])
+def test_pipelined_host_run_matches_device_run(eng, reverse_out, ntiles):
     """Batches of 4 Mi point rows or more run their host-buffer form in
-    slices whose upload, launches and download overlap; the result must equal
-    the device-buffer run, also when the tiles' outputs lie in the opposite
-    order to their points."""
+    slices whose upload, launches and download overlap (20 tiles: the full
+    ramp of slices; 6 tiles: one tile per slice); the result must equal the
+    device-buffer run, also when the tiles' outputs lie in the opposite order
+    to their points."""
     from terranni_b200 import engine
     rng = np.random.default_rng(17)
     rows, tiles, sides = [], [], []
     pt = 0
-    ntiles = 20                     # at least the slice count, with 4 Mi rows or more: sliced
+    per = (4 << 20) // ntiles + 1   # point rows per tile: 4 Mi or more in all
     for k in range(ntiles):
         side = int(rng.integers(150, 400))
-        n = int(rng.integers(220_000, 400_000))
+        n = int(rng.integers(per, per + 200_000))
         xyz = terrain_case(int(rng.integers(1, 1 << 30)), side, n, lakes=2, lake_r=(0.05 * side, 0.2 * side))
         xyz[:, 0] += 1_000_000 * k
         rows.append(xyz)
