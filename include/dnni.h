@@ -128,7 +128,8 @@ dnni_status dnni_interpolate_segment(dnni_ctx *ctx, const dnni_workpackage *wp,
                                      float *out_h, uint32_t *out_site, dnni_stats *stats);
 
 /* Device buffers on the context's device.  Work is queued on `stream`
- * (a cudaStream_t; NULL = the context's own stream).  The call synchronises
+ * (a cudaStream_t; NULL = the context's own stream, a blocking stream
+ * ordered with the legacy default stream).  The call synchronises
  * once, after the point bounding box, to size the search bins; it returns
  * with the remaining work queued unless stats is non-NULL, in which case it
  * waits for completion to fill the counters. */
@@ -201,7 +202,8 @@ typedef struct dnni_batch_options {
 dnni_status dnni_batch_create(dnni_ctx *ctx, const dnni_tile *tiles, int32_t ntiles,
                               const dnni_batch_options *options, dnni_batch **out);
 /* Runs every tile on device buffers, queued on `stream` (NULL = the
- * context's stream).  Returns with the work queued unless stats is non-NULL,
+ * context's stream, a blocking stream: ordered with the legacy default
+ * stream).  Returns with the work queued unless stats is non-NULL,
  * in which case it waits, reports totals over the tiles (ms_total is the
  * device time of the run; per-phase times too when the batch runs without
  * a graph) and checks the points against the declared extents

@@ -417,7 +417,10 @@ dnni_status dnni_init(const dnni_settings* settings, dnni_ctx** out) {
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) { delete c; return DNNI_E_CUDA; }
     c->sm_count = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return DNNI_E_CUDA; }
+    // a blocking stream: work queued on the context's stream is ordered with
+    // the legacy default stream, so callers that pass NULL (or a framework's
+    // default stream, whose handle is 0) read finished results there
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess) { delete c; return DNNI_E_CUDA; }
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) { dnni_destroy(c); return DNNI_E_CUDA; }
     if (cudaMallocHost(&c->h_sc, sizeof(Scalars)) != cudaSuccess ||

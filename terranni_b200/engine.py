@@ -435,6 +435,10 @@ class Batch:
         self.close()
 
     def run_device(self, d_xyz, d_h, d_gid=None, d_site=None, stream=None, stats=False):
+        """dnni_batch_run_device: queued on `stream` (a raw cudaStream_t, e.g.
+        torch.cuda.current_stream().cuda_stream; None = the context's own
+        stream) and returns before the kernels finish unless stats is asked
+        for (which synchronises)."""
         st = Stats() if stats else None
         self._eng._check(lib().dnni_batch_run_device(self._h, _ptr(d_xyz), _ptr(d_gid), _ptr(d_h), _ptr(d_site),
                                                      stream, ctypes.byref(st) if st is not None else None))
