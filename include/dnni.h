@@ -424,6 +424,13 @@ typedef struct dnni_st_options {
 dnni_status dnni_interpolate_spacetime(dnni_ctx *ctx, const dnni_workpackage *wp, const dnni_st_options *opt,
                                        const int32_t *xyz, const int32_t *t, int64_t n, float *h_out,
                                        dnni_stats *stats);
+/* The same on device buffers (points, times and heights on the context's
+ * device), queued on `stream` (NULL = the context's stream); the call waits
+ * once, for the per-time-value counts that size the batch, and returns with
+ * the rest queued unless stats is non-NULL. */
+dnni_status dnni_interpolate_spacetime_device(dnni_ctx *ctx, const dnni_workpackage *wp, const dnni_st_options *opt,
+                                              const int32_t *d_xyz, const int32_t *d_t, int64_t n, float *d_h,
+                                              void *stream, dnni_stats *stats);
 
 /* ---- input: LAS point files ----
  *

@@ -300,14 +300,12 @@ void launch_st_final(const BatchTables& bt, int ncta, int rs, const int2* pix, i
 
 }  // namespace dnni
 
-extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpackage* wp, const dnni_st_options* o,
-                                                  const int32_t* xyz, const int32_t* tt, int64_t n, float* h_out,
-                                                  dnni_stats* stats) {
-    if (!c) return DNNI_E_INVAL;
-    c->err.clear();
-    if (!wp || !o || !h_out || n < 0 || (n > 0 && (!xyz || !tt)))
-        return set_err(c, DNNI_E_INVAL, "NULL argument or negative point count");
-    DeviceGuard g(c->device);
+// Both entry points: host buffers (device = false: points and times copied
+// in, heights copied out, the call waits) or device buffers (queued on st;
+// it waits once, for the per-value counts, and at the end only for stats).
+static dnni_status spacetime_run(dnni_ctx* c, const dnni_workpackage* wp, const dnni_st_options* o,
+                                 const int32_t* xyz, const int32_t* tt, int64_t n, float* h_out, bool device,
+                                 cudaStream_t st, dnni_stats* stats) {
     const int rt = o->time_radius, tau = o->time_scale;
     if (rt < 0 || rt > kStMaxRadius || tau <= 0 || (int64_t)rt * tau > (1LL << 30))
         return set_err(c, DNNI_E_INVAL, "time_radius must be in [0, 16], time_scale > 0, their product <= 2^30");
@@ -320,18 +318,20 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
     if (npix * V >= (int64_t)INT32_MAX) return set_err(c, DNNI_E_INVAL, "raster pixels x time values exceed 2^31");
 
     if (n > (int64_t)INT32_MAX - 1) return set_err(c, DNNI_E_INVAL, "more than 2^31 - 2 points");
-    cudaStream_t st = c->stream;
     const int64_t t0 = (int64_t)o->cur_time - 2 * rt;
     const int64_t nb = std::max<int64_t>(n, 1);
-    if ((rs = dnni_ensure(c, c->st.xin, sizeof(int32_t) * 3 * (size_t)nb)) ||
-        (rs = dnni_ensure(c, c->st.tin, sizeof(int32_t) * (size_t)nb)) ||
+    if ((!device && ((rs = dnni_ensure(c, c->st.xin, sizeof(int32_t) * 3 * (size_t)nb)) ||
+                     (rs = dnni_ensure(c, c->st.tin, sizeof(int32_t) * (size_t)nb)) ||
+                     (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)))) ||
         (rs = dnni_ensure(c, c->st.xyz, sizeof(int32_t) * 3 * (size_t)nb)) ||
         (rs = dnni_ensure(c, c->st.idx, sizeof(uint32_t) * (size_t)nb)) ||
         (rs = dnni_ensure(c, c->st.gs, sizeof(StGroupStats))) ||
         (rs = dnni_ensure(c, c->st.site, sizeof(uint32_t) * (size_t)(V * npix))) ||
-        (rs = dnni_ensure(c, c->st.pix, sizeof(int2) * (size_t)(S * npix))) ||
-        (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)))
+        (rs = dnni_ensure(c, c->st.pix, sizeof(int2) * (size_t)(S * npix))))
         return rs;
+    const int32_t* dxyz = device ? xyz : (const int32_t*)c->st.xin.p;
+    const int32_t* dt = device ? tt : (const int32_t*)c->st.tin.p;
+    float* dh = device ? h_out : (float*)c->out_h.p;
     const bool timing = stats || (c->s.flags & DNNI_F_TIMING);
     if (timing) CK(cudaEventRecord(c->ev[0], st));
 
@@ -340,10 +340,11 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
     k_st_init<<<1, 128, 0, st>>>(gs);
     const int nchunk = (int)((n + kStChunk - 1) / kStChunk);
     if (n > 0) {
-        CK(cudaMemcpyAsync(c->st.xin.p, xyz, sizeof(int32_t) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(c->st.tin.p, tt, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
-        k_st_count<<<nchunk, 256, 0, st>>>((const int32_t*)c->st.xin.p, (const int32_t*)c->st.tin.p, n, t0, V,
-                                           wp->origin_x, wp->origin_y, gs);
+        if (!device) {
+            CK(cudaMemcpyAsync(c->st.xin.p, xyz, sizeof(int32_t) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(c->st.tin.p, tt, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+        }
+        k_st_count<<<nchunk, 256, 0, st>>>(dxyz, dt, n, t0, V, wp->origin_x, wp->origin_y, gs);
     }
     StGroupStats hg;
     CK(cudaMemcpyAsync(&hg, gs, sizeof(StGroupStats), cudaMemcpyDeviceToHost, st));
@@ -365,8 +366,7 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
             zmax = std::max(zmax, hg.bb[v][5]);
         }
     if (m > 0)
-        k_st_scatter<<<nchunk, 256, 0, st>>>((const int32_t*)c->st.xin.p, (const int32_t*)c->st.tin.p, n, P, gs,
-                                             (int32_t*)c->st.xyz.p, (uint32_t*)c->st.idx.p);
+        k_st_scatter<<<nchunk, 256, 0, st>>>(dxyz, dt, n, P, gs, (int32_t*)c->st.xyz.p, (uint32_t*)c->st.idx.p);
 
     // 2. nearest site per time value: one 2-D batch, one tile per value
     std::vector<dnni_tile> tiles((size_t)V);
@@ -416,8 +416,8 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
     k_init_scalars<<<1, 32, 0, st>>>(bt, a.sc, a.ctr);
     int2* pix = (int2*)c->st.pix.p;
     const int64_t lifts = (int64_t)S * npix;
-    k_st_lift<<<(unsigned)((lifts + 255) / 256), 256, 0, st>>>(T, P, (const uint32_t*)c->st.site.p,
-                                                               (const int32_t*)c->st.xin.p, pix, a.sc);
+    k_st_lift<<<(unsigned)((lifts + 255) / 256), 256, 0, st>>>(T, P, (const uint32_t*)c->st.site.p, dxyz, pix,
+                                                               a.sc);
     k_st_decide<<<1, 32, 0, st>>>(a.sc, m > 0 ? zmin : 1, m > 0 ? zmax : 0, npix, S);
     if (timing) CK(cudaEventRecord(c->ev[2], st));
     CK(cudaMemsetAsync(a.D, 0, sizeof(unsigned long long) * (size_t)cells, st));
@@ -426,15 +426,15 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
     for (int s = 0; s < S; ++s) k_scatter_spans<<<nrt, dim3(32, 8), 0, st>>>(bt, pix + (int64_t)s * npix, a.sc, a.D, a.Dc);
     if (timing) CK(cudaEventRecord(c->ev[3], st));
     k_rowscan<<<hb.grow_base.back(), kScanThreads, 0, st>>>(bt, a.D, a.Dc, a.sc);
-    launch_st_final(bt, hb.ct_base.back(), hb.rs, pix, S, npix, a.sc, a.D, a.Dc, (float*)c->out_h.p, st);
+    launch_st_final(bt, hb.ct_base.back(), hb.rs, pix, S, npix, a.sc, a.D, a.Dc, dh, st);
     CK(cudaGetLastError());
     if (timing) CK(cudaEventRecord(c->ev[4], st));
-    CK(cudaMemcpyAsync(h_out, c->out_h.p, sizeof(float) * (size_t)cells, cudaMemcpyDeviceToHost, st));
+    if (!device) CK(cudaMemcpyAsync(h_out, c->out_h.p, sizeof(float) * (size_t)cells, cudaMemcpyDeviceToHost, st));
     if (stats) {
         memset(stats, 0, sizeof(*stats));
         CK(cudaMemcpyAsync(c->h_sc, a.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
     }
-    CK(cudaStreamSynchronize(st));
+    if (!device || timing) CK(cudaStreamSynchronize(st));
     c->calls++;
     if (timing) {
         float ms[4];
@@ -453,8 +453,31 @@ extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpa
         stats->n_cells = cells;
         stats->n_pixels = npix * S;
         fold_stats(c->h_sc, 1, stats);
-        stats->h2d_bytes = (int64_t)(16 * n);
-        stats->d2h_bytes = (int64_t)(sizeof(float) * cells);
+        stats->h2d_bytes = device ? 0 : (int64_t)(16 * n);
+        stats->d2h_bytes = device ? 0 : (int64_t)(sizeof(float) * cells);
     }
     return DNNI_OK;
+}
+
+extern "C" dnni_status dnni_interpolate_spacetime(dnni_ctx* c, const dnni_workpackage* wp, const dnni_st_options* o,
+                                                  const int32_t* xyz, const int32_t* tt, int64_t n, float* h_out,
+                                                  dnni_stats* stats) {
+    if (!c) return DNNI_E_INVAL;
+    c->err.clear();
+    if (!wp || !o || !h_out || n < 0 || (n > 0 && (!xyz || !tt)))
+        return set_err(c, DNNI_E_INVAL, "NULL argument or negative point count");
+    DeviceGuard g(c->device);
+    return spacetime_run(c, wp, o, xyz, tt, n, h_out, false, c->stream, stats);
+}
+
+extern "C" dnni_status dnni_interpolate_spacetime_device(dnni_ctx* c, const dnni_workpackage* wp,
+                                                         const dnni_st_options* o, const int32_t* d_xyz,
+                                                         const int32_t* d_t, int64_t n, float* d_h, void* stream,
+                                                         dnni_stats* stats) {
+    if (!c) return DNNI_E_INVAL;
+    c->err.clear();
+    if (!wp || !o || !d_h || n < 0 || (n > 0 && (!d_xyz || !d_t)))
+        return set_err(c, DNNI_E_INVAL, "NULL argument or negative point count");
+    DeviceGuard g(c->device);
+    return spacetime_run(c, wp, o, d_xyz, d_t, n, d_h, true, stream ? (cudaStream_t)stream : c->stream, stats);
 }

@@ -214,6 +214,8 @@ _SIGS = {
                              ctypes.c_double, ctypes.c_float], ctypes.c_int),
     "dnni_interpolate_spacetime": ([_P, ctypes.POINTER(WorkPackage), ctypes.POINTER(StOptions), _P, _P,
                                     ctypes.c_int64, _P, _P], ctypes.c_int),
+    "dnni_interpolate_spacetime_device": ([_P, ctypes.POINTER(WorkPackage), ctypes.POINTER(StOptions), _P, _P,
+                                           ctypes.c_int64, _P, _P, _P], ctypes.c_int),
     "dnni_interpolate_compat": ([_P, ctypes.POINTER(CompatSettings), ctypes.POINTER(CompatWP), _P, ctypes.c_int64,
                                  _P, _P], ctypes.c_int),
     "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
@@ -333,6 +335,17 @@ class Engine:
         self._check(lib().dnni_interpolate_spacetime(self._h, ctypes.byref(wp), ctypes.byref(opt), _ptr(xyz), _ptr(t),
                                                      xyz.shape[0], _ptr(h), ctypes.byref(st)))
         return h, st
+
+    def interpolate_spacetime_device(self, wp: WorkPackage, d_xyz, d_t, n, d_h, cur_time, time_radius, time_scale,
+                                     stream=None, stats=True):
+        """dnni_interpolate_spacetime_device: device buffers (torch tensors or
+        raw addresses), queued on `stream` (raw cudaStream_t)."""
+        st = Stats() if stats else None
+        opt = StOptions(int(cur_time), int(time_radius), int(time_scale), 0)
+        self._check(lib().dnni_interpolate_spacetime_device(
+            self._h, ctypes.byref(wp), ctypes.byref(opt), _ptr(d_xyz), _ptr(d_t), int(n), _ptr(d_h), stream,
+            ctypes.byref(st) if st is not None else None))
+        return st
 
     def interpolate_device(self, wp: WorkPackage, d_xyz, n, d_h, d_gid=None, d_site=None, stream=None,
                            stats=True):

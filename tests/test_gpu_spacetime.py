@@ -100,3 +100,21 @@ def test_spacetime_negative_times_and_origin(eng, oracle):
     h, _ = eng.interpolate_spacetime(engine.make_wp(72, 72, 100, **args), xyz, t, -3, 1, 100)
     assert np.array_equal(h.view(np.uint32), ref["h"].view(np.uint32))
     assert (ref["h"] != np.float32(-9999.0)).mean() > 0.9
+
+
+def test_spacetime_device_buffers_equal_host_buffers(eng):
+    # dnni_interpolate_spacetime_device: the same heights from device-resident
+    # points and times, read back after the call queued on torch's stream
+    import torch
+    from terranni_b200 import engine
+    xyz, t = _terrain(41, 160, 12000, 100, 8, 2, 6)
+    wp = engine.make_wp(160, 160, 100, raster=(-3, -3, 163, 163))
+    h_host, _ = eng.interpolate_spacetime(wp, xyz, t, 8, 2, 100)
+    d_xyz = torch.from_numpy(xyz).cuda()
+    d_t = torch.from_numpy(t).cuda()
+    for stats in (True, False):
+        d_h = torch.zeros(160 * 160, dtype=torch.float32, device="cuda")
+        eng.interpolate_spacetime_device(wp, d_xyz, d_t, xyz.shape[0], d_h, 8, 2, 100,
+                                         stream=torch.cuda.current_stream().cuda_stream, stats=stats)
+        h = d_h.cpu().numpy().reshape(160, 160)
+        assert np.array_equal(h.view(np.uint32), h_host.view(np.uint32))
