@@ -391,6 +391,11 @@ typedef struct dnni_compat_wp {         /* nni::WorkPackage (nni.h:66-70) */
 
 dnni_status dnni_interpolate_compat(dnni_ctx *ctx, const dnni_compat_settings *settings, const dnni_compat_wp *wp,
                                     const double *xyz, int64_t n, float *h_out, int32_t *res_out);
+/* The same on device buffers, queued on `stream` (NULL = the context's
+ * stream); returns with the work queued. */
+dnni_status dnni_interpolate_compat_device(dnni_ctx *ctx, const dnni_compat_settings *settings,
+                                           const dnni_compat_wp *wp, const double *d_xyz, int64_t n, float *d_h,
+                                           int32_t *d_res, void *stream);
 
 /* ---- space-time interpolation: nni::performNNI with timeRadius > 0 ----
  *

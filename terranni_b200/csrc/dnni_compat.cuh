@@ -239,11 +239,11 @@ __global__ void __launch_bounds__(256) k_compat_cells(CompatGeom G, const double
 
 }  // namespace dnni
 
-extern "C" dnni_status dnni_interpolate_compat(dnni_ctx* c, const dnni_compat_settings* s, const dnni_compat_wp* wp,
-                                               const double* xyz, int64_t n, float* h_out, int32_t* res_out) {
-    if (!c || !s || !wp || !h_out || n < 0 || (n > 0 && !xyz)) return DNNI_E_INVAL;
-    c->err.clear();
-    DeviceGuard g(c->device);
+// Both entry points: host buffers (device = false: points copied in,
+// heights and quotients copied out, the call waits) or device buffers
+// (queued on st; the call returns with the work queued).
+static dnni_status compat_run(dnni_ctx* c, const dnni_compat_settings* s, const dnni_compat_wp* wp, const double* xyz,
+                              int64_t n, float* h_out, int32_t* res_out, bool device, cudaStream_t st) {
     if (s->scale <= 0 || !(s->cell_size > 0) || wp->nrows <= 0 || wp->ncols <= 0 || s->multiplier <= 0)
         return set_err(c, DNNI_E_INVAL, "scale, cell size, grid sides and multiplier must be positive");
     if ((uint64_t)n >= 0xFFFFFFFFull) return set_err(c, DNNI_E_INVAL, "too many points for 32-bit draw order");
@@ -286,32 +286,51 @@ extern "C" dnni_status dnni_interpolate_compat(dnni_ctx* c, const dnni_compat_se
     if ((rs = dnni_ensure(c, c->scr.D, sizeof(unsigned long long) * (size_t)(xp * yp))) ||
         (rs = dnni_ensure(c, c->scr.cnt, tbytes)) ||
         (rs = dnni_ensure(c, c->scr.rank, sizeof(uint32_t) * (size_t)list_n)) ||
-        (rs = dnni_ensure(c, c->in_xyz, sizeof(double) * 3 * (size_t)std::max<int64_t>(n, 1))) ||
-        (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)) ||
-        (res_out && (rs = dnni_ensure(c, c->out_site, sizeof(int32_t) * (size_t)cells))))
+        (!device && ((rs = dnni_ensure(c, c->in_xyz, sizeof(double) * 3 * (size_t)std::max<int64_t>(n, 1))) ||
+                     (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)) ||
+                     (res_out && (rs = dnni_ensure(c, c->out_site, sizeof(int32_t) * (size_t)cells))))))
         return rs;
-    cudaStream_t st = c->stream;
+    const double* dxyz = device ? xyz : (const double*)c->in_xyz.p;
+    float* dh = device ? h_out : (float*)c->out_h.p;
+    int32_t* dres = res_out ? (device ? res_out : (int32_t*)c->out_site.p) : nullptr;
     unsigned long long* key = (unsigned long long*)c->scr.D.p;
     long long* toff = (long long*)c->scr.cnt.p;
     int* tcnt = (int*)(toff + nt + 1);
     int* tcur = tcnt + nt;
     CK(cudaMemsetAsync(tcnt, 0, sizeof(int) * (size_t)nt, st));
     if (n > 0) {
-        CK(cudaMemcpyAsync(c->in_xyz.p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
-        k_compat_count<<<c->sm_count * 8, 256, 0, st>>>(G, (const double*)c->in_xyz.p, n, ntx, tcnt);
+        if (!device) CK(cudaMemcpyAsync(c->in_xyz.p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
+        k_compat_count<<<c->sm_count * 8, 256, 0, st>>>(G, dxyz, n, ntx, tcnt);
     }
     k_compat_offsets<<<1, 1024, 0, st>>>(tcnt, nt, toff, tcur);
     if (n > 0)
-        k_compat_fill<<<c->sm_count * 8, 256, 0, st>>>(G, (const double*)c->in_xyz.p, n, ntx, toff, tcur,
-                                                       (uint32_t*)c->scr.rank.p, list_n);
+        k_compat_fill<<<c->sm_count * 8, 256, 0, st>>>(G, dxyz, n, ntx, toff, tcur, (uint32_t*)c->scr.rank.p, list_n);
     CK(cudaFuncSetAttribute(k_compat_sites, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCpTileSmem));
-    k_compat_sites<<<nt, 256, kCpTileSmem, st>>>(G, (const double*)c->in_xyz.p, ntx, toff,
-                                                 (const uint32_t*)c->scr.rank.p, list_n, key);
-    k_compat_cells<<<(int)((cells + 255) / 256), 256, 0, st>>>(G, (const double*)c->in_xyz.p, key, (float*)c->out_h.p,
-                                                               res_out ? (int32_t*)c->out_site.p : nullptr);
+    k_compat_sites<<<nt, 256, kCpTileSmem, st>>>(G, dxyz, ntx, toff, (const uint32_t*)c->scr.rank.p, list_n, key);
+    k_compat_cells<<<(int)((cells + 255) / 256), 256, 0, st>>>(G, dxyz, key, dh, dres);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h_out, c->out_h.p, sizeof(float) * (size_t)cells, cudaMemcpyDeviceToHost, st));
-    if (res_out) CK(cudaMemcpyAsync(res_out, c->out_site.p, sizeof(int32_t) * (size_t)cells, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    if (!device) {
+        CK(cudaMemcpyAsync(h_out, c->out_h.p, sizeof(float) * (size_t)cells, cudaMemcpyDeviceToHost, st));
+        if (res_out)
+            CK(cudaMemcpyAsync(res_out, c->out_site.p, sizeof(int32_t) * (size_t)cells, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
     return DNNI_OK;
+}
+
+extern "C" dnni_status dnni_interpolate_compat(dnni_ctx* c, const dnni_compat_settings* s, const dnni_compat_wp* wp,
+                                               const double* xyz, int64_t n, float* h_out, int32_t* res_out) {
+    if (!c || !s || !wp || !h_out || n < 0 || (n > 0 && !xyz)) return DNNI_E_INVAL;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    return compat_run(c, s, wp, xyz, n, h_out, res_out, false, c->stream);
+}
+
+extern "C" dnni_status dnni_interpolate_compat_device(dnni_ctx* c, const dnni_compat_settings* s,
+                                                      const dnni_compat_wp* wp, const double* d_xyz, int64_t n,
+                                                      float* d_h, int32_t* d_res, void* stream) {
+    if (!c || !s || !wp || !d_h || n < 0 || (n > 0 && !d_xyz)) return DNNI_E_INVAL;
+    c->err.clear();
+    DeviceGuard g(c->device);
+    return compat_run(c, s, wp, d_xyz, n, d_h, d_res, true, stream ? (cudaStream_t)stream : c->stream);
 }

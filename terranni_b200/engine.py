@@ -216,6 +216,8 @@ _SIGS = {
                                     ctypes.c_int64, _P, _P], ctypes.c_int),
     "dnni_interpolate_spacetime_device": ([_P, ctypes.POINTER(WorkPackage), ctypes.POINTER(StOptions), _P, _P,
                                            ctypes.c_int64, _P, _P, _P], ctypes.c_int),
+    "dnni_interpolate_compat_device": ([_P, ctypes.POINTER(CompatSettings), ctypes.POINTER(CompatWP), _P,
+                                        ctypes.c_int64, _P, _P, _P], ctypes.c_int),
     "dnni_interpolate_compat": ([_P, ctypes.POINTER(CompatSettings), ctypes.POINTER(CompatWP), _P, ctypes.c_int64,
                                  _P, _P], ctypes.c_int),
     "dnni_batch_autotune": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, _P, _P, ctypes.c_int32,
@@ -398,6 +400,12 @@ class Engine:
         self._check(lib().dnni_interpolate_compat(self._h, ctypes.byref(settings), ctypes.byref(wp), _ptr(pts),
                                                   pts.shape[0], _ptr(h), _ptr(res)))
         return h, res
+
+    def interpolate_compat_device(self, settings: CompatSettings, wp: CompatWP, d_pts, n, d_h, d_res=None,
+                                  stream=None):
+        """dnni_interpolate_compat_device: device buffers, queued on `stream`."""
+        self._check(lib().dnni_interpolate_compat_device(self._h, ctypes.byref(settings), ctypes.byref(wp),
+                                                         _ptr(d_pts), int(n), _ptr(d_h), _ptr(d_res), stream))
 
     def clear(self):
         self._check(lib().dnni_clear(self._h))

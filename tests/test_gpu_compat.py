@@ -70,3 +70,23 @@ def test_compat_rejects_bad_settings(eng):
     with pytest.raises(engine.DnniError) as ei:
         eng.interpolate_compat(se, we, np.zeros((1, 3)))
     assert ei.value.status == 1
+
+
+def test_compat_device_buffers_equal_host_buffers(eng, oracle):
+    import torch
+    from terranni_b200 import engine
+    c = _cases()[0]
+    zmax = float(c["pts"][:, 2].max())
+    mult = oracle.compat_multiplier(c["sr"], c["scale"], c["cell"], zmax, c["pmin"])
+    se = engine.CompatSettings(scale=c["scale"], cell_size=c["cell"], site_radius=c["sr"], query_radius=c["qr"],
+                               point_min=c["pmin"], multiplier=mult, total_ncols=c["ncols"], total_nrows=c["nrows"])
+    we = engine.CompatWP(origin_x=c["origin"][0], origin_y=c["origin"][1], grid_origin_x=0.0, grid_origin_y=0.0,
+                         nrows=c["nrows"], ncols=c["ncols"])
+    h, res = eng.interpolate_compat(se, we, c["pts"])
+    d_pts = torch.from_numpy(np.ascontiguousarray(c["pts"], np.float64)).cuda()
+    d_h = torch.zeros(c["nrows"] * c["ncols"], dtype=torch.float32, device="cuda")
+    d_r = torch.zeros(c["nrows"] * c["ncols"], dtype=torch.int32, device="cuda")
+    eng.interpolate_compat_device(se, we, d_pts, c["pts"].shape[0], d_h, d_r,
+                                  stream=torch.cuda.current_stream().cuda_stream)
+    assert np.array_equal(d_h.cpu().numpy().reshape(h.shape).view(np.uint32), h.view(np.uint32))
+    assert np.array_equal(d_r.cpu().numpy().reshape(res.shape), res)
