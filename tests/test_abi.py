@@ -70,3 +70,33 @@ def test_sinusoid_workload_shape():
     assert xyz[:, :2].min() >= 0 and xyz[:, :2].max() < 51200
     z = xyz[:, 2] * 0.01
     assert -80.5 < z.min() < 0 < z.max() < 80.5
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    # a C99 translation unit (what cgo, JNI or ctypes bindings would see)
+    # takes the address of every declared function and links against the
+    # library
+    import subprocess
+    names = declared("dnni.h")
+    src = tmp_path / "abi.c"
+    src.write_text("#include <stdio.h>\n#include \"dnni.h\"\ntypedef void (*fn_t)(void);\nint main(void) {\n"
+                   "    fn_t fns[] = {\n" + "".join(f"        (fn_t)&{n},\n" for n in names) + "    };\n"
+                   "    printf(\"%d\\n\", (int)(sizeof(fns) / sizeof(fns[0])));\n"
+                   "    return dnni_version() == 10000 ? 0 : 1;\n}\n")
+    exe = tmp_path / "abi"
+    lib = os.path.join(ROOT, "terranni_b200")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L", lib, "-ldnni", f"-Wl,-rpath,{lib}"], check=True,
+                   capture_output=True, text=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and int(r.stdout) == len(names)
+
+
+def test_new_entry_points_reject_null_arguments():
+    from terranni_b200 import engine
+    L = engine.lib()
+    for name in ("dnni_interpolate_spacetime", "dnni_interpolate_spacetime_device", "dnni_interpolate_compat",
+                 "dnni_interpolate_compat_device"):
+        f = getattr(L, name)
+        args = [0 if t in (ctypes.c_int64, ctypes.c_int32, ctypes.c_int) else None for t in f.argtypes]
+        assert f(*args) == 1, name                 # NULL context: DNNI_E_INVAL
