@@ -134,3 +134,49 @@ def test_space_time_caller_matches_oracle(tmp_path, oracle, rt, delta):
         assert np.array_equal(got["h"].view(np.uint32), want.view(np.uint32))
         first = cur + 1 if delta else cur + 1 - 2 * rt
         assert pos[cur] == int(np.searchsorted(times, first))
+
+
+def _stub_build(tmp_path):
+    """The time demo linked against tests/native/dnni_stub.c (no GPU)."""
+    lib = tmp_path / "libdnni.so"
+    subprocess.run(["gcc", "-shared", "-fPIC", "-std=c99", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "native", "dnni_stub.c"), "-o", str(lib)], check=True,
+                   capture_output=True, text=True)
+    exe = tmp_path / "time_demo"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(ROOT, "include"), TSRC, "-o", str(exe),
+                    "-L", str(tmp_path), "-ldnni", f"-Wl,-rpath,{tmp_path}"], check=True, capture_output=True,
+                   text=True)
+    return exe
+
+
+@pytest.mark.parametrize("rt,delta", [(1, 1), (1, 0), (2, 1), (2, 0)])
+def test_space_time_stream_handling_on_cpu(tmp_path, rt, delta):
+    """The drop-in's space-time reads (nni.cpp:750-788), seeks and Delta-mode
+    slice reuse (nni.cpp:325-359), with a stub engine: each call hands the
+    engine exactly the points within 2 rt of its time, and the stream ends
+    where the reference's seeks leave it."""
+    exe = _stub_build(tmp_path)
+    rng = np.random.default_rng(3)
+    n = 4000
+    times = np.sort(rng.integers(0, 13, n)).astype(np.int32)
+    pts = np.zeros(n, POINT4D)
+    pts["x"], pts["y"], pts["z"], pts["t"] = rng.uniform(0, 30, n), rng.uniform(0, 30, n), 1.0, times
+    pin = tmp_path / "pts.bin"
+    pts.tofile(pin)
+    log = tmp_path / "calls.log"
+    t0, t1 = 4, 8
+    env = dict(os.environ, DNNI_STUB_LOG=str(log))
+    r = subprocess.run([str(exe), str(pin), str(tmp_path / "out_"), "30", "30", "1.0", "3.0", str(rt), str(t0),
+                        str(t1), str(delta)], capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 0, r.stderr
+    pos = {int(a[1]): int(a[3]) for a in (ln.split() for ln in r.stdout.splitlines()) if a[0] == "t"}
+    calls = [ln.split() for ln in log.read_text().splitlines()]
+    assert [c[0] for c in calls] == ["spacetime"] * (t1 - t0 + 1)
+    for cur, c in zip(range(t0, t1 + 1), calls):
+        want = int(np.count_nonzero(np.abs(times - cur) <= 2 * rt))
+        assert int(c[1]) == want
+        assert int(c[2]) >= cur - 2 * rt and int(c[3]) <= cur + 2 * rt
+        first = cur + 1 if delta else cur + 1 - 2 * rt
+        assert pos[cur] == int(np.searchsorted(times, first))
+        out = np.fromfile(tmp_path / f"out_{cur}.bin", OUTPOINT)
+        assert out.shape[0] == 30 * 30 and np.all(out["h"] == 1.0)
