@@ -180,3 +180,37 @@ def test_space_time_stream_handling_on_cpu(tmp_path, rt, delta):
         assert pos[cur] == int(np.searchsorted(times, first))
         out = np.fromfile(tmp_path / f"out_{cur}.bin", OUTPOINT)
         assert out.shape[0] == 30 * 30 and np.all(out["h"] == 1.0)
+
+
+@pytest.mark.parametrize("compat", [False, True])
+def test_reference_caller_host_logic_on_cpu(tmp_path, compat):
+    """The 2-D drop-in with a stub engine: the time slice's points go to the
+    engine (canonical or reference-default call), and the OutPoints cover the
+    work package clipped to the global grid, i-major (nni.cpp:836-858)."""
+    lib = tmp_path / "libdnni.so"
+    subprocess.run(["gcc", "-shared", "-fPIC", "-std=c99", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "native", "dnni_stub.c"), "-o", str(lib)], check=True,
+                   capture_output=True, text=True)
+    exe = tmp_path / "demo"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(ROOT, "include"), SRC, "-o", str(exe),
+                    "-L", str(tmp_path), "-ldnni", f"-Wl,-rpath,{tmp_path}"], check=True, capture_output=True,
+                   text=True)
+    rng = np.random.default_rng(4)
+    n = 3000
+    pts = np.zeros(n, POINT4D)
+    pts["x"], pts["y"], pts["z"] = 100.0 + rng.uniform(0, 40, n), 200.0 + rng.uniform(0, 30, n), 5.0
+    pts["t"] = np.where(np.arange(n) < 2500, 0, 1)          # the stream's next slice follows
+    pin, pout, log = tmp_path / "pts.bin", tmp_path / "out.bin", tmp_path / "calls.log"
+    pts.tofile(pin)
+    args = [str(exe), str(pin), str(pout), "40", "30", "1.0", "100", "200", "7", "3", "45", "30", "3.0"]
+    if compat:
+        args += ["5", "5.0", "0", "10000"]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=120, env=dict(os.environ, DNNI_STUB_LOG=str(log)))
+    assert r.returncode == 0, r.stderr
+    call = log.read_text().split()
+    assert call[0] == ("compat" if compat else "segment") and int(call[1]) == 2500
+    assert "stream position 2500 of 3000" in r.stdout          # left at the next slice (nni.cpp:782-788)
+    got = np.fromfile(pout, OUTPOINT)
+    want = [(i + 7, j + 3) for i in range(40) for j in range(30) if i + 7 < 45 and j + 3 < 30]
+    assert got.shape[0] == len(want)
+    assert np.array_equal(got["i"], [w[0] for w in want]) and np.array_equal(got["j"], [w[1] for w in want])
