@@ -704,7 +704,10 @@ def run_engine_segment(args, world, rank, local):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(st.h2d_bytes),
                     "d2h_bytes_per_step": int(st.d2h_bytes),
                     "note": "the segment call is host to host: its value is already end to end"},
-            "gpu_launches": int(sum(4 + x.batches * (KERNELS_PER_BATCH + 1) for x in stats)),
+            # per call: bucket counts, two partition passes, bucket boxes and the
+            # occupancy map; per batch: the gather, the batch's sequence and the
+            # halo check
+            "gpu_launches": int(sum(5 + x.batches * (KERNELS_PER_BATCH + 2) for x in stats)),
             "clocks": clk.summary(), "nodata_cells": nod,
         }), flush=True)
     eng.close()
