@@ -796,6 +796,10 @@ def run_engine_spacetime(args, world, rank, local):
             "e2e": {"value": cells * args.steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(st.h2d_bytes),
                     "d2h_bytes_per_step": int(st.d2h_bytes), "ms_per_step": ms_step,
                     "note": "host to host from pinned buffers (upload, grouping by time on the device, download)"},
+            # per call: grouping (3), the per-value nearest-site batch (12), the
+            # lift and packing decision (3), one span pass per slice, the row scan
+            # and the gather-and-divide
+            "gpu_launches": args.steps * (20 + 2 * rt + 1),
             "cpu_baseline": cpu, "clocks": clk.summary(),
         }), flush=True)
     eng.close()
