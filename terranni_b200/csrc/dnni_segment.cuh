@@ -623,11 +623,16 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
             // sqrt(2)/2 of c.  d is 1-Lipschitz, so d(p') >= |c - q| -
             // sqrt(2)/2 > h_s - 1.21; R <= h_s - 2 over those two lines rules
             // p out.  A side on the grid's edge has no pixel beyond it.
-            const double R = std::sqrt((double)mr2 + 1.0);
-            const bool okB = all_buckets[k] || R <= T.hp;
+            // A tile whose point box held no point found no site at all
+            // (mr2 < 0): unless its box already covers every bucket (there is
+            // no point anywhere), the nearest sites lie beyond the box at a
+            // distance nothing here bounds, so the point halo doubles.
+            const bool none = mr2 < 0;
+            const double R = std::sqrt((double)std::max(mr2, 0) + 1.0);
+            const bool okB = all_buckets[k] || (!none && R <= T.hp);
             SegTile U = T;
             bool again = !okB;
-            if (!okB) U.hp = std::max(2 * T.hp, (int)std::ceil(R) + 3);
+            if (!okB) U.hp = none ? std::max(2 * T.hp, 8) : std::max(2 * T.hp, (int)std::ceil(R) + 3);
             for (int sd = 0; sd < 4; ++sd) {
                 if (clipped[4 * k + sd]) continue;
                 const double Rs = std::sqrt((double)ring[4 * k + sd] + 1.0);

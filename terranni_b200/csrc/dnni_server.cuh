@@ -397,13 +397,17 @@ void srv_finish(dnni_server* s, SrvSlot& sl, cudaError_t e) {
             const Scalars& sc = sl.h_sc[pos++];
             int mr2 = -1;
             for (int l = 0; l < kStatSlots; ++l) mr2 = std::max(mr2, sc.max_r2[l]);
-            const double R = std::sqrt((double)mr2 + 1.0);
-            const bool okA = it.all_raster || R <= it.hr - 2;
-            const bool okB = it.all_buckets || R <= it.hr;
+            // no site found (mr2 < 0): the box held no point, so unless it
+            // covers every bucket the sites lie beyond it (the occupancy bound
+            // rules this out; the check keeps it from being accepted anyway)
+            const bool none = mr2 < 0;
+            const double R = std::sqrt((double)std::max(mr2, 0) + 1.0);
+            const bool okA = it.all_raster || none || R <= it.hr - 2;
+            const bool okB = it.all_buckets || (!none && R <= it.hr);
             if (sl.h_ctr->err & kErrRange) {
                 q.status = DNNI_E_RANGE;
             } else if (!(okA && okB)) {
-                q.hr_force = std::max(2 * it.hr, (int)std::ceil(R) + 3);
+                q.hr_force = none ? std::max(2 * it.hr, 8) : std::max(2 * it.hr, (int)std::ceil(R) + 3);
                 q.runs++;
                 s->queue.push_front(it.ticket);
                 continue;

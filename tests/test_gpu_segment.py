@@ -65,3 +65,18 @@ def test_segment_without_points_is_all_nodata(eng):
     h, s, st = eng.segment_run(np.zeros((0, 3), np.int32), 300, 200, 100, tile=128, site=True)
     assert np.all(h == np.float32(-9999.0)) and np.all(s == 0xFFFFFFFF)
     assert st.tile_runs == st.tiles
+
+
+@pytest.mark.parametrize("npts,halo", [(1, 0), (3, 0), (5, 4)])
+def test_segment_with_a_few_points_for_the_whole_grid(eng, npts, halo):
+    # the occupancy bound makes halos of hundreds of cells (or, from a small
+    # first halo, reruns grow them); the grid must still equal one work package
+    from terranni_b200 import engine
+    rng = np.random.default_rng(npts)
+    xyz = np.stack([rng.integers(0, 60_000, npts), rng.integers(0, 40_000, npts),
+                    rng.integers(0, 9000, npts)], 1).astype(np.int32)
+    ref_h, ref_s, _ = eng.interpolate(engine.make_wp(600, 400, 100), xyz, site=True)
+    h, s, st = eng.segment_run(xyz, 600, 400, 100, tile=128, halo=halo, tiles_per_batch=8, site=True)
+    assert np.array_equal(s, ref_s)
+    assert np.array_equal(h.view(np.uint32), ref_h.view(np.uint32))
+    assert st.max_halo > 100
