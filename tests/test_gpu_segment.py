@@ -80,3 +80,18 @@ def test_segment_with_a_few_points_for_the_whole_grid(eng, npts, halo):
     assert np.array_equal(s, ref_s)
     assert np.array_equal(h.view(np.uint32), ref_h.view(np.uint32))
     assert st.max_halo > 100
+
+
+def test_segment_with_all_points_beyond_the_grid(eng):
+    # the points lie 2-3 km west of and below the grid: they fall into the
+    # edge buckets, the occupancy bound underestimates their distance, and
+    # the halo checks must grow the boxes until the stitched grid equals one
+    # work package
+    from terranni_b200 import engine
+    rng = np.random.default_rng(9)
+    xyz = np.stack([rng.integers(-300_000, -200_000, 30), rng.integers(-250_000, 40_000, 30),
+                    rng.integers(0, 9000, 30)], 1).astype(np.int32)
+    ref_h, ref_s, _ = eng.interpolate(engine.make_wp(400, 300, 100), xyz, site=True)
+    h, s, st = eng.segment_run(xyz, 400, 300, 100, tile=128, halo=0, tiles_per_batch=4, site=True)
+    assert np.array_equal(s, ref_s)
+    assert np.array_equal(h.view(np.uint32), ref_h.view(np.uint32))
