@@ -4,6 +4,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -100,3 +101,29 @@ def test_new_entry_points_reject_null_arguments():
         f = getattr(L, name)
         args = [0 if t in (ctypes.c_int64, ctypes.c_int32, ctypes.c_int) else None for t in f.argtypes]
         assert f(*args) == 1, name                 # NULL context: DNNI_E_INVAL
+
+
+def test_pinned_host_allocation_arguments():
+    # dnni_host_alloc / dnni_host_free: NULL handling, and without a device a
+    # clean DNNI_E_NOMEM with NULL
+    import torch
+    from terranni_b200 import engine
+    L = engine.lib()
+    assert L.dnni_host_alloc(16, None) == 1
+    assert L.dnni_host_free(None) == 0
+    if torch.cuda.is_available():
+        return
+    p = ctypes.c_void_p()
+    assert L.dnni_host_alloc(1 << 20, ctypes.byref(p)) == 2 and not p.value
+
+
+@pytest.mark.gpu
+def test_pinned_host_allocation():
+    from terranni_b200 import engine
+    L = engine.lib()
+    p = ctypes.c_void_p()
+    assert L.dnni_host_alloc(1 << 20, ctypes.byref(p)) == 0 and p.value
+    buf = (ctypes.c_uint8 * (1 << 20)).from_address(p.value)
+    buf[0], buf[(1 << 20) - 1] = 7, 9
+    assert buf[0] == 7 and buf[(1 << 20) - 1] == 9
+    assert L.dnni_host_free(p) == 0
