@@ -62,3 +62,16 @@ def test_collinear_points(eng, oracle):
     t = rng.integers(0, 180, 3000)
     xyz = np.stack([t * 100 + 50, t * 100 + 50, rng.integers(0, 1000, 3000)], 1).astype(np.int32)
     _check(eng, oracle, 200, 200, 100, xyz, raster=(-4, -4, 204, 204))
+
+
+@pytest.mark.parametrize("raster", [(20, 15, 90, 60), (130, -40, 190, 10), (-60, 50, -5, 140)])
+def test_rasters_that_do_not_cover_the_grid(eng, oracle, raster):
+    # a raster inside the grid, and rasters beside it (cells take only the
+    # discs that reach them; the rest are NODATA)
+    rng = np.random.default_rng(sum(raster) & 0xFFFF)
+    n = 6000 if raster[0] >= 0 and raster[2] <= 120 else 40     # sparse sites: discs reach the grid
+    xyz = np.stack([rng.integers(-8000, 22000, n), rng.integers(-6000, 16000, n),
+                    rng.integers(0, 3000, n)], 1).astype(np.int32)
+    ref = _check(eng, oracle, 120, 100, 100, xyz, raster=raster)
+    nod = (ref["h"] == np.float32(-9999.0)).mean()
+    assert 0.0 < nod < 1.0
