@@ -118,3 +118,19 @@ def test_spacetime_device_buffers_equal_host_buffers(eng):
                                          stream=torch.cuda.current_stream().cuda_stream, stats=stats)
         h = d_h.cpu().numpy().reshape(160, 160)
         assert np.array_equal(h.view(np.uint32), h_host.view(np.uint32))
+
+
+def test_spacetime_largest_time_radius(eng, oracle):
+    # time radius 16: 33 slices over 65 time values (the largest parameter
+    # block and batch of the space-time path)
+    from terranni_b200 import engine
+    rng = np.random.default_rng(16)
+    n = 5000
+    xyz = np.stack([rng.integers(0, 4800, n), rng.integers(0, 4000, n), rng.integers(0, 9000, n)], 1).astype(np.int32)
+    t = rng.integers(-40, 41, n).astype(np.int32)
+    wp_o = oracle.make_wp(48, 40, 100, raster=(-2, -2, 50, 42))
+    wp_e = engine.make_wp(48, 40, 100, raster=(-2, -2, 50, 42))
+    ref = oracle.interpolate_spacetime(wp_o, xyz, t, 0, 16, 25)
+    h, st = eng.interpolate_spacetime(wp_e, xyz, t, 0, 16, 25)
+    assert np.array_equal(h.view(np.uint32), ref["h"].view(np.uint32))
+    assert st.n_pixels == 33 * 52 * 44
