@@ -156,13 +156,21 @@ dnni_status dnni_interpolate_segment_device(dnni_ctx *ctx, const dnni_workpackag
  * box), right after the bounding-box pass.
  *
  * Runs on the calling thread's current device and queues on `stream`
- * (a cudaStream_t, NULL = the legacy default stream); it waits once, for the
- * bounding box, and returns with the rest queued.  The first call on each
- * device looks up the array's device address; make that first call before
- * any stream capture.  Every call shares the one array and overwrites what
- * the previous call left in it (what must start at zero is cleared on each
- * call), so calls whose work overlaps on the GPU race: serialise them, e.g.
- * on one stream. */
+ * (a cudaStream_t, NULL = the legacy default stream).  With n > 0 it waits
+ * on `stream` once, for the points' bounding box (the search bins are sized
+ * from it), and returns with the rest queued.  A point beyond +-2^30 LAS
+ * units of the origin returns DNNI_E_RANGE after that wait; the bin-grid
+ * check that the other calls report is not read back here, because a grid
+ * planned from the measured bounding box holds every point.
+ *
+ * The first call on each device looks up the array's device address, with
+ * that device current, and keeps it for the life of the process; make that
+ * first call before any stream capture.  The address does not survive
+ * cudaDeviceReset: after resetting a device, do not use this entry point on
+ * it again in the same process.  Every call shares the one array and
+ * overwrites what the previous call left in it (what must start at zero is
+ * cleared on each call), so calls whose work overlaps on the GPU race:
+ * serialise them, e.g. on one stream. */
 dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpackage *wp, const int32_t *d_xyz,
                                                     const uint32_t *d_gid, int64_t n, float *d_h,
                                                     uint32_t *d_site, void *stream);

@@ -421,19 +421,31 @@ int orc_work_stats(const orc_wp *wp, const int32_t *r2, int64_t out[3]) {
 /* reference depth-buffer emulation (float32 lifted planes)             */
 /* ------------------------------------------------------------------ */
 
-/* Depth of the lifted plane of site (sx, sy) at pixel centre (px, py), all in
- * work-package-local metres, evaluated with the float arithmetic of
- * nni.cpp:186-216 (halfwidth from wp.nrows, a/b/z_offset in float).  The
- * rasteriser interpolates the plane between the square's vertices; evaluating
- * the same plane at the pixel centre is the approximation made here. */
-static inline float plane_depth(float hw, float sx, float sy, float px, float py) {
-    float zpx = (sx + hw) / hw;
-    float zpy = (sy + hw) / hw;
-    float zoff = zpx * zpx + zpy * zpy;
-    float a = -2.0f * zpx / hw;
-    float b = -2.0f * zpy / hw;
+/* The lifted plane of a site (or query) whose offset from the work-package
+ * origin is (dx, dy) metres, as drawPlane forms it (nni.cpp:186-200): the
+ * offset stays in double (site.p - x_offset), zpx = (dx + halfwidth) /
+ * halfwidth and the slopes a = -2.0 * zpx / halfwidth are evaluated in
+ * double and rounded to float once each, and z_offset is the float sum of
+ * the float squares (the time term is zero in 2-D). */
+typedef struct { float a, b, zoff; } orc_plane;
+
+static inline orc_plane plane_of(float hw, double dx, double dy) {
+    orc_plane P;
+    float zpx = (float)((dx + (double)hw) / (double)hw);
+    float zpy = (float)((dy + (double)hw) / (double)hw);
+    P.zoff = zpx * zpx + zpy * zpy;
+    P.a = (float)((-2.0 * (double)zpx) / (double)hw);
+    P.b = (float)((-2.0 * (double)zpy) / (double)hw);
+    return P;
+}
+
+/* Depth of a plane at a pixel centre (px, py), in float as the vertex depths
+ * of nni.cpp:208-216 are formed.  The rasteriser interpolates the plane
+ * between the square's vertices; evaluating the same plane at the pixel
+ * centre is the approximation made here. */
+static inline float plane_depth(const orc_plane *P, float hw, float px, float py) {
     float zx = px + hw, zy = py + hw;
-    return a * zx + b * zy + zoff;
+    return P->a * zx + P->b * zy + P->zoff;
 }
 
 /* optional quantisation to an unsigned fixed-point depth buffer of `bits` bits
@@ -510,9 +522,9 @@ int orc_gl_disagreement(const orc_wp *wp, const int32_t *xyz, const uint32_t *gi
             }
             for (int64_t c = 0; c < nc; c++) {
                 const orc_pt *s = &t.p[cand[c]];
-                float sx = (float)((double)(s->x - wp->origin_x) * xy_scale);
-                float sy = (float)((double)(s->y - wp->origin_y) * xy_scale);
-                double d = quant_depth(plane_depth(hw, sx, sy, px, py), depth_bits);
+                const orc_plane P = plane_of(hw, (double)(s->x - wp->origin_x) * xy_scale,
+                                             (double)(s->y - wp->origin_y) * xy_scale);
+                double d = quant_depth(plane_depth(&P, hw, px, py), depth_bits);
                 if (!have || d <= bestd) { bestd = d; bg = s->gid; bz = s->z; have = 1; }
             }
             out[0]++;
@@ -583,8 +595,9 @@ int orc_compat(const orc_compat_settings *s, const orc_compat_wp *wp, const doub
     double rs = s->site_radius / sqrt(2.0);
     /* site step */
     for (int64_t k = 0; k < n; k++) {
-        float sx = (float)(pts[3 * k] - wp->origin_x);
-        float sy = (float)(pts[3 * k + 1] - wp->origin_y);
+        double dx = pts[3 * k] - (double)wp->origin_x, dy = pts[3 * k + 1] - (double)wp->origin_y;
+        float sx = (float)dx, sy = (float)dy;
+        const orc_plane P = plane_of(hw, dx, dy);
         uint32_t zc = (uint32_t)floor((pts[3 * k + 2] + zOffset + 1) * zMult);
         float x0 = (float)(sx - rs), x1 = (float)(sx + rs), y0 = (float)(sy - rs), y1 = (float)(sy + rs);
         int64_t i0 = (int64_t)ceil((x0 - left) / pixel_size - 0.5), i1 = (int64_t)ceil((x1 - left) / pixel_size - 0.5) - 1;
@@ -597,7 +610,7 @@ int orc_compat(const orc_compat_settings *s, const orc_compat_wp *wp, const doub
             for (int64_t pi = i0; pi <= i1; pi++) {
                 float cx = (float)(left + (pi + 0.5) * pixel_size);
                 float cy = (float)(bottom + (pj + 0.5) * pixel_size);
-                float d = plane_depth(hw, sx, sy, cx, cy);
+                float d = plane_depth(&P, hw, cx, cy);
                 if (d <= dep[pj * xp + pi]) { dep[pj * xp + pi] = d; col[pj * xp + pi] = zc; }
             }
     }
@@ -606,6 +619,7 @@ int orc_compat(const orc_compat_settings *s, const orc_compat_wp *wp, const doub
     for (int64_t j = 0; j < wp->nrows; j++)
         for (int64_t i = 0; i < wp->ncols; i++) {
             float qx = (float)(i * query_spacing), qy = (float)(j * query_spacing);
+            const orc_plane Q = plane_of(hw, i * query_spacing, j * query_spacing);
             float x0 = (float)(qx - rq), x1 = (float)(qx + rq), y0 = (float)(qy - rq), y1 = (float)(qy + rq);
             int64_t i0 = (int64_t)ceil((x0 - left) / pixel_size - 0.5), i1 = (int64_t)ceil((x1 - left) / pixel_size - 0.5) - 1;
             int64_t j0 = (int64_t)ceil((y0 - bottom) / pixel_size - 0.5), j1 = (int64_t)ceil((y1 - bottom) / pixel_size - 0.5) - 1;
@@ -619,7 +633,7 @@ int orc_compat(const orc_compat_settings *s, const orc_compat_wp *wp, const doub
                     if (zc == 0) continue;                       /* cuda_nni.cu:423 */
                     float cx = (float)(left + (pi + 0.5) * pixel_size);
                     float cy = (float)(bottom + (pj + 0.5) * pixel_size);
-                    float d = plane_depth(hw, qx, qy, cx, cy);
+                    float d = plane_depth(&Q, hw, cx, cy);
                     if (d <= dep[pj * xp + pi]) {
                         int64_t w = j * wp->ncols + i;
                         numer[w] = (int32_t)((uint32_t)numer[w] + zc);   /* int32 wrap as atomicAdd */

@@ -29,18 +29,24 @@ struct CompatGeom {
 };
 
 // A site's (or query's) lifted plane: its slopes and offset depend on the
-// point only, so they are formed once per point (drawPlane, nni.cpp:186-212).
+// point only, so they are formed once per point, as drawPlane forms them
+// (nni.cpp:186-200): the point's offset (dx, dy) from the work-package
+// origin stays in double, zpx = (dx + halfwidth) / halfwidth and the slopes
+// a = -2.0 * zpx / halfwidth are evaluated in double and rounded to float
+// once each, and the offset is the float sum of the float squares (the time
+// term is zero in 2-D).
 struct CompatPlane {
     float a, b, zoff;
 };
 
-__device__ __forceinline__ CompatPlane compat_plane(float hw, float sx, float sy) {
-    const float zpx = __fdiv_rn(__fadd_rn(sx, hw), hw);
-    const float zpy = __fdiv_rn(__fadd_rn(sy, hw), hw);
+__device__ __forceinline__ CompatPlane compat_plane(float hw, double dx, double dy) {
+    const double h = (double)hw;
+    const float zpx = __double2float_rn(__ddiv_rn(__dadd_rn(dx, h), h));
+    const float zpy = __double2float_rn(__ddiv_rn(__dadd_rn(dy, h), h));
     CompatPlane P;
     P.zoff = __fadd_rn(__fmul_rn(zpx, zpx), __fmul_rn(zpy, zpy));
-    P.a = __fdiv_rn(__fmul_rn(-2.0f, zpx), hw);
-    P.b = __fdiv_rn(__fmul_rn(-2.0f, zpy), hw);
+    P.a = __double2float_rn(__ddiv_rn(__dmul_rn(-2.0, (double)zpx), h));
+    P.b = __double2float_rn(__ddiv_rn(__dmul_rn(-2.0, (double)zpy), h));
     return P;
 }
 
@@ -72,18 +78,22 @@ __device__ __forceinline__ float compat_unorder(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
 }
 
-// A point's square of site influence: its position relative to the work
-// package (float, as drawPlane has it) and the pixels [i0,i1] x [j0,j1]
-// whose centres the square covers (empty when i0 > i1 or j0 > j1).
+// A point's square of site influence: its offset from the work package
+// (double, and rounded to float as drawPlane's px, py) and the pixels
+// [i0,i1] x [j0,j1] whose centres the square covers (empty when i0 > i1 or
+// j0 > j1).
 struct CompatSquare {
+    double dx, dy;
     float sx, sy;
     long long i0, i1, j0, j1;
 };
 
 __device__ __forceinline__ CompatSquare compat_square(const CompatGeom& G, const double* __restrict__ xyz, int64_t k) {
     CompatSquare q;
-    q.sx = __double2float_rn(__dsub_rn(xyz[3 * k], (double)G.ox));
-    q.sy = __double2float_rn(__dsub_rn(xyz[3 * k + 1], (double)G.oy));
+    q.dx = __dsub_rn(xyz[3 * k], (double)G.ox);
+    q.dy = __dsub_rn(xyz[3 * k + 1], (double)G.oy);
+    q.sx = __double2float_rn(q.dx);
+    q.sy = __double2float_rn(q.dy);
     const float x0 = __double2float_rn(__dsub_rn((double)q.sx, G.rs)), x1 = __double2float_rn(__dadd_rn((double)q.sx, G.rs));
     const float y0 = __double2float_rn(__dsub_rn((double)q.sy, G.rs)), y1 = __double2float_rn(__dadd_rn((double)q.sy, G.rs));
     compat_span(x0, x1, G.left, G.pixel_size, G.xp, q.i0, q.i1);
@@ -173,7 +183,7 @@ __global__ void __launch_bounds__(256) k_compat_sites(CompatGeom G, const double
         const long long i0 = max(q.i0, px0), i1 = min(q.i1, px0 + pw - 1);
         const long long j0 = max(q.j0, py0), j1 = min(q.j1, py0 + ph - 1);
         const unsigned long long low = 0xFFFFFFFFull - (unsigned long long)k;
-        const CompatPlane P = compat_plane(G.hw, q.sx, q.sy);
+        const CompatPlane P = compat_plane(G.hw, q.dx, q.dy);
         for (long long pj = j0; pj <= j1; ++pj) {
             const float cy = compat_centre(pj, G.bottom, G.pixel_size);
             for (long long pi = i0; pi <= i1; ++pi) {
@@ -204,8 +214,9 @@ __global__ void __launch_bounds__(256) k_compat_cells(CompatGeom G, const double
     const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (w >= (int64_t)G.ncols * G.nrows) return;
     const int i = (int)(w % G.ncols), j = (int)(w / G.ncols);
-    const float qx = __double2float_rn(__dmul_rn((double)i, G.qspacing));
-    const float qy = __double2float_rn(__dmul_rn((double)j, G.qspacing));
+    const double qdx = __dmul_rn((double)i, G.qspacing), qdy = __dmul_rn((double)j, G.qspacing);
+    const float qx = __double2float_rn(qdx);
+    const float qy = __double2float_rn(qdy);
     const float x0 = __double2float_rn(__dsub_rn((double)qx, G.rq)), x1 = __double2float_rn(__dadd_rn((double)qx, G.rq));
     const float y0 = __double2float_rn(__dsub_rn((double)qy, G.rq)), y1 = __double2float_rn(__dadd_rn((double)qy, G.rq));
     long long i0, i1, j0, j1;
@@ -213,7 +224,7 @@ __global__ void __launch_bounds__(256) k_compat_cells(CompatGeom G, const double
     compat_span(y0, y1, G.bottom, G.pixel_size, G.yp, j0, j1);
     uint32_t numer = 0;
     int32_t denom = 0;
-    const CompatPlane Q = compat_plane(G.hw, qx, qy);
+    const CompatPlane Q = compat_plane(G.hw, qdx, qdy);
     for (long long pj = j0; pj <= j1; ++pj) {
         const float cy = compat_centre(pj, G.bottom, G.pixel_size);
         for (long long pi = i0; pi <= i1; ++pi) {

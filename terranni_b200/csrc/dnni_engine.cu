@@ -1055,7 +1055,9 @@ unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
 // In host code g_noalloc_scratch is only a host-side stand-in for the array,
 // not a device address: a kernel given it would fault or, where the GPU can
 // reach host memory, silently use the wrong memory.  The device address is
-// looked up once per device, with that device current, on the first call.
+// looked up once per device, with that device current, on the first call,
+// and kept for the life of the process (a cudaDeviceReset of the device
+// would leave it stale; the header tells callers not to mix the two).
 dnni_status noalloc_base(int dev, unsigned char** out) {
     if (dev < 0 || dev >= kNoAllocMaxDevices) return DNNI_E_INVAL;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -1154,8 +1156,7 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
         batch_add(hb, t, 0, 0, d_site ? 0 : -1);
         if (!carve_noalloc(base, scratch_sizes(hb), a)) return DNNI_E_SCRATCH;
         pack_tables(hb, tbl.data());
-        if (cudaMemcpyAsync(a.tables, tbl.data(), tbl.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess)
+        if (cudaMemcpyAsync(a.tables, tbl.data(), tbl.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
             return DNNI_E_CUDA;
         bt = device_tables(a.tables, 1);
     }

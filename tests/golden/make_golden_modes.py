@@ -10,6 +10,7 @@ Run:  python tests/golden/make_golden_modes.py
 """
 from __future__ import annotations
 
+import math
 import os
 import sys
 
@@ -26,7 +27,6 @@ OUT = os.path.join(HERE, "golden_modes.npz")
 
 def z_multiplier(sr, scale, cell, zmax, pmin):
     # terranni.cpp:675-684
-    import math
     pw = int(math.ceil(2.0 * sr * scale / cell))
     max_sum = pw * pw * (zmax - pmin)
     m = 1
@@ -55,6 +55,36 @@ def main():
         out[p + "params"] = np.array([scale, cell, sr, qr, pmin, mult, origin[0], origin[1], nrows, ncols],
                                      np.float64)
         out[p + "pts"], out[p + "h"], out[p + "res"] = pts, h, res
+    # near-ties: pairs of sites mirrored about pixel centres, at UTM-scale
+    # origins, where the depth test is decided by the last bits of the planes;
+    # with drawPlane's double-then-round slopes (nni.cpp:194-200) the kept
+    # site differs in some cells from a rule that rounds the site offset to
+    # float first
+    for m, seed in enumerate((6, 8)):
+        k = len(compat_cases) + m
+        rng = np.random.default_rng(seed)
+        scale, cell, sr, qr, pmin, ncols, nrows = 1, 1.0, 3.0, 2.5, 0, 5, 5
+        origin = (500000.0 + float(rng.integers(0, 1000)) + 0.25, 4100000.0 + float(rng.integers(0, 1000)) + 0.5)
+        ps = cell / scale
+        po = math.ceil((float(np.float32(qr)) - math.floor(scale / 2.0) * ps) / ps) + 1
+        left = 0 - cell / 2.0 - po * ps
+        pts = []
+        for _ in range(12):
+            pi = int(rng.integers(0, ncols * scale + 2 * po))
+            pj = int(rng.integers(0, nrows * scale + 2 * po))
+            cx, cy = left + (pi + 0.5) * ps, left + (pj + 0.5) * ps
+            d, ang = rng.uniform(0.2, 0.6), rng.uniform(0, math.pi)
+            ex, ey = d * math.cos(ang), d * math.sin(ang)
+            z1, z2 = rng.uniform(10, 40, 2)
+            pts.append((origin[0] + cx + ex, origin[1] + cy + ey, z1))
+            pts.append((origin[0] + cx - ex, origin[1] + cy - ey, z2))
+        pts = np.array(pts)
+        mult = 1000
+        h, res = compat_restated(scale, cell, sr, qr, pmin, mult, origin[0], origin[1], nrows, ncols, pts)
+        p = f"compat{k}_"
+        out[p + "params"] = np.array([scale, cell, sr, qr, pmin, mult, origin[0], origin[1], nrows, ncols],
+                                     np.float64)
+        out[p + "pts"], out[p + "h"], out[p + "res"] = pts, h, res
     st_cases = [
         (8, 6, 100, (-2, -1, 10, 8), 5, 1, 100, 40),
         (7, 7, 50, (0, 0, 7, 7), -2, 2, 40, 36),
@@ -71,7 +101,7 @@ def main():
         p = f"st{k}_"
         out[p + "params"] = np.array([ncols, nrows, cs, *raster, cur, rt, tau], np.int64)
         out[p + "xyz"], out[p + "t"], out[p + "Z"], out[p + "C"], out[p + "h"] = xyz, t, Z, C, h
-    out["n_compat"] = np.array([len(compat_cases)])
+    out["n_compat"] = np.array([len(compat_cases) + 2])
     out["n_st"] = np.array([len(st_cases)])
     np.savez_compressed(OUT, **out)
     print("wrote", OUT)

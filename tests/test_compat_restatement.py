@@ -14,12 +14,21 @@ import pytest
 F = np.float32
 
 
-def _depth(hw, sx, sy, px, py):
-    zpx = (sx + hw) / hw
-    zpy = (sy + hw) / hw
+def _plane(hw, dx, dy):
+    """drawPlane's slopes and offset (nni.cpp:186-200): zpx, zpy, a and b
+    are formed in double from the double site offset and rounded to float
+    once each; the offset is a float sum of float squares."""
+    h = float(hw)
+    zpx = F((dx + h) / h)
+    zpy = F((dy + h) / h)
     zoff = zpx * zpx + zpy * zpy
-    a = (F(-2.0) * zpx) / hw
-    b = (F(-2.0) * zpy) / hw
+    a = F((-2.0 * float(zpx)) / h)
+    b = F((-2.0 * float(zpy)) / h)
+    return a, b, zoff
+
+
+def _depth(hw, plane, px, py):
+    a, b, zoff = plane
     zx, zy = px + hw, py + hw
     return (a * zx + b * zy) + zoff
 
@@ -45,13 +54,15 @@ def compat_restated(scale, cell, sr, qr_d, pmin, mult, ox, oy, nrows, ncols, pts
     cx = [F(left + (p + 0.5) * ps) for p in range(xp)]
     cy = [F(left + (p + 0.5) * ps) for p in range(yp)]
     for x, y, z in pts:                                   # draw order: later equal depths win
-        sx, sy = F(x - float(F(ox))), F(y - float(F(oy)))
+        dx, dy = x - float(F(ox)), y - float(F(oy))
+        sx, sy = F(dx), F(dy)
+        plane = _plane(hw, dx, dy)
         zc = np.uint32(int(math.floor(((z + zoffset) + 1) * mult)))
         i0, i1 = _span(F(float(sx) - rs), F(float(sx) + rs), left, ps, xp)
         j0, j1 = _span(F(float(sy) - rs), F(float(sy) + rs), left, ps, yp)
         for pj in range(j0, j1 + 1):
             for pi in range(i0, i1 + 1):
-                d = _depth(hw, sx, sy, cx[pi], cy[pj])
+                d = _depth(hw, plane, cx[pi], cy[pj])
                 if d <= dep[pj, pi]:
                     dep[pj, pi] = d
                     col[pj, pi] = zc
@@ -61,6 +72,7 @@ def compat_restated(scale, cell, sr, qr_d, pmin, mult, ox, oy, nrows, ncols, pts
     for j in range(nrows):
         for i in range(ncols):
             qx, qy = F(i * qs), F(j * qs)
+            qplane = _plane(hw, i * qs, j * qs)
             i0, i1 = _span(F(float(qx) - rq), F(float(qx) + rq), left, ps, xp)
             j0, j1 = _span(F(float(qy) - rq), F(float(qy) + rq), left, ps, yp)
             numer, denom = 0, 0
@@ -68,7 +80,7 @@ def compat_restated(scale, cell, sr, qr_d, pmin, mult, ox, oy, nrows, ncols, pts
                 for pi in range(i0, i1 + 1):
                     if col[pj, pi] == 0:
                         continue
-                    if _depth(hw, qx, qy, cx[pi], cy[pj]) <= dep[pj, pi]:
+                    if _depth(hw, qplane, cx[pi], cy[pj]) <= dep[pj, pi]:
                         numer = (numer + int(col[pj, pi])) & 0xFFFFFFFF       # int32 sum with wrap
                         denom += 1
             if denom == 0:
