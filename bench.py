@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small-radius", type=int, default=0)
     ap.add_argument("--bin-target", type=int, default=0)
+    ap.add_argument("--span-window", type=int, default=0,
+                    help="64-bit words of shared memory per raster tile for the span window (0 = default)")
     ap.add_argument("--no-autotune", action="store_true", help="mixed: skip the autotuner (context defaults)")
     ap.add_argument("--tune-sample", type=int, default=256, help="mixed: tiles the autotuner times")
     return ap.parse_args()
@@ -504,7 +506,7 @@ def run_engine_mixed(args, world, rank, local):
     d_h = torch.empty(max(nout, 1), dtype=torch.float32, device="cuda")
     stream = torch.cuda.Stream()           # the engine launches on exactly this stream
     sp = stream.cuda_stream
-    opts = dict(small_radius=args.small_radius, bin_target=args.bin_target)
+    opts = dict(small_radius=args.small_radius, bin_target=args.bin_target, span_window=args.span_window)
     tune = None
     if not args.no_autotune:              # outside the timed region
         t0 = time.perf_counter()
@@ -609,6 +611,7 @@ def run_engine_mixed(args, world, rank, local):
                        "side_max": int(sides.max()),
                        "form": "batched: all tiles in one CUDA-graph launch sequence per step",
                        "small_radius": opts["small_radius"] or 3, "bin_target": opts["bin_target"] or 4,
+                       "span_window": opts["span_window"] or 8192,
                        "order_by_cost": True, "autotune": tune,
                        "l2": f"inputs larger than L2 ({xyz.nbytes / 1e9:.1f} GB points per step)",
                        "parallelism": f"dp{world} (independent tiles)"},

@@ -100,6 +100,12 @@ typedef struct dnni_stats {
     int32_t packed;         /* 1 when (Z,C) shared one 64-bit accumulator */
     int32_t bin_size;       /* search-bin edge chosen, LAS units */
     int32_t pad;
+    int64_t evals_dense;    /* candidate distance evaluations of the ring search */
+    int64_t evals_far;      /* and of the far pass (seeds and disc search) */
+    int64_t span_hist[16];  /* spans per radius bucket: bucket k holds the
+                               span-path pixels with floor(sqrt(R2)) in
+                               [2^(k-1), 2^k) (k = 15: all larger); filled
+                               by statistics runs without a graph */
 } dnni_stats;
 
 /* ---- lifecycle: nni::init / nni::cleanup (nni.h:83-85, nni.cpp:563-598) ---- */
@@ -204,6 +210,12 @@ typedef struct dnni_batch_options {
     int32_t bin_target;            /* 0 = the context's setting */
     int32_t use_graph;             /* capture the launch sequence in a CUDA graph */
     int32_t order_by_cost;         /* schedule the largest tiles first */
+    int32_t span_window;           /* 64-bit words of shared memory per raster
+                                      tile in which the span path merges its
+                                      markers (256..26624); 0 = default (8192) */
+    int32_t far_group;             /* pixels the far pass searches together:
+                                      1 = 32 x 1 rows, 2 = 8 x 4 blocks;
+                                      0 = default (2) */
 } dnni_batch_options;
 
 /* Plans the tiles and allocates the batch's device scratch (allocates). */
@@ -350,7 +362,7 @@ dnni_status dnni_server_destroy(dnni_server *srv);
 typedef struct dnni_tune_trial {
     int32_t small_radius, bin_target;
     float ms;                          /* device time of one run of the sample */
-    int32_t pad;
+    int32_t span_window;
 } dnni_tune_trial;
 
 typedef struct dnni_tune_report {

@@ -137,6 +137,8 @@ void set_dense_smem_attr() {
     std::lock_guard<std::mutex> lock(mu);
     if (dev >= 0 && dev < 64 && !done[dev]) {
         cudaFuncSetAttribute(k_near_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmem);
+        cudaFuncSetAttribute(k_scatter_window, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(unsigned long long) * kSpanWindowMaxWords));
         done[dev] = true;
     }
 }
@@ -177,7 +179,8 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     }
     if (ev) cudaEventRecord(ev[0], st);
     const int nrt = hb.rt_base.back();
-    k_near_dense<<<nrt, dim3(32, 8), kDenseSmem, st>>>(bt, a.sorted, a.start, a.pix, d_site, a.far, a.sc, a.ctr);
+    k_near_dense<<<nrt, dim3(32, 8), kDenseSmem, st>>>(bt, a.sorted, a.start, a.pix, d_site, a.far, a.sc, a.ctr,
+                                                       hb.far_blocks);
     if (nchunk > 0)
         k_near_far<<<sms * 6, 256, 0, st>>>(bt, a.sorted, a.start, a.bmask, a.smask, a.near, a.far, a.pix, d_site,
                                             a.sc, a.ctr);
@@ -186,7 +189,8 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     if (ev) cudaEventRecord(ev[1], st);
     cudaMemsetAsync(a.D, 0, sizeof(unsigned long long) * hb.n_cells, st);
     cudaMemsetAsync(a.Dc, 0, sizeof(int) * hb.n_cells, st);
-    k_scatter_spans<<<nrt, dim3(32, 8), 0, st>>>(bt, a.pix, a.sc, a.D, a.Dc);
+    k_scatter_window<<<nrt, dim3(32, 8), sizeof(unsigned long long) * hb.win_words, st>>>(bt, a.pix, a.sc, a.D,
+                                                                                         a.Dc, hb.win_words);
     if (ev) cudaEventRecord(ev[2], st);
     const int ngrow = hb.grow_base.back();
     k_rowscan<<<ngrow, kScanThreads, 0, st>>>(bt, a.D, a.Dc, a.sc);
@@ -195,20 +199,26 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
 
 // Sums the per-tile scalars into dnni_stats.
 void fold_stats(const Scalars* s, int n, dnni_stats* st) {
-    int64_t big = 0, sp = 0, nod = 0;
+    int64_t big = 0, sp = 0, nod = 0, evd = 0, evf = 0;
     int mx = -1, packed = 1;
+    for (int k = 0; k < kSpanHistBuckets; ++k) st->span_hist[k] = 0;
     for (int t = 0; t < n; ++t) {
         for (int k = 0; k < kStatSlots; ++k) {
             big += (int64_t)s[t].big_pixels[k];
             sp += (int64_t)s[t].spans[k];
             nod += (int64_t)s[t].nodata[k];
+            evd += (int64_t)s[t].evals_dense[k];
+            evf += (int64_t)s[t].evals_far[k];
             mx = std::max(mx, s[t].max_r2[k]);
         }
+        for (int k = 0; k < kSpanHistBuckets; ++k) st->span_hist[k] += (int64_t)s[t].span_hist[k];
         packed &= s[t].packed;
     }
     st->big_pixels = big;
     st->spans = sp;
     st->nodata_cells = nod;
+    st->evals_dense = evd;
+    st->evals_far = evf;
     st->max_r2 = mx;
     st->packed = packed;
 }
@@ -312,6 +322,7 @@ static dnni_status run_device(dnni_ctx* c, const dnni_workpackage* wp, const int
     launch_body(hb, bt, a, d_xyz, d_gid, d_h, d_site, c->sm_count, st, timing ? &c->ev[1] : nullptr);
     CK(cudaGetLastError());
     if (timing) CK(cudaEventRecord(c->ev[4], st));
+    if (stats) k_span_hist<<<hb.rt_base.back(), dim3(32, 8), 0, st>>>(bt, a.pix, a.sc);
     c->calls++;
     if (timing) {
         CK(cudaEventSynchronize(c->ev[4]));
@@ -346,7 +357,11 @@ static dnni_status plan_batch(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
                               HostBatch& hb, std::vector<int>& order) {
     const int rs_ = o.small_radius ? o.small_radius : c->s.small_radius;
     const int bt_ = o.bin_target ? o.bin_target : c->s.bin_target;
-    if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0) return set_err(c, DNNI_E_INVAL, "bad batch options");
+    const int ww_ = o.span_window ? o.span_window : kSpanWindowWords;
+    if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0 || ww_ < 256 || ww_ > kSpanWindowMaxWords || o.far_group < 0 ||
+        o.far_group > 2)
+        return set_err(c, DNNI_E_INVAL, "bad batch options");
+    const int fb_ = o.far_group ? o.far_group - 1 : kFarBlocksDefault;
     std::vector<TileParams> plan(ntiles);
     std::vector<int64_t> cost(ntiles);
     for (int k = 0; k < ntiles; ++k) {
@@ -383,6 +398,8 @@ static dnni_status plan_batch(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
     if (o.order_by_cost) std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
     hb = HostBatch();
     hb.rs = rs_;
+    hb.win_words = ww_;
+    hb.far_blocks = fb_;
     for (int k : order) batch_add(hb, plan[k], tiles[k].pt_offset, tiles[k].out_offset, tiles[k].site_offset);
     if (hb.too_big) return set_err(c, DNNI_E_INVAL, "batch too large for one launch sequence: split it");
     return DNNI_OK;
@@ -628,6 +645,7 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
     }
     if (stats) {
         CK(cudaEventRecord(c->ev[4], st));
+        if (!b->use_graph) k_span_hist<<<b->hb.rt_base.back(), dim3(32, 8), 0, st>>>(b->bt, b->arr.pix, b->arr.sc);
         const int n = (int)b->hb.tiles.size();
         CK(cudaMemcpyAsync(b->h_sc.data(), b->arr.sc, sizeof(Scalars) * n, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(c->h_ctr, b->arr.ctr, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
@@ -947,10 +965,11 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     std::vector<int> order;
     std::vector<dnni_tune_trial> trials;
     cudaStream_t st = c->stream;
-    auto trial = [&](int rs_, int bt_, float* ms) -> dnni_status {
+    auto trial = [&](int rs_, int bt_, int ww_, float* ms) -> dnni_status {
         dnni_batch_options o = given;
         o.small_radius = rs_;
         o.bin_target = bt_;
+        o.span_window = ww_;
         dnni_status rs = plan_batch(c, smp.data(), m, o, hb, order);
         if (rs) return rs;
         if ((rs = ensure_scratch(c, tscr, scratch_sizes(hb), a))) return rs;
@@ -967,36 +986,46 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
         float t = 0;
         CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
         *ms = t / 2;
-        trials.push_back(dnni_tune_trial{rs_, bt_, *ms, 0});
+        trials.push_back(dnni_tune_trial{rs_, bt_, *ms, ww_});
         return DNNI_OK;
     };
     dnni_status rs = dnni_ensure(c, hbuf, sizeof(float) * std::max<int64_t>(out, 1));
     const int rs0 = given.small_radius ? given.small_radius : c->s.small_radius;
     const int bt0 = given.bin_target ? given.bin_target : (c->s.bin_target ? c->s.bin_target : 4);
+    const int ww0 = given.span_window ? given.span_window : kSpanWindowWords;
     float ms_default = 0, best_ms = 0;
-    int best_rs = rs0, best_bt = bt0;
-    if (!rs) rs = trial(rs0, bt0, &ms_default);
+    int best_rs = rs0, best_bt = bt0, best_ww = ww0;
+    if (!rs) rs = trial(rs0, bt0, ww0, &ms_default);
     best_ms = ms_default;
-    // coordinate search: the bin size first, then the stencil/span split
+    // coordinate search: the bin size first, then the stencil/span split,
+    // then the span path's shared-memory window
     static const int kBinTargets[] = {2, 3, 4, 6, 8, 12};
     static const int kRadii[] = {1, 2, 3, 4, 5, 6};
+    static const int kWindows[] = {4096, 8192, 12288, 18432, 26624};
     for (int bt_ : kBinTargets) {
         if (rs || bt_ == bt0) continue;
         float ms = 0;
-        rs = trial(rs0, bt_, &ms);
+        rs = trial(rs0, bt_, ww0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_bt = bt_; }
     }
     for (int r_ : kRadii) {
         if (rs || r_ == rs0 || r_ > kMaxSmallRadius) continue;
         float ms = 0;
-        rs = trial(r_, best_bt, &ms);
+        rs = trial(r_, best_bt, ww0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_rs = r_; }
+    }
+    for (int w_ : kWindows) {
+        if (rs || w_ == ww0) continue;
+        float ms = 0;
+        rs = trial(best_rs, best_bt, w_, &ms);
+        if (!rs && ms < best_ms) { best_ms = ms; best_ww = w_; }
     }
     release_scratch(c, tscr);
     dnni_release(hbuf, c);
     if (rs) return rs;
     options->small_radius = best_rs;
     options->bin_target = best_bt;
+    options->span_window = best_ww;
     if (report) {
         memset(report, 0, sizeof(*report));
         report->ntrials = (int32_t)std::min<size_t>(trials.size(), 32);
@@ -1004,7 +1033,9 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
         report->ms_default = ms_default;
         for (int k = 0; k < report->ntrials; ++k) {
             report->trial[k] = trials[k];
-            if (trials[k].small_radius == best_rs && trials[k].bin_target == best_bt) report->best = k;
+            if (trials[k].small_radius == best_rs && trials[k].bin_target == best_bt &&
+                trials[k].span_window == best_ww)
+                report->best = k;
         }
     }
     return DNNI_OK;

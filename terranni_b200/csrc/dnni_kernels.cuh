@@ -88,7 +88,9 @@ __global__ void k_init_scalars(BatchTables bt, Scalars* sc, BatchCounters* ctr) 
     }
     if (l < kStatSlots) {
         s->max_r2[l] = -1; s->big_pixels[l] = 0; s->spans[l] = 0; s->nodata[l] = 0;
+        s->evals_dense[l] = 0; s->evals_far[l] = 0;
     }
+    if (l < kSpanHistBuckets) s->span_hist[l] = 0;
 }
 
 // Bounding box of each tile's points relative to its origin, with range checks
@@ -406,12 +408,17 @@ __device__ __forceinline__ void settle_pixel(const TileParams& T, int i, int j, 
     if (site && T.site_off >= 0) site[T.site_off + o] = b.gid;
 }
 
-__device__ __forceinline__ void warp_stats(const TileParams& T, int R2, Scalars* __restrict__ s, int slot) {
+// Per-warp statistics of settled pixels: span-path pixels and spans, the
+// largest R2, and the candidate distance evaluations made (nev per lane,
+// counted into evals_dense or evals_far).
+__device__ __forceinline__ void warp_stats(const TileParams& T, int R2, Scalars* __restrict__ s, int slot, int nev,
+                                           bool far_pass) {
     const int rs2 = T.rs * T.rs;
     const unsigned big = (R2 > rs2) ? 1u : 0u;
     const unsigned sp = big ? 2u * (unsigned)isqrt_i32(R2) + 1u : 0u;
     const unsigned nbig = __reduce_add_sync(0xffffffffu, big);
     const unsigned nsp = __reduce_add_sync(0xffffffffu, sp);
+    const unsigned nv = __reduce_add_sync(0xffffffffu, (unsigned)nev);
     const int mx = __reduce_max_sync(0xffffffffu, R2);
     if ((threadIdx.x & 31) == 0) {
         slot &= kStatSlots - 1;
@@ -419,6 +426,7 @@ __device__ __forceinline__ void warp_stats(const TileParams& T, int R2, Scalars*
             atomicAdd(&s->big_pixels[slot], (unsigned long long)nbig);
             atomicAdd(&s->spans[slot], (unsigned long long)nsp);
         }
+        if (nv) atomicAdd(far_pass ? &s->evals_far[slot] : &s->evals_dense[slot], (unsigned long long)nv);
         if (mx >= 0) atomicMax(&s->max_r2[slot], mx);
     }
 }
@@ -428,6 +436,11 @@ __device__ __forceinline__ void warp_stats(const TileParams& T, int R2, Scalars*
 struct FarSlot {
     int tile, pix, idx, pad;
 };
+
+// R2 of a pixel record that the ring search left unsettled (the far pass
+// overwrites it); real records hold R2 >= -1.
+constexpr int kPixFar = -2;
+constexpr int kFarBlocksDefault = 1;   // far groups of 8 x 4 pixels
 
 // Dense pass.  One CTA per 32 x kTileY raster tile of a work package
 // (blockDim 32 x 8; warp w takes pixel rows w, w + 8, ... of the tile): the
@@ -440,7 +453,8 @@ struct FarSlot {
 __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int4* __restrict__ pts_all,
                                                        const int* __restrict__ start_all, int2* __restrict__ pix,
                                                        uint32_t* __restrict__ site, FarSlot* __restrict__ far,
-                                                       Scalars* __restrict__ sc, BatchCounters* __restrict__ ctr) {
+                                                       Scalars* __restrict__ sc, BatchCounters* __restrict__ ctr,
+                                                       int far_blocks) {
     extern __shared__ int4 smem[];
     int4* s_pts = smem;
     int* s_lstart = (int*)(smem + kWinMaxPts);
@@ -548,7 +562,7 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
     const bool valid = i < T.rw && j < T.rh;
     int R2 = -1;
     bool far_pixel = false;
-    Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+    Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1, 0};
     if (valid) {
         if (T.npts > 0) {
             const int px = (T.rx0 + i) * T.cs, py = (T.ry0 + j) * T.cs;
@@ -572,19 +586,49 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
             if (site && T.site_off >= 0) site[T.site_off + o] = 0xFFFFFFFFu;
         }
     }
-    // worklist: a warp with any unsettled pixel appends its whole row of 32
-    // slots as one group (settled or absent pixels as empty slots), so that
-    // a far warp later takes 32 neighbouring pixels of one tile
-    const unsigned mfar = __ballot_sync(0xffffffffu, far_pixel);
-    if (mfar) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(&ctr->nfar, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        far[base + lane] = far_pixel ? FarSlot{t, j * T.rw + i, b.idx, 0} : FarSlot{t, -1, -1, 0};
+    if (far_blocks) {
+        // marked for the block pass below: the record holds the best site
+        // found so far (-1: none) and kPixFar
+        if (far_pixel) pix[T.pix_off + (int64_t)j * T.rw + i] = make_int2(b.idx, kPixFar);
+    } else {
+        // worklist: a warp with any unsettled pixel appends its whole row of
+        // 32 slots as one group (settled or absent pixels as empty slots), so
+        // that a far warp later takes 32 neighbouring pixels of one tile
+        const unsigned mfar = __ballot_sync(0xffffffffu, far_pixel);
+        if (mfar) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&ctr->nfar, 32);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            far[base + lane] = far_pixel ? FarSlot{t, j * T.rw + i, b.idx, 0} : FarSlot{t, -1, -1, 0};
+        }
     }
-    warp_stats(T, R2, sc + t, blockIdx.x + threadIdx.y + 8 * sub);
+    warp_stats(T, R2, sc + t, blockIdx.x + threadIdx.y + 8 * sub, b.nev, false);
     }
     __syncthreads();     // the next band restages the window
+    }
+    if (far_blocks) {
+        // worklist in 8 x 4 pixel blocks: a block with any unsettled pixel
+        // appends its 32 pixels as one group (lane = 8 * row + column), so
+        // that a far warp takes a compact patch whose discs overlap most;
+        // the records written above are visible after the barrier
+        __syncthreads();
+        for (int blk = warp; blk < (kTileX / 8) * (kTileY / 4); blk += 8) {
+            const int ii = i0 + (blk % (kTileX / 8)) * 8 + (lane & 7);
+            const int jj = j0 + (blk / (kTileX / 8)) * 4 + (lane >> 3);
+            bool fp = false;
+            int idx = -1;
+            if (ii < T.rw && jj < T.rh) {
+                const int2 r = pix[T.pix_off + (int64_t)jj * T.rw + ii];
+                fp = r.y == kPixFar;
+                idx = r.x;
+            }
+            if (__ballot_sync(0xffffffffu, fp)) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&ctr->nfar, 32);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                far[base + lane] = fp ? FarSlot{t, jj * T.rw + ii, idx, 0} : FarSlot{t, -1, -1, 0};
+            }
+        }
     }
 }
 
@@ -723,6 +767,7 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
                     qc &= qc - 1;
                     const int64_t id = (blk << 6) + l;
                     const int s0 = __ldg(&start[id]), e0 = __ldg(&start[id + 1]);
+                    if (act) b.nev += e0 - s0;
                     for (int q = s0; q < e0; ++q) {
                         const int4 p = __ldg(&pts[q]);
                         if (act) consider(b, p, q, px, py);
@@ -766,13 +811,16 @@ __global__ void __launch_bounds__(256, 4) k_near_far(BatchTables bt, const int4*
         const uint64_t* smask = smask_all + T.sup_off;
         const bool act = item.pix >= 0;
         int i = 0, j = 0, px = 0, py = 0;
-        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1};
+        Best b{LLONG_MAX, 0xFFFFFFFFu, INT_MAX, -1, 0};
         if (act) {
             i = item.pix % T.rw;
             j = item.pix / T.rw;
             px = (T.rx0 + i) * T.cs;
             py = (T.ry0 + j) * T.cs;
-            if (item.idx >= 0) consider(b, __ldg(&pts[item.idx]), item.idx, px, py);
+            if (item.idx >= 0) {
+                consider(b, __ldg(&pts[item.idx]), item.idx, px, py);
+                b.nev += 1;
+            }
             int bx = udiv32((long long)px - g.gx0, g.bs), by = udiv32((long long)py - g.gy0, g.bs);
             bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
             by = by < g.nby - 1 ? by : g.nby - 1;
@@ -786,7 +834,7 @@ __global__ void __launch_bounds__(256, 4) k_near_far(BatchTables bt, const int4*
             settle_pixel(T, i, j, b, pix, site);
             R2 = r2_of(b.d2, (long long)T.cs * T.cs, T.r2cap);
         }
-        warp_stats(T, R2, sc + t, blockIdx.x * 3 + (threadIdx.x >> 5));
+        warp_stats(T, R2, sc + t, blockIdx.x * 3 + (threadIdx.x >> 5), b.nev, true);
     }
 }
 
@@ -874,6 +922,179 @@ __global__ void __launch_bounds__(256) k_scatter_spans(BatchTables bt, const int
         }
     }
     }
+}
+
+// Span path through a shared-memory window.  The discs of one 32 x kTileY
+// raster tile cover a window of grid cells a little larger than the tile by
+// the largest radius; the window is processed in chunks of whole rows that
+// fit `win_words` 64-bit words of shared memory.  For each chunk every disc
+// of the tile adds its row spans' markers (+v at the first cell, -v after
+// the last: the per-row difference form of k_scatter_spans) to the chunk
+// with shared-memory atomics, and the chunk's non-zero words are then added
+// to the grid's difference array with one coalesced global atomic each.  The
+// markers of a tile's discs fall on far fewer distinct cells than there are
+// markers (neighbouring pixels' discs share rows and end near each other),
+// so the grid sees a fraction of the global atomics of the direct path, and
+// those it sees are contiguous.  The sum is the same: the words add modulo
+// 2^64 in any order and the packed form is linear.  Tiles with the unpacked
+// accumulators (separate int64 Z and int32 C), and windows wider than one
+// chunk row, take the direct path.
+constexpr int kSpanWindowWords = 8192;      // default: 64 KB per CTA, three CTAs per SM
+constexpr int kSpanWindowMaxWords = 26624;  // 208 KB, the most one CTA may take
+
+// Minimum (or maximum) of v over a 32 x 8 CTA; red: 8 ints of shared memory.
+template <bool kMax>
+__device__ __forceinline__ int block_reduce_int(int v, int* red) {
+    v = kMax ? __reduce_max_sync(0xffffffffu, v) : __reduce_min_sync(0xffffffffu, v);
+    if (threadIdx.x == 0) red[threadIdx.y] = v;
+    __syncthreads();
+    int r = red[0];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) r = kMax ? max(r, red[k]) : min(r, red[k]);
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const int2* __restrict__ pix,
+                                                        const Scalars* __restrict__ sc,
+                                                        unsigned long long* __restrict__ D_all,
+                                                        int* __restrict__ Dc_all, int win_words) {
+    extern __shared__ unsigned long long sw[];
+    __shared__ int red[8];
+    const int t = find_tile(bt.rt_base, bt.ntiles, blockIdx.x);
+    const TileParams& T = bt.tiles[t];
+    const int lt = blockIdx.x - __ldg(&bt.rt_base[t]);
+    const int ntx = (T.rw + kTileX - 1) / kTileX;
+    const int i = (lt % ntx) * kTileX + threadIdx.x;
+    const int jt = (lt / ntx) * kTileY + threadIdx.y;
+    const int rs2 = T.rs * T.rs;
+    const int px = T.rx0 + i;
+    int R2v[kDenseSub], zv[kDenseSub], rv[kDenseSub];
+    int xlo = INT_MAX, xhi = INT_MIN, ylo = INT_MAX, yhi = INT_MIN;
+#pragma unroll
+    for (int sub = 0; sub < kDenseSub; ++sub) {
+        const int j = jt + 8 * sub;
+        int R2 = -1, z = 0;
+        if (i < T.rw && j < T.rh) {
+            const int2 r = pix[T.pix_off + (int64_t)j * T.rw + i];
+            z = r.x;
+            R2 = r.y;
+        }
+        const int r = R2 > rs2 ? isqrt_i32(R2) : -1;
+        R2v[sub] = R2;
+        zv[sub] = z;
+        rv[sub] = r;
+        if (r >= 0) {
+            const int py = T.ry0 + j;
+            xlo = min(xlo, px - r);
+            xhi = max(xhi, px + r + 1);
+            ylo = min(ylo, py - r);
+            yhi = max(yhi, py + r);
+        }
+    }
+    xlo = block_reduce_int<false>(xlo, red);
+    if (xlo == INT_MAX) return;                 // no disc in this tile takes the span path
+    xhi = block_reduce_int<true>(xhi, red);
+    ylo = block_reduce_int<false>(ylo, red);
+    yhi = block_reduce_int<true>(yhi, red);
+    const int c0 = max(xlo, 0), c1 = min(xhi, T.ncols - 1);
+    const int r0 = max(ylo, 0), r1 = min(yhi, T.nrows - 1);
+    if (c0 > c1 || r0 > r1) return;             // every disc lies outside the grid
+    const Scalars& s = sc[t];
+    const bool packed = s.packed != 0;
+    unsigned long long* D = D_all + T.cell_off;
+    int* Dc = Dc_all + T.cell_off;
+    const int W = c1 - c0 + 1;
+    const int CH = win_words / W;
+    if (!packed || CH < 1) {
+        // direct path: every span's markers straight to the grid
+#pragma unroll 1
+        for (int sub = 0; sub < kDenseSub; ++sub) {
+            const int r = rv[sub];
+            if (r < 0) continue;
+            const int R2 = R2v[sub], z = zv[sub];
+            const int py = T.ry0 + jt + 8 * sub;
+            const unsigned long long v = span_word(z, s.zbase, s.kbits);
+            int w = r;
+            for (int dy = 0; dy <= r; ++dy) {
+                const long long t2 = (long long)R2 - (long long)dy * dy;
+                while ((long long)w * w > t2) --w;
+                emit_span(py + dy, px - w, px + w, T.ncols, T.nrows, packed, v, z, D, Dc);
+                if (dy) emit_span(py - dy, px - w, px + w, T.ncols, T.nrows, packed, v, z, D, Dc);
+            }
+        }
+        return;
+    }
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+#pragma unroll 1
+    for (int y0 = r0; y0 <= r1; y0 += CH) {
+        const int y1 = min(y0 + CH - 1, r1);
+        const int nw = (y1 - y0 + 1) * W;
+        for (int e = tid; e < nw; e += 256) sw[e] = 0ull;
+        __syncthreads();
+#pragma unroll 1
+        for (int sub = 0; sub < kDenseSub; ++sub) {
+            const int r = rv[sub];
+            if (r < 0) continue;
+            const int py = T.ry0 + jt + 8 * sub;
+            const int ya = max(py - r, y0), yb = min(py + r, y1);
+            if (ya > yb) continue;
+            const unsigned R2 = (unsigned)R2v[sub];
+            const unsigned long long v = span_word(zv[sub], s.zbase, s.kbits);
+            int dy = ya - py;
+            unsigned w = (unsigned)isqrt_i32((int)(R2 - (unsigned)(dy * dy)));
+            for (int y = ya; y <= yb; ++y, ++dy) {
+                const unsigned t2 = R2 - (unsigned)(dy * dy);
+                if (dy <= 0) {
+                    while ((w + 1) * (w + 1) <= t2) ++w;
+                } else {
+                    while (w * w > t2) --w;
+                }
+                const int a = max(px - (int)w, 0), b = px + (int)w + 1;
+                if (a > T.ncols - 1 || b <= 0) continue;   // this row's span misses the grid
+                const int row = (y - y0) * W - c0;     // a and b lie in [c0, c1]
+                atomicAdd(&sw[row + a], v);
+                if (b < T.ncols) atomicAdd(&sw[row + b], (unsigned long long)(-(long long)v));
+            }
+        }
+        __syncthreads();
+        for (int rr = threadIdx.y; rr <= y1 - y0; rr += 8) {
+            const unsigned long long* src = sw + rr * W;
+            unsigned long long* dst = D + (int64_t)(y0 + rr) * T.ncols + c0;
+            for (int c = threadIdx.x; c < W; c += 32) {
+                const unsigned long long v = src[c];
+                if (v) atomicAdd(&dst[c], v);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Statistics only (not part of the launch sequence): spans per radius
+// bucket of the span-path pixels (r = floor(sqrt(R2)), bucket = bit length
+// of r), one CTA per 32 x kTileY raster tile.
+__global__ void __launch_bounds__(256) k_span_hist(BatchTables bt, const int2* __restrict__ pix, Scalars* sc) {
+    __shared__ unsigned hist[kSpanHistBuckets];
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid < kSpanHistBuckets) hist[tid] = 0;
+    __syncthreads();
+    const int t = find_tile(bt.rt_base, bt.ntiles, blockIdx.x);
+    const TileParams& T = bt.tiles[t];
+    const int lt = blockIdx.x - __ldg(&bt.rt_base[t]);
+    const int ntx = (T.rw + kTileX - 1) / kTileX;
+    const int i = (lt % ntx) * kTileX + threadIdx.x;
+    const int rs2 = T.rs * T.rs;
+    for (int sub = 0; sub < kDenseSub; ++sub) {
+        const int j = (lt / ntx) * kTileY + threadIdx.y + 8 * sub;
+        if (i >= T.rw || j >= T.rh) continue;
+        const int R2 = pix[T.pix_off + (int64_t)j * T.rw + i].y;
+        if (R2 <= rs2) continue;
+        const int r = isqrt_i32(R2);
+        const int k = min(32 - __clz(r), kSpanHistBuckets - 1);
+        atomicAdd(&hist[k], 2u * (unsigned)r + 1u);
+    }
+    __syncthreads();
+    if (tid < kSpanHistBuckets && hist[tid]) atomicAdd(&sc[t].span_hist[tid], (unsigned long long)hist[tid]);
 }
 
 // In-place inclusive prefix of one grid row (256 threads, 4 values each per step).

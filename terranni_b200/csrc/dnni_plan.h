@@ -125,6 +125,8 @@ struct HostBatch {
     int64_t out_end = 0, site_end = 0;   // extent of the caller's output arrays used
     int64_t cost = 0;
     int rs = 3;                          // stencil radius shared by the batch
+    int win_words = kSpanWindowWords;    // shared-memory words of the span window per CTA
+    int far_blocks = kFarBlocksDefault;  // far groups: 1 = 8 x 4 pixel blocks, 0 = 32 x 1 rows
     bool too_big = false;                // a launch index or the far worklist would pass int32
 };
 

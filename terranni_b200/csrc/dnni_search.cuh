@@ -90,6 +90,8 @@ struct TileParams {
     int64_t site_off;            // site map in the caller's array, -1 = none
 };
 
+constexpr int kSpanHistBuckets = 16;   // span radius r in [2^(k-1), 2^k), k = 0: r = 0
+
 struct Scalars {
     int32_t bbox[6];             // min/max of x-ox, y-oy, z
     int32_t err;
@@ -101,6 +103,9 @@ struct Scalars {
     unsigned long long big_pixels[kStatSlots];
     unsigned long long spans[kStatSlots];
     unsigned long long nodata[kStatSlots];
+    unsigned long long evals_dense[kStatSlots];   // candidate evaluations of the ring search
+    unsigned long long evals_far[kStatSlots];     // and of the far pass (seeds and disc search)
+    unsigned long long span_hist[kSpanHistBuckets];   // spans per radius bucket (statistics runs)
 };
 
 // ---------------------------------------------------------------------------
@@ -148,6 +153,7 @@ struct Best {
     uint32_t gid;
     int z;
     int idx;      // position of the site in the sorted point array
+    int nev;      // candidate distance evaluations made for this pixel
 };
 
 DNNI_HD void consider(Best& b, const int4 p, int q, int px, int py) {
@@ -212,6 +218,7 @@ DNNI_HD bool ring_done(long long best, long long px, long long py, long long gx0
 }
 
 DNNI_HD void scan_points(Best& b, const int4* __restrict__ pts, int s, int e, int px, int py) {
+    b.nev += e - s;
     for (int q = s; q < e; ++q) consider(b, DNNI_LDG(&pts[q]), q, px, py);
 }
 
@@ -284,6 +291,7 @@ DNNI_HD bool search_bins_window(const BinGrid& g, const BinWindow& w, int px, in
             if (k > 0 && box_lb(px, py, X0, X0 + bs - 1, Y0, Y0 + bs - 1) > b.d2) continue;
             const int lk = (y - w.wy0) * w.wnx + (x - w.wx0);
             const int s0 = w.lstart[lk], e0 = w.lstart[lk + 1], g0 = w.gstart[lk];
+            b.nev += e0 - s0;
             for (int q = s0; q < e0; ++q) consider(b, w.lpts[q], g0 + (q - s0), px, py);
         }
         if (ring_done(b.d2, px, py, gx0, gy0, bs, bx - k, bx + k, by - k, by + k, g.nbx, g.nby)) return true;
@@ -297,6 +305,7 @@ DNNI_HD bool search_bins_window(const BinGrid& g, const BinWindow& w, int px, in
 // is two rows plus two columns.  b.idx holds a window-local point index on
 // return (window_global_index converts it).  Same result as search_bins.
 DNNI_HD void scan_local(Best& b, const int4* lpts, int s, int e, int px, int py) {
+    b.nev += e - s;
     for (int q = s; q < e; ++q) consider(b, lpts[q], q, px, py);
 }
 
@@ -344,6 +353,7 @@ struct Best32 {
     unsigned long long key;   // d2 << 32 | gid; ~0 = none
     int z;
     int idx;
+    int nev;                  // candidate distance evaluations
 };
 
 DNNI_HD void consider32(Best32& b, const int4 p, int q, int px, int py) {
@@ -360,6 +370,7 @@ DNNI_HD void consider32(Best32& b, const int4 p, int q, int px, int py) {
 DNNI_HD long long best32_d2(const Best32& b) { return b.key == ~0ull ? LLONG_MAX : (long long)(b.key >> 32); }
 
 DNNI_HD void scan_local32(Best32& b, const int4* lpts, int s, int e, int px, int py) {
+    b.nev += e - s;
     for (int q = s; q < e; ++q) consider32(b, lpts[q], q, px, py);
 }
 
@@ -392,7 +403,7 @@ DNNI_HD bool search_window_fast32(const BinGrid& g, const BinWindow& w, int px, 
     bx = bx < g.nbx - 1 ? bx : g.nbx - 1;
     by = by < g.nby - 1 ? by : g.nby - 1;
     const int lx = bx - w.wx0, ly = by - w.wy0;
-    Best32 b{~0ull, INT_MAX, -1};
+    Best32 b{~0ull, INT_MAX, -1, 0};
     bool done;
     {
         const int x0 = lx - 1 > 0 ? lx - 1 : 0, x1 = lx + 1 < w.wnx - 1 ? lx + 1 : w.wnx - 1;
@@ -427,6 +438,7 @@ DNNI_HD bool search_window_fast32(const BinGrid& g, const BinWindow& w, int px, 
     out.gid = b.key == ~0ull ? 0xFFFFFFFFu : (uint32_t)(b.key & 0xFFFFFFFFull);
     out.z = b.z;
     out.idx = b.idx;
+    out.nev += b.nev;
     return done;
 }
 

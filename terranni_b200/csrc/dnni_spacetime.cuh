@@ -423,7 +423,9 @@ static dnni_status spacetime_run(dnni_ctx* c, const dnni_workpackage* wp, const 
     CK(cudaMemsetAsync(a.D, 0, sizeof(unsigned long long) * (size_t)cells, st));
     CK(cudaMemsetAsync(a.Dc, 0, sizeof(int) * (size_t)cells, st));
     const int nrt = hb.rt_base.back();
-    for (int s = 0; s < S; ++s) k_scatter_spans<<<nrt, dim3(32, 8), 0, st>>>(bt, pix + (int64_t)s * npix, a.sc, a.D, a.Dc);
+    for (int s = 0; s < S; ++s)
+        k_scatter_window<<<nrt, dim3(32, 8), sizeof(unsigned long long) * hb.win_words, st>>>(
+            bt, pix + (int64_t)s * npix, a.sc, a.D, a.Dc, hb.win_words);
     if (timing) CK(cudaEventRecord(c->ev[3], st));
     k_rowscan<<<hb.grow_base.back(), kScanThreads, 0, st>>>(bt, a.D, a.Dc, a.sc);
     launch_st_final(bt, hb.ct_base.back(), hb.rs, pix, S, npix, a.sc, a.D, a.Dc, dh, st);

@@ -57,11 +57,14 @@ class Stats(ctypes.Structure):
         ("big_pixels", ctypes.c_int64), ("spans", ctypes.c_int64), ("nodata_cells", ctypes.c_int64),
         ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
         ("max_r2", ctypes.c_int32), ("packed", ctypes.c_int32), ("bin_size", ctypes.c_int32),
-        ("pad", ctypes.c_int32),
+        ("pad", ctypes.c_int32), ("evals_dense", ctypes.c_int64), ("evals_far", ctypes.c_int64),
+        ("span_hist", ctypes.c_int64 * 16),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pad", "span_hist")}
+        d["span_hist"] = list(self.span_hist)
+        return d
 
 
 class Tile(ctypes.Structure):
@@ -76,7 +79,8 @@ class Tile(ctypes.Structure):
 
 class BatchOptions(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32),
-                ("use_graph", ctypes.c_int32), ("order_by_cost", ctypes.c_int32)]
+                ("use_graph", ctypes.c_int32), ("order_by_cost", ctypes.c_int32),
+                ("span_window", ctypes.c_int32), ("far_group", ctypes.c_int32)]
 
 
 class Segment(ctypes.Structure):
@@ -161,7 +165,7 @@ class CompatWP(ctypes.Structure):
 
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
-                ("pad", ctypes.c_int32)]
+                ("span_window", ctypes.c_int32)]
 
 
 class TuneReport(ctypes.Structure):
@@ -170,7 +174,7 @@ class TuneReport(ctypes.Structure):
 
     def as_dict(self):
         t = [{"small_radius": self.trial[k].small_radius, "bin_target": self.trial[k].bin_target,
-              "ms": self.trial[k].ms} for k in range(self.ntrials)]
+              "span_window": self.trial[k].span_window, "ms": self.trial[k].ms} for k in range(self.ntrials)]
         return {"sample_tiles": self.sample_tiles, "ms_default": self.ms_default,
                 "best": t[self.best] if t else None, "trials": t}
 
@@ -360,18 +364,21 @@ class Engine:
             stream, ctypes.byref(st) if st is not None else None))
         return st
 
-    def batch(self, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False):
+    def batch(self, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False, span_window=0,
+              far_group=0):
         """Plans a batch of tiles (dnni_batch_create) -> Batch."""
-        return Batch(self, tiles, small_radius, bin_target, use_graph, order_by_cost)
+        return Batch(self, tiles, small_radius, bin_target, use_graph, order_by_cost, span_window, far_group)
 
-    def autotune(self, tiles, d_xyz, d_gid=None, sample_tiles=256, small_radius=0, bin_target=0):
-        """dnni_batch_autotune -> (dict(small_radius, bin_target), report dict)."""
+    def autotune(self, tiles, d_xyz, d_gid=None, sample_tiles=256, small_radius=0, bin_target=0, span_window=0,
+                 far_group=0):
+        """dnni_batch_autotune -> (dict(small_radius, bin_target, span_window), report dict)."""
         arr = (Tile * len(tiles))(*tiles)
-        opt = BatchOptions(int(small_radius), int(bin_target), 0, 0)
+        opt = BatchOptions(int(small_radius), int(bin_target), 0, 0, int(span_window), int(far_group))
         rep = TuneReport()
         self._check(lib().dnni_batch_autotune(self._h, arr, len(tiles), _ptr(d_xyz), _ptr(d_gid), int(sample_tiles),
                                               ctypes.byref(opt), ctypes.byref(rep)))
-        return {"small_radius": opt.small_radius, "bin_target": opt.bin_target}, rep.as_dict()
+        return ({"small_radius": opt.small_radius, "bin_target": opt.bin_target, "span_window": opt.span_window},
+                rep.as_dict())
 
     def segment_run(self, xyz, ncols, nrows, cell_size, origin=(0, 0), tile=0, halo=0, tiles_per_batch=0,
                     z_scale=0.01, z_offset=0.0, nodata=-9999.0, small_radius=0, site=False, out_h=None):
@@ -429,10 +436,12 @@ def make_tile(wp: WorkPackage, pt_offset, pt_count, out_offset, site_offset=-1, 
 class Batch:
     """A planned batch of tiles (dnni_batch); runs many times."""
 
-    def __init__(self, eng: Engine, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False):
+    def __init__(self, eng: Engine, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False,
+                 span_window=0, far_group=0):
         self._eng = eng
         arr = (Tile * len(tiles))(*tiles)
-        opt = BatchOptions(int(small_radius), int(bin_target), int(bool(use_graph)), int(bool(order_by_cost)))
+        opt = BatchOptions(int(small_radius), int(bin_target), int(bool(use_graph)), int(bool(order_by_cost)),
+                           int(span_window), int(far_group))
         h = _P()
         eng._check(lib().dnni_batch_create(eng.handle, arr, len(tiles), ctypes.byref(opt), ctypes.byref(h)))
         self._h = h
