@@ -210,9 +210,11 @@ typedef struct dnni_batch_options {
     int32_t bin_target;            /* 0 = the context's setting */
     int32_t use_graph;             /* capture the launch sequence in a CUDA graph */
     int32_t order_by_cost;         /* schedule the largest tiles first */
-    int32_t span_window;           /* 64-bit words of shared memory per raster
+    int32_t span_window;           /* 8-byte cells of shared memory per raster
                                       tile in which the span path merges its
-                                      markers (256..26624); 0 = default (8192) */
+                                      markers (256..26624), 1 = no window (every
+                                      marker straight to the grid); 0 = default
+                                      (4096) */
     int32_t far_group;             /* pixels the far pass searches together:
                                       1 = 32 x 1 rows, 2 = 8 x 4 blocks;
                                       0 = default (2) */

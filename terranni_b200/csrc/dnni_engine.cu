@@ -358,8 +358,8 @@ static dnni_status plan_batch(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
     const int rs_ = o.small_radius ? o.small_radius : c->s.small_radius;
     const int bt_ = o.bin_target ? o.bin_target : c->s.bin_target;
     const int ww_ = o.span_window ? o.span_window : kSpanWindowWords;
-    if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0 || ww_ < 256 || ww_ > kSpanWindowMaxWords || o.far_group < 0 ||
-        o.far_group > 2)
+    if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0 || (ww_ != 1 && ww_ < 256) || ww_ > kSpanWindowMaxWords ||
+        o.far_group < 0 || o.far_group > 2)
         return set_err(c, DNNI_E_INVAL, "bad batch options");
     const int fb_ = o.far_group ? o.far_group - 1 : kFarBlocksDefault;
     std::vector<TileParams> plan(ntiles);
@@ -1001,7 +1001,7 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     // then the span path's shared-memory window
     static const int kBinTargets[] = {2, 3, 4, 6, 8, 12};
     static const int kRadii[] = {1, 2, 3, 4, 5, 6};
-    static const int kWindows[] = {4096, 8192, 12288, 18432, 26624};
+    static const int kWindows[] = {1, 2048, 4096, 8192, 12288};   // 1: no window
     for (int bt_ : kBinTargets) {
         if (rs || bt_ == bt0) continue;
         float ms = 0;

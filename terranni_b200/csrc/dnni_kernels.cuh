@@ -7,7 +7,7 @@
 //     colour buffer)                       -> k_bin_* + k_near_dense/far
 //   nni.cpp:794-820 performNNIQueries / nni.cpp:483-534 makeBlocks and
 //     cuda_nni.cu:407-488 calcNNI (query planes OR-blended into bit masks,
-//     then per-pixel int32 atomics)        -> k_scatter_spans + k_final stencil
+//     then per-pixel int32 atomics)        -> k_scatter_window + k_final stencil
 //   cuda_nni.cu:491-503 divide, cuda_nni.cu:399-402 zeroValues
 //                                          -> k_rowscan + k_final
 //
@@ -880,66 +880,26 @@ __device__ __forceinline__ void emit_span(int row, int a, int b, int ncols, int 
     }
 }
 
-// Span path: every pixel with R2 > rs^2 adds its disc as row spans
-// (+v at the first cell, -v after the last) to the per-row difference array.
-// One CTA (32 x 8 threads) per 32 x kTileY raster tile; a warp takes 32
-// consecutive pixels of one row at a time (rows w, w + 8, ...), so one
-// iteration's markers fall on two rows near each other in memory.
-__global__ void __launch_bounds__(256) k_scatter_spans(BatchTables bt, const int2* __restrict__ pix,
-                                                       const Scalars* __restrict__ sc,
-                                                       unsigned long long* __restrict__ D_all,
-                                                       int* __restrict__ Dc_all) {
-    const int t = find_tile(bt.rt_base, bt.ntiles, blockIdx.x);
-    const TileParams& T = bt.tiles[t];
-    const int lt = blockIdx.x - __ldg(&bt.rt_base[t]);
-    const int ntx = (T.rw + kTileX - 1) / kTileX;
-#pragma unroll 1
-    for (int sub = 0; sub < kDenseSub; ++sub) {
-    const int i = (lt % ntx) * kTileX + threadIdx.x, j = (lt / ntx) * kTileY + threadIdx.y + 8 * sub;
-    int R2 = -1, z = 0;
-    if (i < T.rw && j < T.rh) {
-        const int2 r = pix[T.pix_off + (int64_t)j * T.rw + i];
-        z = r.x;
-        R2 = r.y;
-    }
-    const bool big = R2 > T.rs * T.rs;
-    if (!__any_sync(0xffffffffu, big)) continue;
-    const int r = big ? isqrt_i32(R2) : -1;
-    const int rmax = __reduce_max_sync(0xffffffffu, r);
-    const Scalars& s = sc[t];
-    const bool packed = s.packed != 0;
-    const unsigned long long v = span_word(z, s.zbase, s.kbits);
-    unsigned long long* D = D_all + T.cell_off;
-    int* Dc = Dc_all + T.cell_off;
-    const int px = T.rx0 + i, py = T.ry0 + j;
-    int w = r;
-    for (int dy = 0; dy <= rmax; ++dy) {
-        if (dy <= r) {
-            const long long t2 = (long long)R2 - (long long)dy * dy;
-            while ((long long)w * w > t2) --w;
-            emit_span(py + dy, px - w, px + w, T.ncols, T.nrows, packed, v, z, D, Dc);
-            if (dy) emit_span(py - dy, px - w, px + w, T.ncols, T.nrows, packed, v, z, D, Dc);
-        }
-    }
-    }
-}
-
-// Span path through a shared-memory window.  The discs of one 32 x kTileY
-// raster tile cover a window of grid cells a little larger than the tile by
-// the largest radius; the window is processed in chunks of whole rows that
-// fit `win_words` 64-bit words of shared memory.  For each chunk every disc
-// of the tile adds its row spans' markers (+v at the first cell, -v after
-// the last: the per-row difference form of k_scatter_spans) to the chunk
-// with shared-memory atomics, and the chunk's non-zero words are then added
-// to the grid's difference array with one coalesced global atomic each.  The
+// Span path: every pixel with R2 > rs^2 adds its disc as row spans (+v at
+// the first cell, -v after the last, into the per-row difference words).
+// One CTA (32 x 8 threads) per 32 x kTileY raster tile.  The tile's discs
+// cover a window of grid cells a little larger than the tile by the largest
+// radius; the window is processed in chunks of whole rows that fit
+// `win_words` 8-byte cells of shared memory.  For each chunk every disc of
+// the tile adds its row spans' markers (z - zbase and 1 at the first cell,
+// their negatives after the last) to two int32 arrays with native
+// shared-memory atomics,
+// and each touched cell is then added to the grid's difference array as one
+// packed word, (sum << K) + count, with one coalesced global atomic.  The
 // markers of a tile's discs fall on far fewer distinct cells than there are
 // markers (neighbouring pixels' discs share rows and end near each other),
 // so the grid sees a fraction of the global atomics of the direct path, and
 // those it sees are contiguous.  The sum is the same: the words add modulo
 // 2^64 in any order and the packed form is linear.  Tiles with the unpacked
-// accumulators (separate int64 Z and int32 C), and windows wider than one
-// chunk row, take the direct path.
-constexpr int kSpanWindowWords = 8192;      // default: 64 KB per CTA, three CTAs per SM
+// accumulators (separate int64 Z and int32 C), with a z range the int32
+// window sums could overflow, or with windows wider than one chunk row,
+// take the direct path.
+constexpr int kSpanWindowWords = 4096;      // default: 32 KB per CTA (two int32 arrays)
 constexpr int kSpanWindowMaxWords = 26624;  // 208 KB, the most one CTA may take
 
 // Minimum (or maximum) of v over a 32 x 8 CTA; red: 8 ints of shared memory.
@@ -1006,7 +966,13 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
     int* Dc = Dc_all + T.cell_off;
     const int W = c1 - c0 + 1;
     const int CH = win_words / W;
-    if (!packed || CH < 1) {
+    // the window sums z relative to zbase and the counts in two int32 arrays
+    // (native shared-memory atomics); a window cell receives at most one
+    // marker per pixel of the tile, so |sum| <= kTileX * kTileY * zabs must
+    // stay below 2^31
+    const long long zabs = max((long long)s.bbox[5] - s.zbase, s.zbase - (long long)s.bbox[4]);
+    const bool fits32 = zabs < (1LL << 31) / (kTileX * kTileY);
+    if (!packed || CH < 1 || !fits32) {
         // direct path: every span's markers straight to the grid
 #pragma unroll 1
         for (int sub = 0; sub < kDenseSub; ++sub) {
@@ -1026,11 +992,16 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
         return;
     }
     const int tid = threadIdx.y * 32 + threadIdx.x;
+    int* sz = reinterpret_cast<int*>(sw);     // z - zbase sums
+    int* scn = sz + win_words;                // counts
 #pragma unroll 1
     for (int y0 = r0; y0 <= r1; y0 += CH) {
         const int y1 = min(y0 + CH - 1, r1);
         const int nw = (y1 - y0 + 1) * W;
-        for (int e = tid; e < nw; e += 256) sw[e] = 0ull;
+        for (int e = tid; e < nw; e += 256) {
+            sz[e] = 0;
+            scn[e] = 0;
+        }
         __syncthreads();
 #pragma unroll 1
         for (int sub = 0; sub < kDenseSub; ++sub) {
@@ -1040,7 +1011,7 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
             const int ya = max(py - r, y0), yb = min(py + r, y1);
             if (ya > yb) continue;
             const unsigned R2 = (unsigned)R2v[sub];
-            const unsigned long long v = span_word(zv[sub], s.zbase, s.kbits);
+            const int zr = (int)((long long)zv[sub] - s.zbase);
             int dy = ya - py;
             unsigned w = (unsigned)isqrt_i32((int)(R2 - (unsigned)(dy * dy)));
             for (int y = ya; y <= yb; ++y, ++dy) {
@@ -1053,17 +1024,23 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
                 const int a = max(px - (int)w, 0), b = px + (int)w + 1;
                 if (a > T.ncols - 1 || b <= 0) continue;   // this row's span misses the grid
                 const int row = (y - y0) * W - c0;     // a and b lie in [c0, c1]
-                atomicAdd(&sw[row + a], v);
-                if (b < T.ncols) atomicAdd(&sw[row + b], (unsigned long long)(-(long long)v));
+                atomicAdd(&sz[row + a], zr);
+                atomicAdd(&scn[row + a], 1);
+                if (b < T.ncols) {
+                    atomicAdd(&sz[row + b], -zr);
+                    atomicAdd(&scn[row + b], -1);
+                }
             }
         }
         __syncthreads();
+        // one packed word per touched cell: (sum zrel << K) + count, modulo 2^64
         for (int rr = threadIdx.y; rr <= y1 - y0; rr += 8) {
-            const unsigned long long* src = sw + rr * W;
             unsigned long long* dst = D + (int64_t)(y0 + rr) * T.ncols + c0;
             for (int c = threadIdx.x; c < W; c += 32) {
-                const unsigned long long v = src[c];
-                if (v) atomicAdd(&dst[c], v);
+                const int zs = sz[rr * W + c], cn = scn[rr * W + c];
+                if (zs | cn)
+                    atomicAdd(&dst[c], ((unsigned long long)(long long)zs << s.kbits) +
+                                           (unsigned long long)(long long)cn);
             }
         }
         __syncthreads();

@@ -9,7 +9,7 @@
 //     colour buffer)                       -> k_bin_* + k_nearest
 //   nni.cpp:794-820 performNNIQueries / nni.cpp:483-534 makeBlocks and
 //     cuda_nni.cu:407-488 calcNNI (query planes OR-blended into bit masks,
-//     then per-pixel int32 atomics)        -> k_scatter_spans + k_final stencil
+//     then per-pixel int32 atomics)        -> k_scatter_window + k_final stencil
 //   cuda_nni.cu:491-503 divide, cuda_nni.cu:399-402 zeroValues
 //                                          -> k_rowscan + k_final
 //
