@@ -828,6 +828,18 @@ __global__ void __launch_bounds__(256, 4) k_near_far(BatchTables bt, const int4*
             if (nb >= 0) seed_from_block(g, pts, start, bmask, nb, px, py, b);
             if (b.d2 == LLONG_MAX) seed_from_superblocks(g, pts, start, bmask, smask, px, py, b);
         }
+        // the seeds of the group's corner lanes are candidates for every
+        // pixel of the group: a lane whose own seed came from a distant
+        // block starts the disc search with a tighter bound
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int src = (k & 1 ? 7 : 0) + (k & 2 ? 24 : 0);
+            const int q = __shfl_sync(0xffffffffu, b.idx, src);
+            if (act && q >= 0) {
+                consider(b, __ldg(&pts[q]), q, px, py);
+                b.nev += 1;
+            }
+        }
         search_disc_warp(g, pts, start, bmask, smask, act, px, py, b);
         int R2 = -1;
         if (act) {
