@@ -187,6 +187,57 @@ def cpu_baseline(xyz, side, window, seed_note):
                       f"single-thread C oracle (k-d tree nearest site + row-span scatter), {dt:.2f} s"}
 
 
+def fp64_errors(oracle, ref, h, z_scale=0.01, z_offset=0.0):
+    """Max and RMS |h - h_FP64| over the cells with data, h_FP64 from the
+    oracle's exact integer sums (the FP64 checker)."""
+    import numpy as np
+    ok = ref["C"] > 0
+    truth = oracle.exact_height_f64(ref["Z"][ok], ref["C"][ok], z_scale, z_offset)
+    e = np.abs(np.asarray(h)[ok].astype(np.float64) - truth)
+    return float(e.max(initial=0.0)), float(np.sqrt(np.mean(e * e))) if e.size else 0.0
+
+
+def window_accuracy(oracle, h_grid, xyz, x0, y0, win, halo, cell=100, origin=(0, 0)):
+    """Checks the cells [x0, x0+win) x [y0, y0+win) of a grid that one work
+    package over the whole grid defines (raster = grid) against the oracle's
+    work package over those cells alone, with a raster `halo` cells wider on
+    each side (every pixel whose disc can reach them, for halos above the
+    largest disc radius) and the points within twice the halo (every pixel's
+    nearest site): heights bit for bit and their FP64 error."""
+    import numpy as np
+    ox, oy = origin[0] + x0 * cell, origin[1] + y0 * cell
+    lo_x, hi_x = ox - 2 * halo * cell, ox + (win + 2 * halo) * cell
+    lo_y, hi_y = oy - 2 * halo * cell, oy + (win + 2 * halo) * cell
+    sel = (xyz[:, 0] >= lo_x) & (xyz[:, 0] < hi_x) & (xyz[:, 1] >= lo_y) & (xyz[:, 1] < hi_y)
+    wp = oracle.make_wp(win, win, cell, ox, oy, raster=(-halo, -halo, win + halo, win + halo))
+    ref = oracle.interpolate(wp, xyz[sel])
+    g = np.ascontiguousarray(h_grid[y0:y0 + win, x0:x0 + win])
+    mx, rms = fp64_errors(oracle, ref, g)
+    return {"window": [int(x0), int(y0), int(win)], "halo_cells": int(halo), "points": int(sel.sum()),
+            "bit_exact_vs_oracle": bool(np.array_equal(g.view(np.uint32), ref["h"].view(np.uint32))),
+            "max_abs_err_m": mx, "rms_err_m": rms}
+
+
+def depth_disagreement(oracle, cases, budget_s):
+    """The reference's float32 depth-buffer site choice (emulated by the
+    oracle) against the exact nearest site, over (wp, xyz) cases until the
+    budget is spent: fractions of raster pixels."""
+    pix = site = zd = 0
+    used = 0
+    t0 = time.perf_counter()
+    for wp, xyz in cases:
+        if time.perf_counter() - t0 >= budget_s:
+            break
+        r = oracle.gl_disagreement(wp, xyz)
+        pix += r["pixels"]
+        site += r["site_differs"]
+        zd += r["z_differs"]
+        used += 1
+    n = max(pix, 1)
+    return {"cases": used, "pixels": pix, "site_frac": site / n, "z_frac": zd / n, "depth_bits": 24,
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
 def run_reference_tile4096(args, world, rank):
     """CPU rendition of the reference's algorithm with all host threads."""
     if rank != 0:
@@ -339,7 +390,19 @@ def run_engine_tile4096(args, world, rank, local):
                      "nodata_cells": nod},
         }
         if not args.no_cpu_baseline:
+            from oracle import oracle
             out["cpu_baseline"] = cpu_baseline(xyz, side, min(args.cpu_window, side), "same tile")
+            # the whole tile against the oracle (one work package, as run)
+            ref = oracle.interpolate(oracle.make_wp(side, side, 100), xyz)
+            mx, rms = fp64_errors(oracle, ref, out_p)
+            out["accuracy"] = {"cells_checked": cells, "bit_exact_vs_oracle":
+                               bool(np.array_equal(out_p.view(np.uint32), ref["h"].view(np.uint32))),
+                               "max_abs_err_m": mx, "rms_err_m": rms}
+            del ref
+            win = 256
+            sub = xyz[(xyz[:, 0] < win * 100) & (xyz[:, 1] < win * 100)]
+            out["ref_depth_disagreement"] = depth_disagreement(
+                oracle, [(oracle.make_wp(win, win, 100), sub)], 30.0)
         print(json.dumps(out), flush=True)
     eng.close()
     if world > 1:
@@ -635,7 +698,14 @@ def run_engine_mixed(args, world, rank, local):
                      "nodata_cells": nod},
         }
         if not args.no_cpu_baseline:
+            from oracle import oracle
             out["cpu_baseline"], out["accuracy"] = cpu_baseline_mixed(w, h_gpu, args.cpu_seconds)
+            cases = []
+            for k in sample_order(len(w["lay"]))[:out["accuracy"]["tiles_checked"]]:
+                L = w["lay"][k]
+                cases.append((oracle.make_wp(L["side"], L["side"], L["cell"], *L["origin"]),
+                              w["xyz"][L["pt"]:L["pt"] + L["n"]]))
+            out["ref_depth_disagreement"] = depth_disagreement(oracle, cases, 0.5 * args.cpu_seconds)
         print(json.dumps(out), flush=True)
     eng.close()
     if tdist is not None:
@@ -694,6 +764,14 @@ def run_engine_segment(args, world, rank, local):
     cells = side * side
     value = cells * args.steps * world / dt_max
     nod = int(np.count_nonzero(h_out == np.float32(-9999.0)))
+    acc = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # a window in the middle of the mosaic, across tile seams, against the
+        # oracle's work package over it with a halo above the largest disc
+        from oracle import oracle
+        win = 256
+        x0 = y0 = max(0, side // 2 - win // 2 - args.seg_tile // 2 + 7)
+        acc = window_accuracy(oracle, h_out, xyz, x0, y0, min(win, side), halo=min(600, side // 2))
     if rank == 0:
         peak, peak_kind = peaks()
         ms_step = 1000 * dt_max / args.steps
@@ -720,7 +798,7 @@ def run_engine_segment(args, world, rank, local):
             # occupancy map; per batch: the gather, the batch's sequence and the
             # halo check
             "gpu_launches": int(sum(5 + x.batches * (KERNELS_PER_BATCH + 2) for x in stats)),
-            "clocks": clk.summary(), "nodata_cells": nod,
+            "clocks": clk.summary(), "nodata_cells": nod, "accuracy": acc,
         }), flush=True)
     eng.close()
     if tdist is not None:
@@ -770,7 +848,7 @@ def run_engine_spacetime(args, world, rank, local):
     dev_ms = float(np.mean([x.ms_total for x in stats]))
     # CPU baseline and parity on a window of the same cloud (the oracle is
     # test infrastructure: here it only times and checks)
-    cpu = None
+    cpu = acc = None
     if rank == 0 and not args.no_cpu_baseline:
         win = 512
         sel = (xyz[:, 0] < (win + 8) * 100) & (xyz[:, 1] < (win + 8) * 100)
@@ -784,6 +862,10 @@ def run_engine_spacetime(args, world, rank, local):
                "sample": f"oracle space-time k-d restatement, one {win}x{win} window of the same cloud "
                          f"({int(sel.sum())} points), {cpu_s:.1f} s",
                "bit_exact_vs_engine": bool(np.array_equal(got.view(np.uint32), ref["h"].view(np.uint32)))}
+        mx, rms = fp64_errors(oracle, ref, got)
+        acc = {"cells_checked": win * win, "bit_exact_vs_oracle": cpu["bit_exact_vs_engine"],
+               "max_abs_err_m": mx, "rms_err_m": rms,
+               "note": "the engine on a window of the same cloud as its own work package"}
     if rank == 0:
         peak, peak_kind = peaks()
         ms_step = 1000 * dt / args.steps
@@ -812,7 +894,7 @@ def run_engine_spacetime(args, world, rank, local):
             # lift and packing decision (3), one span pass per slice, the row scan
             # and the gather-and-divide
             "gpu_launches": args.steps * (20 + 2 * rt + 1),
-            "cpu_baseline": cpu, "clocks": clk.summary(),
+            "cpu_baseline": cpu, "accuracy": acc, "clocks": clk.summary(),
         }), flush=True)
     eng.close()
 
@@ -856,7 +938,7 @@ def run_engine_compat(args, world, rank, local):
             h[:], _ = eng.interpolate_compat(se, we, pts)
         dt = time.perf_counter() - t1
         clk.mark("t_end")
-    cpu = None
+    cpu = acc = None
     if rank == 0 and not args.no_cpu_baseline:
         win = 250
         sel = (pts[:, 0] < (win + 8) * cell) & (pts[:, 1] < (win + 8) * cell)
@@ -871,6 +953,9 @@ def run_engine_compat(args, world, rank, local):
                "sample": f"oracle compat restatement, one {win}x{win} window of the same cloud "
                          f"({int(sel.sum())} points), {cpu_s:.1f} s",
                "bit_exact_vs_engine": bool(np.array_equal(got.view(np.uint32), ref.view(np.uint32)))}
+        acc = {"cells_checked": win * win, "bit_exact_vs_oracle": cpu["bit_exact_vs_engine"],
+               "note": "reference-default semantics: heights carry the reference's own zMultiplier "
+                       "quantisation and truncating divide, so no FP64 error is stated"}
     if rank == 0:
         peak, peak_kind = peaks()
         cells = side * side
@@ -892,7 +977,7 @@ def run_engine_compat(args, world, rank, local):
                          "algorithmic_bytes": alg},
             "e2e": {"value": cells * 1000.0 / ms_step, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
                     "d2h_bytes_per_step": 4 * cells, "note": "the call is host to host"},
-            "gpu_launches": 5 * args.steps, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gpu_launches": 5 * args.steps, "cpu_baseline": cpu, "accuracy": acc, "clocks": clk.summary(),
         }), flush=True)
     eng.close()
 
@@ -900,6 +985,36 @@ def run_engine_compat(args, world, rank, local):
 # ---------------------------------------------------------------------------
 # served: DEM requests against a resident cloud
 # ---------------------------------------------------------------------------
+
+def served_accuracy(reqs, outs, xyz, count, reach_m=450.0, win=128):
+    """The lower-left win x win cells of the `count` smallest requests whose
+    window, with a raster halo of reach_m (above the largest nearest-site
+    distance of the cloud's lakes) on every side, lies inside the cloud's box,
+    checked against the oracle (window_accuracy); a request's result is the
+    window of the interpolation over the whole cloud on its lattice."""
+    from oracle import oracle
+    wx0, wx1 = int(xyz[:, 0].min()), int(xyz[:, 0].max())
+    wy0, wy1 = int(xyz[:, 1].min()), int(xyz[:, 1].max())
+    checks = []
+    for k in sorted(range(len(reqs)), key=lambda k: reqs[k]["ncols"] * reqs[k]["nrows"]):
+        r = reqs[k]
+        cs = r["cell_size"]
+        halo = int(-(-reach_m * 100 // cs))
+        w = min(win, r["ncols"], r["nrows"])
+        if (r["x0"] - halo * cs < wx0 or r["y0"] - halo * cs < wy0 or r["x0"] + (w + halo) * cs > wx1 or
+                r["y0"] + (w + halo) * cs > wy1):
+            continue
+        c = window_accuracy(oracle, outs[k], xyz, 0, 0, w, halo, cell=cs, origin=(r["x0"], r["y0"]))
+        c["request"] = k
+        checks.append(c)
+        if len(checks) == count:
+            break
+    if not checks:
+        return None
+    return {"windows": checks, "bit_exact_vs_oracle": all(c["bit_exact_vs_oracle"] for c in checks),
+            "max_abs_err_m": max(c["max_abs_err_m"] for c in checks),
+            "rms_err_m": max(c["rms_err_m"] for c in checks)}
+
 
 def run_engine_served(args, world, rank, local):
     """A resident cloud on each GPU (per-rank seed) and a Poisson stream of
@@ -982,6 +1097,9 @@ def run_engine_served(args, world, rank, local):
         clk.mark("t_end")
     st = srv.stats()
     srv.close()
+    acc = None
+    if rank == 0 and not args.no_cpu_baseline:
+        acc = served_accuracy(reqs, outs, xyz, 2)
     if rank == 0:
         best = max(results, key=lambda r: r["cells_per_s"])
         top = results[-1]
@@ -1005,6 +1123,7 @@ def run_engine_served(args, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": "whole request path", "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "achieved": None, "frac": None, "traffic": None},
             "gpu_launches": int(st["batches"] * (KERNELS_PER_BATCH + 1)), "clocks": clk.summary(),
+            "accuracy": acc,
         }), flush=True)
     eng.close()
     if tdist is not None:

@@ -711,6 +711,54 @@ __device__ __forceinline__ uint64_t chord_mask8(bool act, long long px, long lon
     return m;
 }
 
+// The same mask as the union of each active lane's own cells instead of the
+// hull across the lanes, in 32-bit arithmetic: per lane and cell row the
+// cells that its disc's chord (widened by one unit) crosses, found with a
+// float reciprocal of u and an exact integer correction, as an 8-bit row
+// mask; the warp ORs the lanes' 64-bit masks.  A superset of the cells
+// within some lane's bound, and a subset of chord_mask8's.  Needs every
+// active lane's d2 < 2^31 and 8u < 2^30.  Warp-uniform result.
+__device__ __forceinline__ uint64_t chord_union8(bool act, long long px, long long py, long long d2, long long X0,
+                                                 long long Y0, int u, float inv_u) {
+    uint32_t mlo = 0, mhi = 0;
+    if (act) {
+        constexpr long long kLim = 1LL << 30;   // beyond it no disc (reach < 2^16) touches the 8u window
+        const long long rx64 = px - X0, ry64 = py - Y0;
+        const int rx = (int)(rx64 < -kLim ? -kLim : (rx64 > kLim ? kLim : rx64));
+        const int ry = (int)(ry64 < -kLim ? -kLim : (ry64 > kLim ? kLim : ry64));
+        const int D2 = (int)d2, w8 = 8 * u;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int y0 = r * u, y1 = y0 + u - 1;
+            const int gy = ry < y0 ? y0 - ry : (ry > y1 ? ry - y1 : 0);
+            if (gy > 46340) continue;            // gy^2 > 2^31 > D2
+            const int v = D2 - gy * gy;
+            if (v < 0) continue;
+            const int w = (int)sqrtf((float)v) + 1;
+            const int lo = rx - w, hi = rx + w;
+            if (hi < 0 || lo >= w8) continue;
+            int a = 0, e = 7;
+            if (lo > 0) {
+                a = (int)((float)lo * inv_u);
+                if (a * u > lo) --a; else if ((a + 1) * u <= lo) ++a;
+            }
+            if (hi < w8) {
+                e = (int)((float)hi * inv_u);
+                if (e * u > hi) --e; else if ((e + 1) * u <= hi) ++e;
+            }
+            const uint32_t row = (0xFFu >> (7 - e)) & (0xFFu << a) & 0xFFu;
+            if (r < 4) mlo |= row << (8 * r); else mhi |= row << (8 * (r - 4));
+        }
+    }
+    mlo = __reduce_or_sync(0xffffffffu, mlo);
+    mhi = __reduce_or_sync(0xffffffffu, mhi);
+    return ((uint64_t)mhi << 32) | mlo;
+}
+
+// A candidate block with at most this many points is scanned whole, which
+// costs less than its bin mask.
+constexpr int kFarWholeBlock = 24;
+
 // Warp-cooperative exact search for the 32 pixels of one worklist group
 // (neighbouring pixels of one tile row; inactive lanes have act = false).
 // The warp walks the superblocks of the union of the lanes' bound boxes
@@ -736,6 +784,10 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
     cell_range((xlo + xhi) / 2, (xhi - xlo) / 2 + 1, gx0, u2, g.n2x, sx0, sx1);
     cell_range((ylo + yhi) / 2, (yhi - ylo) / 2 + 1, gy0, u2, g.n2y, sy0, sy1);
     if (sx0 > sx1 || sy0 > sy1) return;
+    // the 32-bit chord masks apply when the cells are small enough (and,
+    // per call, every bound is below 2^31)
+    const bool fast1 = 8 * u1 < (1LL << 30), fast0 = 8 * bs < (1LL << 30);
+    const float inv_u1 = 1.0f / (float)u1, inv_bs = 1.0f / (float)bs;
     const long long cyy = warp_min64(act ? py : LLONG_MAX);
     int csy = udiv32((cyy < gy0 ? gy0 : cyy) - gy0, u2);
     csy = csy < sy0 ? sy0 : (csy > sy1 ? sy1 : csy);
@@ -753,15 +805,27 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
             if (!__any_sync(full, need_s)) continue;
             // 32-bit square roots are within one unit while every bound is below 2^31
             bool small = __all_sync(full, !act || b.d2 < (1LL << 31));
-            uint64_t cand = sm & chord_mask8(act, px, py, b.d2, SX0, SY0, u1, small);
+            uint64_t cand = sm & (small && fast1 ? chord_union8(act, px, py, b.d2, SX0, SY0, (int)u1, inv_u1)
+                                                 : chord_mask8(act, px, py, b.d2, SX0, SY0, u1, small));
             while (cand) {
                 const int m = ffs64(cand);
                 cand &= cand - 1;
                 const long long BX0 = SX0 + (long long)(m & 7) * u1, BY0 = SY0 + (long long)(m >> 3) * u1;
                 const int64_t blk = ((int64_t)sidx << 6) + m;
+                const int bp0 = __ldg(&start[blk << 6]), bp1 = __ldg(&start[(blk + 1) << 6]);
+                if (bp1 - bp0 <= kFarWholeBlock) {
+                    // few points: the block's range whole (its bins are consecutive)
+                    if (act) b.nev += bp1 - bp0;
+                    for (int q = bp0; q < bp1; ++q) {
+                        const int4 p = __ldg(&pts[q]);
+                        if (act) consider(b, p, q, px, py);
+                    }
+                    continue;
+                }
                 const uint64_t bm = __ldg(&bmask[blk]);
                 small = __all_sync(full, !act || b.d2 < (1LL << 31));
-                uint64_t qc = bm & chord_mask8(act, px, py, b.d2, BX0, BY0, bs, small);
+                uint64_t qc = bm & (small && fast0 ? chord_union8(act, px, py, b.d2, BX0, BY0, (int)bs, inv_bs)
+                                                   : chord_mask8(act, px, py, b.d2, BX0, BY0, bs, small));
                 while (qc) {
                     const int l = ffs64(qc);
                     qc &= qc - 1;

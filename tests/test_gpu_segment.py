@@ -54,6 +54,23 @@ def test_segment_equals_one_work_package(eng, ncols, nrows, tile, halo, tpb, n, 
     assert st.points == xyz.shape[0] and st.cells == ncols * nrows
 
 
+def test_segment_mosaic_against_the_oracle(eng, oracle):
+    # the stitched grid checked directly against the oracle's one work
+    # package: site map and heights bit for bit, FP64 error within 1e-4 m
+    ncols, nrows = 900, 700
+    ox, oy = 12_000_000, 34_000_000
+    xyz = _cloud(41, ncols, nrows, 200_000, lakes=3) + np.array([ox, oy, 0], np.int32)
+    h, s, st = eng.segment_run(xyz, ncols, nrows, 100, origin=(ox, oy), tile=256, halo=0, tiles_per_batch=4,
+                               site=True)
+    ref = oracle.interpolate(oracle.make_wp(ncols, nrows, 100, ox, oy), xyz)
+    assert np.array_equal(s, ref["site"])
+    assert np.array_equal(h.view(np.uint32), ref["h"].view(np.uint32))
+    ok = ref["C"] > 0
+    truth = oracle.exact_height_f64(ref["Z"][ok], ref["C"][ok], 0.01, 0.0)
+    assert np.abs(h[ok].astype(np.float64) - truth).max() <= 1e-4
+    assert st.tiles == 12
+
+
 def test_segment_reruns_tiles_whose_halo_is_too_small(eng):
     ncols = nrows = 600
     xyz = _cloud(3, ncols, nrows, 40_000, lakes=4)

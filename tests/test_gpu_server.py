@@ -102,6 +102,29 @@ def test_server_results_match_the_definition_and_the_mix(eng, cloud):
     assert np.all(off[0] == np.float32(-9999.0)) and np.all(off[1] == 0xFFFFFFFF)
 
 
+def test_server_results_against_the_oracle(eng, cloud, oracle):
+    # served windows checked directly against the oracle's interpolation of
+    # the definition (the request's grid, raster = the cloud's box on its
+    # lattice): heights and site map bit for bit, FP64 error within 1e-4 m
+    from terranni_b200 import engine
+    reqs = [dict(x0=3_020_000, y0=7_015_000, ncols=180, nrows=140, cell_size=100, site=True),
+            dict(x0=3_055_500, y0=7_060_700, ncols=90, nrows=120, cell_size=200, site=True)]
+    with eng.server(cloud, slots=2, max_batch=4, slot_bytes=512 << 20) as srv:
+        tickets = [srv.submit(**r) for r in reqs]
+        got = [srv.wait(t, timeout=120) for t in tickets]
+    for r, (h, s, _) in zip(reqs, got):
+        wp, (i0, j0) = _world_wp(engine, cloud, r)
+        owp = oracle.make_wp(r["ncols"], r["nrows"], r["cell_size"], r["x0"], r["y0"],
+                             raster=(wp.raster_x0, wp.raster_y0, wp.raster_x1, wp.raster_y1))
+        ref = oracle.interpolate(owp, cloud)
+        assert np.array_equal(h.view(np.uint32), ref["h"].view(np.uint32))
+        ys, xs = np.mgrid[0:r["nrows"], 0:r["ncols"]]
+        assert np.array_equal(s, ref["site"][ys - j0, xs - i0])
+        ok = ref["C"] > 0
+        truth = oracle.exact_height_f64(ref["Z"][ok], ref["C"][ok], 0.01, 0.0)
+        assert np.abs(h[ok].astype(np.float64) - truth).max() <= 1e-4
+
+
 def test_server_rejects_a_request_beyond_its_slot(eng, cloud):
     from terranni_b200 import engine
     with eng.server(cloud, slots=1, slot_bytes=64 << 20) as srv:
