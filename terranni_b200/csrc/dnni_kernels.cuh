@@ -408,28 +408,36 @@ __device__ __forceinline__ void settle_pixel(const TileParams& T, int i, int j, 
     if (site && T.site_off >= 0) site[T.site_off + o] = b.gid;
 }
 
-// Per-warp statistics of settled pixels: span-path pixels and spans, the
-// largest R2, and the candidate distance evaluations made (nev per lane,
-// counted into evals_dense or evals_far).
-__device__ __forceinline__ void warp_stats(const TileParams& T, int R2, Scalars* __restrict__ s, int slot, int nev,
-                                           bool far_pass) {
-    const int rs2 = T.rs * T.rs;
-    const unsigned big = (R2 > rs2) ? 1u : 0u;
-    const unsigned sp = big ? 2u * (unsigned)isqrt_i32(R2) + 1u : 0u;
-    const unsigned nbig = __reduce_add_sync(0xffffffffu, big);
-    const unsigned nsp = __reduce_add_sync(0xffffffffu, sp);
-    const unsigned nv = __reduce_add_sync(0xffffffffu, (unsigned)nev);
-    const int mx = __reduce_max_sync(0xffffffffu, R2);
-    if ((threadIdx.x & 31) == 0) {
-        slot &= kStatSlots - 1;
-        if (nbig) {
-            atomicAdd(&s->big_pixels[slot], (unsigned long long)nbig);
-            atomicAdd(&s->spans[slot], (unsigned long long)nsp);
+// Statistics of settled pixels, accumulated per thread and flushed once per
+// warp: span-path pixels and their spans, the largest R2, and the candidate
+// distance evaluations made (counted into evals_dense or evals_far).
+struct StatAcc {
+    unsigned big = 0, spans = 0, nev = 0;
+    int mx = -1;
+    __device__ __forceinline__ void add(const TileParams& T, int R2, int n) {
+        if (R2 > T.rs * T.rs) {
+            big += 1u;
+            spans += 2u * (unsigned)isqrt_i32(R2) + 1u;
         }
-        if (nv) atomicAdd(far_pass ? &s->evals_far[slot] : &s->evals_dense[slot], (unsigned long long)nv);
-        if (mx >= 0) atomicMax(&s->max_r2[slot], mx);
+        mx = R2 > mx ? R2 : mx;
+        nev += (unsigned)n;
     }
-}
+    __device__ __forceinline__ void flush(Scalars* __restrict__ s, int slot, bool far_pass) {
+        const unsigned nbig = __reduce_add_sync(0xffffffffu, big);
+        const unsigned nsp = __reduce_add_sync(0xffffffffu, spans);
+        const unsigned nv = __reduce_add_sync(0xffffffffu, nev);
+        const int m = __reduce_max_sync(0xffffffffu, mx);
+        if ((threadIdx.x & 31) == 0) {
+            slot &= kStatSlots - 1;
+            if (nbig) {
+                atomicAdd(&s->big_pixels[slot], (unsigned long long)nbig);
+                atomicAdd(&s->spans[slot], (unsigned long long)nsp);
+            }
+            if (nv) atomicAdd(far_pass ? &s->evals_far[slot] : &s->evals_dense[slot], (unsigned long long)nv);
+            if (m >= 0) atomicMax(&s->max_r2[slot], m);
+        }
+    }
+};
 
 // Far worklist slot: tile, raster pixel index within the tile (-1 = empty
 // slot), sorted-array position of the best site so far (-1 = none).
@@ -474,6 +482,7 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
     const int warp = tid >> 5, lane = tid & 31;
     // the tile's rows go in bands, each with its own staged window: the whole
     // tile when its window fits shared memory, else halves, down to 8 rows
+    StatAcc acc;
     int band = kTileY;
     for (int jb = 0; jb < kTileY && j0 + jb < T.rh; jb += band) {
     int wx0 = 0, wy0 = 0, wnx = 0, wny = 0;
@@ -602,10 +611,11 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
             far[base + lane] = far_pixel ? FarSlot{t, j * T.rw + i, b.idx, 0} : FarSlot{t, -1, -1, 0};
         }
     }
-    warp_stats(T, R2, sc + t, blockIdx.x + threadIdx.y + 8 * sub, b.nev, false);
+    acc.add(T, R2, b.nev);
     }
     __syncthreads();     // the next band restages the window
     }
+    acc.flush(sc + t, blockIdx.x + threadIdx.y, false);
     if (far_blocks) {
         // worklist in 8 x 4 pixel blocks: a block with any unsettled pixel
         // appends its 32 pixels as one group (lane = 8 * row + column), so
@@ -711,50 +721,6 @@ __device__ __forceinline__ uint64_t chord_mask8(bool act, long long px, long lon
     return m;
 }
 
-// The same mask as the union of each active lane's own cells instead of the
-// hull across the lanes, in 32-bit arithmetic: per lane and cell row the
-// cells that its disc's chord (widened by one unit) crosses, found with a
-// float reciprocal of u and an exact integer correction, as an 8-bit row
-// mask; the warp ORs the lanes' 64-bit masks.  A superset of the cells
-// within some lane's bound, and a subset of chord_mask8's.  Needs every
-// active lane's d2 < 2^31 and 8u < 2^30.  Warp-uniform result.
-__device__ __forceinline__ uint64_t chord_union8(bool act, long long px, long long py, long long d2, long long X0,
-                                                 long long Y0, int u, float inv_u) {
-    uint32_t mlo = 0, mhi = 0;
-    if (act) {
-        constexpr long long kLim = 1LL << 30;   // beyond it no disc (reach < 2^16) touches the 8u window
-        const long long rx64 = px - X0, ry64 = py - Y0;
-        const int rx = (int)(rx64 < -kLim ? -kLim : (rx64 > kLim ? kLim : rx64));
-        const int ry = (int)(ry64 < -kLim ? -kLim : (ry64 > kLim ? kLim : ry64));
-        const int D2 = (int)d2, w8 = 8 * u;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const int y0 = r * u, y1 = y0 + u - 1;
-            const int gy = ry < y0 ? y0 - ry : (ry > y1 ? ry - y1 : 0);
-            if (gy > 46340) continue;            // gy^2 > 2^31 > D2
-            const int v = D2 - gy * gy;
-            if (v < 0) continue;
-            const int w = (int)sqrtf((float)v) + 1;
-            const int lo = rx - w, hi = rx + w;
-            if (hi < 0 || lo >= w8) continue;
-            int a = 0, e = 7;
-            if (lo > 0) {
-                a = (int)((float)lo * inv_u);
-                if (a * u > lo) --a; else if ((a + 1) * u <= lo) ++a;
-            }
-            if (hi < w8) {
-                e = (int)((float)hi * inv_u);
-                if (e * u > hi) --e; else if ((e + 1) * u <= hi) ++e;
-            }
-            const uint32_t row = (0xFFu >> (7 - e)) & (0xFFu << a) & 0xFFu;
-            if (r < 4) mlo |= row << (8 * r); else mhi |= row << (8 * (r - 4));
-        }
-    }
-    mlo = __reduce_or_sync(0xffffffffu, mlo);
-    mhi = __reduce_or_sync(0xffffffffu, mhi);
-    return ((uint64_t)mhi << 32) | mlo;
-}
-
 // A candidate block with at most this many points is scanned whole, which
 // costs less than its bin mask.
 constexpr int kFarWholeBlock = 24;
@@ -784,10 +750,6 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
     cell_range((xlo + xhi) / 2, (xhi - xlo) / 2 + 1, gx0, u2, g.n2x, sx0, sx1);
     cell_range((ylo + yhi) / 2, (yhi - ylo) / 2 + 1, gy0, u2, g.n2y, sy0, sy1);
     if (sx0 > sx1 || sy0 > sy1) return;
-    // the 32-bit chord masks apply when the cells are small enough (and,
-    // per call, every bound is below 2^31)
-    const bool fast1 = 8 * u1 < (1LL << 30), fast0 = 8 * bs < (1LL << 30);
-    const float inv_u1 = 1.0f / (float)u1, inv_bs = 1.0f / (float)bs;
     const long long cyy = warp_min64(act ? py : LLONG_MAX);
     int csy = udiv32((cyy < gy0 ? gy0 : cyy) - gy0, u2);
     csy = csy < sy0 ? sy0 : (csy > sy1 ? sy1 : csy);
@@ -805,8 +767,7 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
             if (!__any_sync(full, need_s)) continue;
             // 32-bit square roots are within one unit while every bound is below 2^31
             bool small = __all_sync(full, !act || b.d2 < (1LL << 31));
-            uint64_t cand = sm & (small && fast1 ? chord_union8(act, px, py, b.d2, SX0, SY0, (int)u1, inv_u1)
-                                                 : chord_mask8(act, px, py, b.d2, SX0, SY0, u1, small));
+            uint64_t cand = sm & chord_mask8(act, px, py, b.d2, SX0, SY0, u1, small);
             while (cand) {
                 const int m = ffs64(cand);
                 cand &= cand - 1;
@@ -824,8 +785,7 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
                 }
                 const uint64_t bm = __ldg(&bmask[blk]);
                 small = __all_sync(full, !act || b.d2 < (1LL << 31));
-                uint64_t qc = bm & (small && fast0 ? chord_union8(act, px, py, b.d2, BX0, BY0, (int)bs, inv_bs)
-                                                   : chord_mask8(act, px, py, b.d2, BX0, BY0, bs, small));
+                uint64_t qc = bm & chord_mask8(act, px, py, b.d2, BX0, BY0, bs, small);
                 while (qc) {
                     const int l = ffs64(qc);
                     qc &= qc - 1;
@@ -910,7 +870,9 @@ __global__ void __launch_bounds__(256, 4) k_near_far(BatchTables bt, const int4*
             settle_pixel(T, i, j, b, pix, site);
             R2 = r2_of(b.d2, (long long)T.cs * T.cs, T.r2cap);
         }
-        warp_stats(T, R2, sc + t, blockIdx.x * 3 + (threadIdx.x >> 5), b.nev, true);
+        StatAcc acc;
+        acc.add(T, R2, b.nev);
+        acc.flush(sc + t, blockIdx.x * 3 + (threadIdx.x >> 5), true);
     }
 }
 
