@@ -187,6 +187,30 @@ def cpu_baseline(xyz, side, window, seed_note):
                       f"single-thread C oracle (k-d tree nearest site + row-span scatter), {dt:.2f} s"}
 
 
+OPS_PER_EVAL = 5   # a candidate evaluation: 2 subtractions, 1 multiply, 1 multiply-add, 1 compare
+
+
+def ops_roofline(peaks, evals_dense, evals_far, spans, ms_dense, ms_far, ms_spans):
+    """Op-count rooflines of the three kernels that dominate a step, against
+    the device's measured throughput of the operation bounding each
+    (dnni_measure_peaks): integer ops of the distance evaluations for the
+    nearest-site kernels, shared-memory atomics of the span window (two per
+    marker, two markers per span row; rows clipped by the grid included)."""
+    def one(work, ms, peak, unit, note):
+        ach = work / (ms / 1000.0) if ms > 0 else 0.0
+        return {"work": int(work), "ms": round(ms, 3), "achieved": ach, "peak": peak, "unit": unit,
+                "frac_ops": ach / peak if peak else None, "work_def": note}
+    return {
+        "peaks_measured": peaks,
+        "k_near_dense": one(OPS_PER_EVAL * evals_dense, ms_dense, peaks["int_ops_per_s"], "int32 ops/s",
+                            f"{OPS_PER_EVAL} integer ops per candidate distance evaluation"),
+        "k_near_far": one(OPS_PER_EVAL * evals_far, ms_far, peaks["int_ops_per_s"], "int32 ops/s",
+                          f"{OPS_PER_EVAL} integer ops per candidate distance evaluation (seeds and disc search)"),
+        "k_scatter_window": one(4 * spans, ms_spans, peaks["smem_atomics_per_s"], "smem atomics/s",
+                                "4 shared-memory atomic adds per span row (z and count at both ends)"),
+    }
+
+
 def fp64_errors(oracle, ref, h, z_scale=0.01, z_offset=0.0):
     """Max and RMS |h - h_FP64| over the cells with data, h_FP64 from the
     oracle's exact integer sums (the FP64 checker)."""
@@ -218,24 +242,35 @@ def window_accuracy(oracle, h_grid, xyz, x0, y0, win, halo, cell=100, origin=(0,
             "max_abs_err_m": mx, "rms_err_m": rms}
 
 
-def depth_disagreement(oracle, cases, budget_s):
-    """The reference's float32 depth-buffer site choice (emulated by the
-    oracle) against the exact nearest site, over (wp, xyz) cases until the
-    budget is spent: fractions of raster pixels."""
+def depth_disagreement(oracle, cases, budget_s, max_pixels=2_000_000, max_side=384):
+    """The reference's site choice by float32 lifted-plane depth in a 32-bit
+    depth buffer (GL_DEPTH_COMPONENT32, nni.cpp:420-424; emulated by the
+    oracle, LEQUAL with the later-drawn site winning) against the exact
+    nearest site, over (wp, xyz) cases of at most max_side cells a side until
+    the budget or the pixel count is spent: fractions of raster pixels.  The
+    emulation considers the sites whose exact squared distance lies within
+    2^-15 * halfwidth^2 of the nearest one; float32 depths (values up to 8,
+    a few ulp of error) cannot order sites much closer than that."""
     pix = site = zd = 0
     used = 0
+    sides = []
     t0 = time.perf_counter()
     for wp, xyz in cases:
-        if time.perf_counter() - t0 >= budget_s:
+        if time.perf_counter() - t0 >= budget_s or pix >= max_pixels:
             break
-        r = oracle.gl_disagreement(wp, xyz)
+        if max(wp.ncols, wp.nrows) > max_side:
+            continue
+        hw = (wp.nrows - 1) * wp.cell_size / 2.0
+        slack = int(max(2.0 ** -15 * hw * hw, 4.0 * wp.cell_size * wp.cell_size))
+        r = oracle.gl_disagreement(wp, xyz, depth_bits=32, slack_units2=slack)
         pix += r["pixels"]
         site += r["site_differs"]
         zd += r["z_differs"]
         used += 1
+        sides.append(int(wp.ncols))
     n = max(pix, 1)
-    return {"cases": used, "pixels": pix, "site_frac": site / n, "z_frac": zd / n, "depth_bits": 24,
-            "seconds": round(time.perf_counter() - t0, 1)}
+    return {"cases": used, "pixels": pix, "site_frac": site / n, "z_frac": zd / n, "depth_bits": 32,
+            "tile_sides": sides, "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def run_reference_tile4096(args, world, rank):
@@ -323,12 +358,14 @@ def run_engine_tile4096(args, world, rank, local):
         clk.mark("t_start")
         ev0.record(stream)
         for _ in range(args.steps):
-            st = eng.interpolate_device(wp, d_xyz, npts, d_h, stream=sp, stats=True)
-            phases.append(st)
+            eng.interpolate_device(wp, d_xyz, npts, d_h, stream=sp, stats=False)
         ev1.record(stream)
         torch.cuda.synchronize()
         clk.mark("t_end")
     barrier()
+    # per-phase device times and counts from untimed calls with statistics
+    for _ in range(2):
+        phases.append(eng.interpolate_device(wp, d_xyz, npts, d_h, stream=sp, stats=True))
     ms = ev0.elapsed_time(ev1)
     ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -360,7 +397,10 @@ def run_engine_tile4096(args, world, rank, local):
         peak, peak_kind = peaks()
         ms_step = ms_max / args.steps
         ph = {k: sum(getattr(p, k) for p in phases) / len(phases)
-              for k in ("ms_bin", "ms_nearest", "ms_scatter", "ms_finalize", "ms_total")}
+              for k in ("ms_bin", "ms_nearest", "ms_dense", "ms_far", "ms_scatter", "ms_finalize", "ms_total")}
+        last = phases[-1]
+        ops = ops_roofline(engine.measure_peaks(local), last.evals_dense, last.evals_far, last.spans, ph["ms_dense"],
+                           ph["ms_far"], ph["ms_scatter"])
         alg_bytes = 12 * npts + 4 * cells
         achieved = alg_bytes / (ms_step / 1000.0) / 1e9
         dom = max(("ms_bin", "ms_nearest", "ms_scatter", "ms_finalize"), key=lambda k: ph[k])
@@ -380,7 +420,7 @@ def run_engine_tile4096(args, world, rank, local):
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes": alg_bytes, "dominant_phase": dom,
-                         "phase_ms": {k: round(v, 4) for k, v in ph.items()}},
+                         "phase_ms": {k: round(v, 4) for k, v in ph.items()}, "ops": ops},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(xyz.nbytes),
                     "d2h_bytes_per_step": int(cells * 4)},
             "gpu_launches": KERNELS_PER_CALL * args.steps,
@@ -600,11 +640,15 @@ def run_engine_mixed(args, world, rank, local):
     value = nout * args.steps * world / (ms_max / 1000.0)
     b.close()
 
-    # per-phase device times from one run without the graph
+    # per-phase device times from one run without the graph, and the
+    # measured peaks of the operations that bound the largest kernels
     with eng.batch(tiles, use_graph=False, order_by_cost=True, **opts) as bp:
         bp.run_device(d_xyz, d_h, stream=sp)
         ph = bp.run_device(d_xyz, d_h, stream=sp, stats=True)
-    phases = {k: round(getattr(ph, k), 4) for k in ("ms_bin", "ms_nearest", "ms_scatter", "ms_finalize", "ms_total")}
+    phases = {k: round(getattr(ph, k), 4) for k in ("ms_bin", "ms_nearest", "ms_dense", "ms_far", "ms_scatter",
+                                                     "ms_finalize", "ms_total")}
+    ops = ops_roofline(engine.measure_peaks(local), ph.evals_dense, ph.evals_far, ph.spans, ph.ms_dense, ph.ms_far,
+                       ph.ms_scatter)
 
     # plain form: one dnni_interpolate_segment_device call per tile, same
     # tiles, same stream, no statistics (the call's only wait is the one it
@@ -689,13 +733,15 @@ def run_engine_mixed(args, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": f"whole hot path per batch ({KERNELS_PER_BATCH} launches)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": alg_bytes,
-                         "dominant_phase": dom, "phase_ms": phases},
+                         "dominant_phase": dom, "phase_ms": phases, "ops": ops},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(xyz.nbytes),
                     "d2h_bytes_per_step": int(nout * 4)},
             "gpu_launches": KERNELS_PER_BATCH * args.steps,
             "clocks": clk.summary(),
             "work": {"span_pixels": st0.big_pixels, "spans": st0.spans, "max_r2": st0.max_r2,
-                     "nodata_cells": nod},
+                     "nodata_cells": nod, "evals_dense": ph.evals_dense, "evals_far": ph.evals_far,
+                     "span_radius_hist": {"bucket_lo": [0] + [1 << (k - 1) for k in range(1, 16)],
+                                          "spans": list(ph.span_hist)}},
         }
         if not args.no_cpu_baseline:
             from oracle import oracle

@@ -106,6 +106,8 @@ typedef struct dnni_stats {
                                span-path pixels with floor(sqrt(R2)) in
                                [2^(k-1), 2^k) (k = 15: all larger); filled
                                by statistics runs without a graph */
+    double ms_dense;        /* of ms_nearest: the ring search (k_near_dense) */
+    double ms_far;          /* and the far pass after it */
 } dnni_stats;
 
 /* ---- lifecycle: nni::init / nni::cleanup (nni.h:83-85, nni.cpp:563-598) ---- */
@@ -508,6 +510,27 @@ dnni_status dnni_write_grid_bin(const char *path, const float *h, int32_t ncols,
 dnni_status dnni_clear(dnni_ctx *ctx);
 /* Print accumulated per-phase device times to stdout (needs DNNI_F_TIMING). */
 dnni_status dnni_print_times(dnni_ctx *ctx);
+
+/* ---- measured peaks of the operations that bound the hot path ----
+ *
+ * Calibration beside dnni::printTimes (nni.cpp:554-560): the throughput this
+ * device reaches on the operations that bound the hot path's kernels, each
+ * from a microbenchmark kernel timed with CUDA events on every SM: 32-bit
+ * integer multiply-adds (the distance evaluations of the nearest-site
+ * search), conflict-free 32-bit shared-memory atomic adds (the span
+ * window's markers) and coalesced 64-bit global atomic adds on an
+ * L2-resident buffer (the window's flush and the direct span path).  The
+ * op-count rooflines divide the kernels' counted work by these.  Allocates
+ * about 32 MB for the duration of the call. */
+typedef struct dnni_peaks {
+    double int_ops_per_s;          /* lane multiply-adds per second */
+    double smem_atomics_per_s;     /* lane atomic adds per second */
+    double l2_red64_per_s;         /* lane atomic adds per second */
+    double sm_clock_mhz;           /* the device's nominal SM clock */
+    int32_t sm_count, pad;
+} dnni_peaks;
+
+dnni_status dnni_measure_peaks(int32_t device, dnni_peaks *out);
 
 /* ---- pinned host memory for the host-buffer entry points ---- */
 

@@ -156,7 +156,8 @@ void launch_prologue(const HostBatch& hb, const BatchTables& bt, const DevArrays
 
 // Launch sequence, part 2: binning, nearest sites, spans, stencil, finalize.
 // Needs no host synchronisation (a batch's whole sequence can be captured).
-// ev[0..2] (optional) mark the ends of binning, nearest sites and spans.
+// ev[0..2] (optional) mark the ends of binning, nearest sites and spans, and
+// ev[4] the end of the ring search (k_near_dense) inside the nearest sites.
 // sites_only: stop after the nearest-site kernels (the site map is the result).
 void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a, const int32_t* d_xyz,
                  const uint32_t* d_gid, float* d_h, uint32_t* d_site, int sms, cudaStream_t st,
@@ -181,6 +182,7 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     const int nrt = hb.rt_base.back();
     k_near_dense<<<nrt, dim3(32, 8), kDenseSmem, st>>>(bt, a.sorted, a.start, a.pix, d_site, a.far, a.sc, a.ctr,
                                                        hb.far_blocks);
+    if (ev) cudaEventRecord(ev[4], st);
     if (nchunk > 0)
         k_near_far<<<sms * 6, 256, 0, st>>>(bt, a.sorted, a.start, a.bmask, a.smask, a.near, a.far, a.pix, d_site,
                                             a.sc, a.ctr);
@@ -335,6 +337,10 @@ static dnni_status run_device(dnni_ctx* c, const dnni_workpackage* wp, const int
             stats->ms_scatter = ms[2];
             stats->ms_finalize = ms[3];
             stats->ms_total = ms[0] + ms[1] + ms[2] + ms[3];
+            float md = 0;
+            cudaEventElapsedTime(&md, c->ev[1], c->ev[5]);
+            stats->ms_dense = md;
+            stats->ms_far = ms[1] - md;
         }
     }
     if (stats) {
@@ -660,6 +666,10 @@ dnni_status dnni_batch_run_device(dnni_batch* b, const int32_t* d_xyz, const uin
             stats->ms_nearest = ph[1];
             stats->ms_scatter = ph[2];
             stats->ms_finalize = ph[3];
+            float md = 0;
+            cudaEventElapsedTime(&md, c->ev[1], c->ev[5]);
+            stats->ms_dense = md;
+            stats->ms_far = ph[1] - md;
         }
         if (c->h_ctr->err & kErrRange)
             return set_err(c, DNNI_E_RANGE, "a point lies beyond its tile's declared extent or the coordinate range");
@@ -1200,3 +1210,4 @@ extern "C" dnni_status dnni_interpolate_segment_device_noalloc(const dnni_workpa
 #include "dnni_server.cuh"
 #include "dnni_compat.cuh"
 #include "dnni_spacetime.cuh"
+#include "dnni_calibrate.cuh"

@@ -58,7 +58,7 @@ class Stats(ctypes.Structure):
         ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
         ("max_r2", ctypes.c_int32), ("packed", ctypes.c_int32), ("bin_size", ctypes.c_int32),
         ("pad", ctypes.c_int32), ("evals_dense", ctypes.c_int64), ("evals_far", ctypes.c_int64),
-        ("span_hist", ctypes.c_int64 * 16),
+        ("span_hist", ctypes.c_int64 * 16), ("ms_dense", ctypes.c_double), ("ms_far", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -163,6 +163,15 @@ class CompatWP(ctypes.Structure):
                 ("grid_origin_y", ctypes.c_float), ("nrows", ctypes.c_int32), ("ncols", ctypes.c_int32)]
 
 
+class Peaks(ctypes.Structure):
+    _fields_ = [("int_ops_per_s", ctypes.c_double), ("smem_atomics_per_s", ctypes.c_double),
+                ("l2_red64_per_s", ctypes.c_double), ("sm_clock_mhz", ctypes.c_double),
+                ("sm_count", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("span_window", ctypes.c_int32)]
@@ -197,6 +206,7 @@ _SIGS = {
     "dnni_print_times": ([_P], ctypes.c_int),
     "dnni_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(_P)], ctypes.c_int),
     "dnni_host_free": ([_P], ctypes.c_int),
+    "dnni_measure_peaks": ([ctypes.c_int32, ctypes.POINTER(Peaks)], ctypes.c_int),
     "dnni_batch_create": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, ctypes.POINTER(BatchOptions),
                            ctypes.POINTER(_P)], ctypes.c_int),
     "dnni_batch_run_device": ([_P, _P, _P, _P, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
@@ -247,6 +257,14 @@ def lib():
 
 def exported_symbols():
     return list(_SIGS)
+
+
+def measure_peaks(device=0):
+    """dnni_measure_peaks -> dict: measured integer multiply-add, shared-memory
+    atomic and L2 64-bit reduction throughput of the device (lane ops/s)."""
+    p = Peaks()
+    _rc(lib().dnni_measure_peaks(int(device), ctypes.byref(p)), "dnni_measure_peaks")
+    return p.as_dict()
 
 
 def make_wp(ncols, nrows, cell_size, origin_x=0, origin_y=0, raster=None, z_scale=0.01, z_offset=0.0,

@@ -44,6 +44,7 @@ def test_init_without_device_fails_cleanly():
 def test_null_arguments_rejected():
     from terranni_b200 import engine
     L = engine.lib()
+    assert L.dnni_measure_peaks(0, None) == 1
     assert L.dnni_init(None, None) == 1
     assert L.dnni_destroy(None) == 1
     assert L.dnni_last_error(None) == b"context is NULL"
