@@ -268,6 +268,13 @@ typedef struct dnni_segment {
     double z_scale, z_offset;
     float nodata;
     int32_t small_radius;          /* 0 = the context's setting */
+    int32_t part, parts;           /* parts > 1: run only the tiles of part `part`
+                                      (0 <= part < parts), a contiguous range of
+                                      the row-major tiles balanced by cost
+                                      (cells + points, dnni_partition_contiguous),
+                                      and write only their cells; the other
+                                      parts' calls, on other GPUs, fill the rest.
+                                      0 or 1 = every tile */
 } dnni_segment;
 
 typedef struct dnni_segment_stats {
@@ -281,6 +288,12 @@ typedef struct dnni_segment_stats {
     int32_t max_halo;              /* largest raster halo any tile needed */
     int32_t batches;               /* launch sequences run */
 } dnni_segment_stats;
+
+/* Splits n items with non-negative costs into `parts` contiguous ranges of
+ * about equal total cost: part p is [first[p], first[p+1]), first[0] = 0,
+ * first[parts] = n.  Host code only (no device needed); the same inputs give
+ * the same ranges on every rank. */
+dnni_status dnni_partition_contiguous(const int64_t *cost, int32_t n, int32_t parts, int32_t *first);
 
 /* h_out: nrows x ncols floats, row-major, row 0 = lowest y; h_site (optional):
  * nrows x ncols uint32 site ids. */

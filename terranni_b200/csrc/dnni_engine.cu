@@ -560,6 +560,26 @@ dnni_status dnni_print_times(dnni_ctx* c) {
     return DNNI_OK;
 }
 
+dnni_status dnni_partition_contiguous(const int64_t* cost, int32_t n, int32_t parts, int32_t* first) {
+    if (!first || parts < 1 || n < 0 || (n > 0 && !cost)) return DNNI_E_INVAL;
+    long double total = 0;
+    for (int32_t k = 0; k < n; ++k) {
+        if (cost[k] < 0) return DNNI_E_INVAL;
+        total += (long double)cost[k];
+    }
+    // boundary p: where the running cost is closest to p / parts of the total
+    first[0] = 0;
+    int32_t k = 0;
+    long double run = 0;
+    for (int32_t p = 1; p < parts; ++p) {
+        const long double goal = total * p / parts;
+        while (k < n && run + (long double)cost[k] / 2 <= goal) run += (long double)cost[k++];
+        first[p] = k;
+    }
+    first[parts] = n;
+    return DNNI_OK;
+}
+
 dnni_status dnni_host_alloc(size_t bytes, void** out) {
     if (!out) return DNNI_E_INVAL;
     if (cudaMallocHost(out, bytes ? bytes : 1) != cudaSuccess) {

@@ -445,31 +445,53 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
         ay0 = std::max(0, T.y0 - T.h[2]);
         ay1 = std::min(s.nrows, T.y1 + T.h[3]);
     };
-    std::vector<SegTile> queue;
+    // the grid's tiles in row-major order, each with a cost (its cells and the
+    // points of the buckets its core touches); a call with parts > 1 runs
+    // the contiguous, cost-balanced range of tiles of its part
+    std::vector<SegTile> cores;
+    std::vector<int64_t> cost;
     for (int y = 0; y < s.nrows; y += s.tile)
         for (int x = 0; x < s.ncols; x += s.tile) {
-            SegTile T{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows), {s.halo, s.halo, s.halo, s.halo},
-                      s.halo};
-            if (s.halo == 0) {
-                for (int k = 0; k < 4; ++k) T.h[k] = 2;
-                for (int it = 0; it < 32; ++it) {
-                    int ax0, ay0, ax1, ay1;
-                    raster_of(T, ax0, ay0, ax1, ay1);
-                    const int hs[4] = {bound_halo(ax0, ay0, std::min(ax0 + 2, ax1), ay1),
-                                       bound_halo(std::max(ax1 - 2, ax0), ay0, ax1, ay1),
-                                       bound_halo(ax0, ay0, ax1, std::min(ay0 + 2, ay1)),
-                                       bound_halo(ax0, std::max(ay1 - 2, ay0), ax1, ay1)};
-                    bool grew = false;
-                    for (int k = 0; k < 4; ++k)
-                        if (hs[k] > T.h[k]) { T.h[k] = hs[k]; grew = true; }
-                    if (!grew) break;
-                }
+            const SegTile T{x, y, std::min(x + s.tile, s.ncols), std::min(y + s.tile, s.nrows),
+                            {s.halo, s.halo, s.halo, s.halo}, s.halo};
+            const int cbx0 = T.x0 / kSegBucketCells, cbx1 = (T.x1 - 1) / kSegBucketCells;
+            int64_t pts = 0;
+            for (int by = T.y0 / kSegBucketCells; by <= (T.y1 - 1) / kSegBucketCells; ++by)
+                pts += start[(size_t)by * nbx + cbx1 + 1] - start[(size_t)by * nbx + cbx0];
+            cores.push_back(T);
+            cost.push_back((int64_t)(T.x1 - T.x0) * (T.y1 - T.y0) + pts);
+        }
+    int k0 = 0, k1 = (int)cores.size();
+    if (s.parts > 1) {
+        std::vector<int32_t> first((size_t)s.parts + 1);
+        if ((rs = dnni_partition_contiguous(cost.data(), (int32_t)cost.size(), s.parts, first.data())))
+            return set_err(c, rs, "tile partition");
+        k0 = first[s.part];
+        k1 = first[s.part + 1];
+    }
+    std::vector<SegTile> queue;
+    for (int kq = k0; kq < k1; ++kq) {
+        SegTile T = cores[kq];
+        if (s.halo == 0) {
+            for (int k = 0; k < 4; ++k) T.h[k] = 2;
+            for (int it = 0; it < 32; ++it) {
                 int ax0, ay0, ax1, ay1;
                 raster_of(T, ax0, ay0, ax1, ay1);
-                T.hp = bound_halo(ax0, ay0, ax1, ay1);
+                const int hs[4] = {bound_halo(ax0, ay0, std::min(ax0 + 2, ax1), ay1),
+                                   bound_halo(std::max(ax1 - 2, ax0), ay0, ax1, ay1),
+                                   bound_halo(ax0, ay0, ax1, std::min(ay0 + 2, ay1)),
+                                   bound_halo(ax0, std::max(ay1 - 2, ay0), ax1, ay1)};
+                bool grew = false;
+                for (int k = 0; k < 4; ++k)
+                    if (hs[k] > T.h[k]) { T.h[k] = hs[k]; grew = true; }
+                if (!grew) break;
             }
-            queue.push_back(T);
+            int ax0, ay0, ax1, ay1;
+            raster_of(T, ax0, ay0, ax1, ay1);
+            T.hp = bound_halo(ax0, ay0, ax1, ay1);
         }
+        queue.push_back(T);
+    }
     const int64_t ntiles = (int64_t)queue.size();
     const auto t_tiles = clk::now();
     int64_t runs = 0, d2h = 0;
@@ -702,6 +724,8 @@ extern "C" dnni_status dnni_segment_run(dnni_ctx* c, const dnni_segment* sp, con
     if ((long long)s.ncols * s.cell_size >= (1LL << 30) || (long long)s.nrows * s.cell_size >= (1LL << 30))
         return set_err(c, DNNI_E_RANGE, "grid extent must stay below 2^30 LAS units");
     if ((uint64_t)n >= 0xFFFFFFFFull) return set_err(c, DNNI_E_INVAL, "more points than 32-bit site ids can name");
+    if (s.parts < 0 || s.parts > 65536 || (s.parts > 1 && (s.part < 0 || s.part >= s.parts)))
+        return set_err(c, DNNI_E_INVAL, "part must lie in [0, parts)");
     // buffers stay with the context (grow-only) for the next call; dnni_clear
     // and dnni_destroy free them
     const dnni_status rs = segment_run(c, s, h_xyz, n, h_out, h_site, stats, c->seg, c->seg_scr);

@@ -88,7 +88,8 @@ class Segment(ctypes.Structure):
                 ("origin_x", ctypes.c_int32), ("origin_y", ctypes.c_int32), ("tile", ctypes.c_int32),
                 ("halo", ctypes.c_int32), ("tiles_per_batch", ctypes.c_int32),
                 ("z_scale", ctypes.c_double), ("z_offset", ctypes.c_double),
-                ("nodata", ctypes.c_float), ("small_radius", ctypes.c_int32)]
+                ("nodata", ctypes.c_float), ("small_radius", ctypes.c_int32),
+                ("part", ctypes.c_int32), ("parts", ctypes.c_int32)]
 
 
 class SegmentStats(ctypes.Structure):
@@ -207,6 +208,7 @@ _SIGS = {
     "dnni_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(_P)], ctypes.c_int),
     "dnni_host_free": ([_P], ctypes.c_int),
     "dnni_measure_peaks": ([ctypes.c_int32, ctypes.POINTER(Peaks)], ctypes.c_int),
+    "dnni_partition_contiguous": ([_P, ctypes.c_int32, ctypes.c_int32, _P], ctypes.c_int),
     "dnni_batch_create": ([_P, ctypes.POINTER(Tile), ctypes.c_int32, ctypes.POINTER(BatchOptions),
                            ctypes.POINTER(_P)], ctypes.c_int),
     "dnni_batch_run_device": ([_P, _P, _P, _P, _P, _P, ctypes.POINTER(Stats)], ctypes.c_int),
@@ -257,6 +259,16 @@ def lib():
 
 def exported_symbols():
     return list(_SIGS)
+
+
+def partition_contiguous(costs, parts):
+    """dnni_partition_contiguous -> first (parts + 1 ints): part p owns items
+    [first[p], first[p+1]) of a cost-balanced contiguous split."""
+    c = np.ascontiguousarray(costs, dtype=np.int64)
+    first = np.zeros(int(parts) + 1, np.int32)
+    _rc(lib().dnni_partition_contiguous(c.ctypes.data if c.size else None, c.size, int(parts),
+                                        first.ctypes.data), "dnni_partition_contiguous")
+    return first
 
 
 def measure_peaks(device=0):
@@ -399,12 +411,15 @@ class Engine:
                 rep.as_dict())
 
     def segment_run(self, xyz, ncols, nrows, cell_size, origin=(0, 0), tile=0, halo=0, tiles_per_batch=0,
-                    z_scale=0.01, z_offset=0.0, nodata=-9999.0, small_radius=0, site=False, out_h=None):
-        """dnni_segment_run: the whole grid from host points in tiles with
-        halos -> (h, site map or None, SegmentStats)."""
+                    z_scale=0.01, z_offset=0.0, nodata=-9999.0, small_radius=0, site=False, out_h=None, part=0,
+                    parts=0):
+        """dnni_segment_run: the whole grid (or, with parts > 1, the tiles of
+        part `part`) from host points in tiles with halos -> (h, site map or
+        None, SegmentStats)."""
         xyz = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1, 3)
         sg = Segment(int(ncols), int(nrows), int(cell_size), int(origin[0]), int(origin[1]), int(tile), int(halo),
-                     int(tiles_per_batch), float(z_scale), float(z_offset), float(nodata), int(small_radius))
+                     int(tiles_per_batch), float(z_scale), float(z_offset), float(nodata), int(small_radius),
+                     int(part), int(parts))
         h = out_h if out_h is not None else np.empty((nrows, ncols), np.float32)
         sm = np.empty((nrows, ncols), np.uint32) if site else None
         st = SegmentStats()

@@ -71,6 +71,28 @@ def test_segment_mosaic_against_the_oracle(eng, oracle):
     assert st.tiles == 12
 
 
+@pytest.mark.parametrize("parts", [2, 3])
+def test_segment_parts_stitch_to_the_whole_grid(eng, parts):
+    # each part's call (here one after another on one GPU; in a multi-GPU
+    # run, one per rank) writes only its own tiles' cells; together the parts
+    # give the whole grid bit for bit, every tile run by exactly one part
+    ncols, nrows = 1000, 760
+    xyz = _cloud(19, ncols, nrows, 250_000, lakes=3)
+    whole, _, st_all = eng.segment_run(xyz, ncols, nrows, 100, tile=200, halo=0, tiles_per_batch=4)
+    h = np.full((nrows, ncols), np.nan, np.float32)
+    tiles = 0
+    for p in range(parts):
+        before = np.isnan(h).sum()
+        _, _, st = eng.segment_run(xyz, ncols, nrows, 100, tile=200, halo=0, tiles_per_batch=4, out_h=h,
+                                   part=p, parts=parts)
+        assert st.tiles > 0 and np.isnan(h).sum() < before
+        if p < parts - 1:
+            assert np.isnan(h).any()
+        tiles += st.tiles
+    assert tiles == st_all.tiles == 5 * 4
+    assert np.array_equal(h.view(np.uint32), whole.view(np.uint32))
+
+
 def test_segment_reruns_tiles_whose_halo_is_too_small(eng):
     ncols = nrows = 600
     xyz = _cloud(3, ncols, nrows, 40_000, lakes=4)
