@@ -62,6 +62,10 @@ def parse():
     ap.add_argument("--srv-side", type=float, default=64000.0, help="served: cloud side, metres")
     ap.add_argument("--srv-requests", type=int, default=200, help="served: requests per arrival rate")
     ap.add_argument("--srv-rates", default="20,100,1000,20000", help="served: Poisson arrival rates, 1/s")
+    ap.add_argument("--srv-block-side", type=float, default=16000.0,
+                    help="mixed: side (m) of the cloud of the served block in the default line (0: none)")
+    ap.add_argument("--srv-block-requests", type=int, default=48, help="mixed: requests per rate of the served block")
+    ap.add_argument("--srv-block-rates", default="100,2000", help="mixed: arrival rates of the served block")
     ap.add_argument("--seg-side", type=int, default=32768, help="segment: grid side in cells (1 m)")
     ap.add_argument("--seg-points", type=int, default=1_500_000_000, help="segment: points")
     ap.add_argument("--seg-tile", type=int, default=2048)
@@ -697,6 +701,13 @@ def run_engine_mixed(args, world, rank, local):
     e2e_value = nout * args.steps * world / e2e_s
     h_gpu = h_out[:nout].copy()
     nod = int(np.count_nonzero(h_gpu == np.float32(-9999.0)))
+    served = None
+    if world == 1 and args.srv_block_side > 0:
+        # a bounded serving run beside the batch (outside its timed region)
+        del d_xyz, d_h
+        torch.cuda.empty_cache()
+        eng.clear()
+        served = served_block(eng, args, local)
 
     if rank == 0:
         peak, peak_kind = peaks()
@@ -738,6 +749,7 @@ def run_engine_mixed(args, world, rank, local):
                     "d2h_bytes_per_step": int(nout * 4)},
             "gpu_launches": KERNELS_PER_BATCH * args.steps,
             "clocks": clk.summary(),
+            "served": served,
             "work": {"span_pixels": st0.big_pixels, "spans": st0.spans, "max_r2": st0.max_r2,
                      "nodata_cells": nod, "evals_dense": ph.evals_dense, "evals_far": ph.evals_far,
                      "span_radius_hist": {"bucket_lo": [0] + [1 << (k - 1) for k in range(1, 16)],
@@ -1039,6 +1051,92 @@ def run_engine_compat(args, world, rank, local):
 # served: DEM requests against a resident cloud
 # ---------------------------------------------------------------------------
 
+def serve_rates(srv, reqs, outs, rates, rng, max_over_ranks=lambda x: x, world=1, barrier=None):
+    """For each arrival rate, a Poisson stream of the requests submitted by a
+    client thread at their arrival times and collected in order; latency =
+    submit -> heights in host memory.  Per rate: cells/s over the stream's
+    span, p50/p99/max latency, mean batch size, the median queueing delay,
+    and the device time line of the server's slots over the stream (time
+    busy, time with two or more slots' batches running at once)."""
+    import numpy as np
+    sizes = [r["ncols"] * r["nrows"] for r in reqs]
+    results = []
+    for rate in rates:
+        if barrier is not None:
+            barrier()
+        st0 = srv.stats()
+        gaps = rng.exponential(1.0 / rate, len(reqs))
+        arrive = np.cumsum(gaps) - gaps[0]
+        tickets = [None] * len(reqs)
+        lat = [None] * len(reqs)
+        ready = threading.Semaphore(0)
+
+        def client():
+            base = time.perf_counter()
+            for k, r in enumerate(reqs):
+                d = base + arrive[k] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets[k] = srv.submit(**r, out_h=outs[k])
+                ready.release()
+
+        c = threading.Thread(target=client)
+        t_first = time.perf_counter()
+        c.start()
+        for k in range(len(reqs)):
+            ready.acquire()
+            _, _, res = srv.wait(tickets[k], timeout=600)
+            lat[k] = res
+        t_last = time.perf_counter()
+        c.join()
+        st1 = srv.stats()
+        span = max_over_ranks(t_last - t_first)
+        cells = sum(sizes)
+        ms = np.array([x["ms_latency"] for x in lat])
+        busy = st1["ms_device_busy"] - st0["ms_device_busy"]
+        overlap = st1["ms_device_overlap"] - st0["ms_device_overlap"]
+        results.append({"rate_per_s": rate, "requests": len(reqs), "cells": cells,
+                        "cells_per_s": cells * world / span, "p50_ms": float(np.percentile(ms, 50)),
+                        "p99_ms": float(np.percentile(ms, 99)), "max_ms": float(ms.max()),
+                        "mean_batch": float(np.mean([x["batch_size"] for x in lat])),
+                        "queue_p50_ms": float(np.percentile([x["ms_queue"] for x in lat], 50)),
+                        "device_busy_frac": busy / (1000.0 * span) if span > 0 else None,
+                        "slot_overlap_frac": overlap / busy if busy > 0 else 0.0})
+    return results
+
+
+def served_block(eng, args, local):
+    """A bounded serving run for the default bench line: a cloud at the
+    served configuration's density (0.49 points/m^2, fBm terrain, clusters,
+    lakes of 50-400 m) over a smaller area, requests drawn as there (side
+    log-uniform 128 m - 8 km, capped by the area; 0.5/1/2 m cells) at two
+    Poisson rates, and two served windows checked against the oracle."""
+    import numpy as np
+    import torch
+    from terranni_b200 import synth
+    side_m, n = args.srv_block_side, int(round(0.4883 * args.srv_block_side ** 2))
+    t0 = time.perf_counter()
+    xyz = torch.empty((n, 3), dtype=torch.int32, pin_memory=True).numpy()
+    synth.config5(seed=BASE_SEED + 15, n=n, side_m=side_m, out=xyz)
+    gen_s = time.perf_counter() - t0
+    reqs = synth.served_requests(args.srv_block_requests, seed=BASE_SEED + 16, side_m=side_m)
+    sizes = [r["ncols"] * r["nrows"] for r in reqs]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    pool = torch.empty(int(offs[-1]), dtype=torch.float32, pin_memory=True).numpy()
+    outs = [pool[offs[k]:offs[k + 1]].reshape(reqs[k]["nrows"], reqs[k]["ncols"]) for k in range(len(reqs))]
+    rates = [float(x) for x in args.srv_block_rates.split(",") if x]
+    with eng.server(xyz) as srv:
+        for k in range(min(3, len(reqs))):                     # warm-up
+            srv.wait(srv.submit(**reqs[k], out_h=outs[k]), timeout=600)
+        results = serve_rates(srv, reqs, outs, rates, np.random.default_rng(BASE_SEED + 17))
+        st = srv.stats()
+    acc = None if args.no_cpu_baseline else served_accuracy(reqs, outs, xyz, 2)
+    return {"cloud_points": n, "cloud_side_m": side_m, "requests_per_rate": len(reqs),
+            "mean_request_cells": float(np.mean(sizes)), "generate_s": round(gen_s, 1),
+            "form": "continuous batching over 2 slots, footprint admission; latency = submit to heights in host memory",
+            "rates": results, "server": st, "accuracy": acc}
+
+
 def served_accuracy(reqs, outs, xyz, count, reach_m=450.0, win=128):
     """The lower-left win x win cells of the `count` smallest requests whose
     window, with a raster halo of reach_m (above the largest nearest-site
@@ -1106,47 +1204,13 @@ def run_engine_served(args, world, rank, local):
     srv = eng.server(xyz)
     rates = [float(x) for x in args.srv_rates.split(",") if x]
     rng = np.random.default_rng(BASE_SEED + 7 + rank)
-    results = []
     with ClockSampler(local) as clk:
         # warm-up: a few requests alone
         for k in range(min(args.warmup, len(reqs))):
             srv.wait(srv.submit(**reqs[k], out_h=outs[k]), timeout=600)
         clk.mark("t_start")
-        for rate in rates:
-            if tdist is not None:
-                tdist.barrier()
-            gaps = rng.exponential(1.0 / rate, len(reqs))
-            arrive = np.cumsum(gaps) - gaps[0]
-            tickets = [None] * len(reqs)
-            lat = [None] * len(reqs)
-            ready = threading.Semaphore(0)
-
-            def client():
-                base = time.perf_counter()
-                for k, r in enumerate(reqs):
-                    d = base + arrive[k] - time.perf_counter()
-                    if d > 0:
-                        time.sleep(d)
-                    tickets[k] = srv.submit(**r, out_h=outs[k])
-                    ready.release()
-
-            c = threading.Thread(target=client)
-            t_first = time.perf_counter()
-            c.start()
-            for k in range(len(reqs)):
-                ready.acquire()
-                _, _, res = srv.wait(tickets[k], timeout=600)
-                lat[k] = res
-            t_last = time.perf_counter()
-            c.join()
-            span = max_over_ranks(t_last - t_first)
-            cells = sum(sizes)
-            ms = np.array([x["ms_latency"] for x in lat])
-            results.append({"rate_per_s": rate, "requests": len(reqs), "cells": cells,
-                            "cells_per_s": cells * world / span, "p50_ms": float(np.percentile(ms, 50)),
-                            "p99_ms": float(np.percentile(ms, 99)), "max_ms": float(ms.max()),
-                            "mean_batch": float(np.mean([x["batch_size"] for x in lat])),
-                            "queue_p50_ms": float(np.percentile([x["ms_queue"] for x in lat], 50))})
+        results = serve_rates(srv, reqs, outs, rates, rng, max_over_ranks, world,
+                              barrier=(tdist.barrier if tdist is not None else None))
         clk.mark("t_end")
     st = srv.stats()
     srv.close()

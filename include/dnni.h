@@ -354,6 +354,9 @@ typedef struct dnni_server_stats {
     int64_t submitted, completed, failed, batches, cells, points;
     int64_t resident_bytes;        /* the bucketed cloud */
     double ms_build;               /* upload, bucketing and bound at creation */
+    double ms_device_busy;         /* device time with at least one batch running */
+    double ms_device_overlap;      /* of it, time with two or more batches (slots) at once */
+    double ms_device_span;         /* first batch start to last batch end */
 } dnni_server_stats;
 
 dnni_status dnni_server_create(dnni_ctx *ctx, const int32_t *h_xyz, int64_t n, const dnni_server_options *options,

@@ -41,6 +41,7 @@ struct SrvItem {
 struct SrvSlot {
     cudaStream_t st = nullptr;
     cudaEvent_t ev = nullptr;
+    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;   // device start and end of the slot's batch
     DevBuf arena;
     unsigned char* h_out = nullptr;   // pinned landing area for results bound for pageable buffers
     size_t h_out_cap = 0;
@@ -80,6 +81,9 @@ struct dnni_server {
     std::vector<SrvSlot> slots;
     std::thread th;
     int64_t submitted = 0, completed = 0, failed = 0, batches = 0, cells = 0, points = 0;
+    // device time line of the batches: [start, end] in ms after `epoch`
+    cudaEvent_t epoch = nullptr;
+    std::vector<std::pair<double, double>> busy;
 };
 
 namespace {
@@ -294,6 +298,7 @@ dnni_status srv_launch(dnni_server* s, SrvSlot& sl, std::vector<SrvItem>& items,
     }
     if (nt) pack_tables(hb, sl.h_tab);
     if (!chunks.empty()) memcpy(sl.h_tab + tbytes, chunks.data(), sizeof(SegChunk) * chunks.size());
+    CK(cudaEventRecord(sl.ev_t0, st));
     if (nt) CK(cudaMemcpyAsync(a.tables, sl.h_tab, tbytes, cudaMemcpyHostToDevice, st));
     if (!chunks.empty()) {
         CK(cudaMemcpyAsync(dch, sl.h_tab + tbytes, sizeof(SegChunk) * chunks.size(), cudaMemcpyHostToDevice, st));
@@ -375,6 +380,7 @@ dnni_status srv_launch(dnni_server* s, SrvSlot& sl, std::vector<SrvItem>& items,
             }
         }
     }
+    CK(cudaEventRecord(sl.ev_t1, st));
     CK(cudaEventRecord(sl.ev, st));
     // batch position of each running item (no cost order: position = index in tr)
     sl.items = items;
@@ -383,6 +389,13 @@ dnni_status srv_launch(dnni_server* s, SrvSlot& sl, std::vector<SrvItem>& items,
 
 // Completion of a slot's batch: halo checks, results, requeues.
 void srv_finish(dnni_server* s, SrvSlot& sl, cudaError_t e) {
+    if (e == cudaSuccess && s->epoch) {
+        float a = 0, b = 0;
+        if (cudaEventElapsedTime(&a, s->epoch, sl.ev_t0) == cudaSuccess &&
+            cudaEventElapsedTime(&b, s->epoch, sl.ev_t1) == cudaSuccess)
+            s->busy.emplace_back(a, b);
+        cudaGetLastError();
+    }
     int pos = 0;
     for (const SrvItem& it : sl.items) {
         SrvReq& q = s->reqs[it.ticket];
@@ -607,6 +620,7 @@ dnni_status dnni_server_create(dnni_ctx* c, const int32_t* h_xyz, int64_t n, con
         for (SrvSlot& sl : s->slots) {
             if (cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess ||
                 cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreate(&sl.ev_t0) != cudaSuccess || cudaEventCreate(&sl.ev_t1) != cudaSuccess ||
                 cudaMallocHost((void**)&sl.h_ctr, sizeof(BatchCounters)) != cudaSuccess) {
                 cudaGetLastError();
                 rs = set_err(c, DNNI_E_CUDA, "slot streams");
@@ -620,11 +634,18 @@ dnni_status dnni_server_create(dnni_ctx* c, const int32_t* h_xyz, int64_t n, con
             dnni_release(sl.arena, c);
             if (sl.st) cudaStreamDestroy(sl.st);
             if (sl.ev) cudaEventDestroy(sl.ev);
+            if (sl.ev_t0) cudaEventDestroy(sl.ev_t0);
+            if (sl.ev_t1) cudaEventDestroy(sl.ev_t1);
             if (sl.h_ctr) cudaFreeHost(sl.h_ctr);
         }
         s->B.release(c);
         delete s;
         return rs;
+    }
+    if (cudaEventCreate(&s->epoch) != cudaSuccess || cudaEventRecord(s->epoch, st) != cudaSuccess) {
+        cudaGetLastError();
+        if (s->epoch) cudaEventDestroy(s->epoch);
+        s->epoch = nullptr;                      // no device time line, nothing else lost
     }
     s->ms_build = 1000.0 * (now_s() - t0);
     s->th = std::thread(srv_loop, s);
@@ -696,6 +717,25 @@ dnni_status dnni_server_get_stats(dnni_server* s, dnni_server_stats* st) {
     st->points = s->points;
     st->resident_bytes = (int64_t)(s->B.sxyz.cap + s->B.sgid.cap);
     st->ms_build = s->ms_build;
+    // the batches' device time line: time with any slot busy, with two or
+    // more busy at once, and the span from the first start to the last end
+    std::vector<std::pair<double, int>> ends;
+    for (const auto& iv : s->busy) {
+        ends.emplace_back(iv.first, +1);
+        ends.emplace_back(iv.second, -1);
+    }
+    std::sort(ends.begin(), ends.end(), [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+        return x.first < y.first || (x.first == y.first && x.second < y.second);
+    });
+    int depth = 0;
+    double prev = 0;
+    for (const auto& e : ends) {
+        if (depth >= 1) st->ms_device_busy += e.first - prev;
+        if (depth >= 2) st->ms_device_overlap += e.first - prev;
+        depth += e.second;
+        prev = e.first;
+    }
+    if (!ends.empty()) st->ms_device_span = ends.back().first - ends.front().first;
     return DNNI_OK;
 }
 
@@ -715,11 +755,14 @@ dnni_status dnni_server_destroy(dnni_server* s) {
             dnni_release(sl.arena, c);
             if (sl.st) cudaStreamDestroy(sl.st);
             if (sl.ev) cudaEventDestroy(sl.ev);
+            if (sl.ev_t0) cudaEventDestroy(sl.ev_t0);
+            if (sl.ev_t1) cudaEventDestroy(sl.ev_t1);
             if (sl.h_tab) cudaFreeHost(sl.h_tab);
             if (sl.h_out) cudaFreeHost(sl.h_out);
             if (sl.h_sc) cudaFreeHost(sl.h_sc);
             if (sl.h_ctr) cudaFreeHost(sl.h_ctr);
         }
+        if (s->epoch) cudaEventDestroy(s->epoch);
         s->B.release(c);
     }
     delete s;

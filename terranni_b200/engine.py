@@ -127,7 +127,9 @@ class RequestResult(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
                 ("batches", ctypes.c_int64), ("cells", ctypes.c_int64), ("points", ctypes.c_int64),
-                ("resident_bytes", ctypes.c_int64), ("ms_build", ctypes.c_double)]
+                ("resident_bytes", ctypes.c_int64), ("ms_build", ctypes.c_double),
+                ("ms_device_busy", ctypes.c_double), ("ms_device_overlap", ctypes.c_double),
+                ("ms_device_span", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

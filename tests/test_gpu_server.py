@@ -84,6 +84,9 @@ def test_server_results_match_the_definition_and_the_mix(eng, cloud):
         st = srv.stats()
     assert st["completed"] == 2 * len(reqs) and st["failed"] == 0
     assert max(m[2]["batch_size"] for m in mix) > 1
+    # the slots' device time line: busy time, overlap of two slots within it
+    assert st["ms_device_busy"] > 0 and 0 <= st["ms_device_overlap"] <= st["ms_device_busy"] + 1e-6
+    assert st["ms_device_span"] >= st["ms_device_busy"] - 1e-6
     for (ha, sa, ra), (hm, smx, rm) in zip(alone, mix):
         assert np.array_equal(ha.view(np.uint32), hm.view(np.uint32))
         if sa is not None:
