@@ -382,7 +382,7 @@ dnni_status dnni_server_destroy(dnni_server *srv);
 typedef struct dnni_tune_trial {
     int32_t small_radius, bin_target;
     float ms;                          /* device time of one run of the sample */
-    int32_t span_window;
+    int32_t span_window, far_group, pad;
 } dnni_tune_trial;
 
 typedef struct dnni_tune_report {

@@ -995,11 +995,12 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     std::vector<int> order;
     std::vector<dnni_tune_trial> trials;
     cudaStream_t st = c->stream;
-    auto trial = [&](int rs_, int bt_, int ww_, float* ms) -> dnni_status {
+    auto trial = [&](int rs_, int bt_, int ww_, int fg_, float* ms) -> dnni_status {
         dnni_batch_options o = given;
         o.small_radius = rs_;
         o.bin_target = bt_;
         o.span_window = ww_;
+        o.far_group = fg_;
         dnni_status rs = plan_batch(c, smp.data(), m, o, hb, order);
         if (rs) return rs;
         if ((rs = ensure_scratch(c, tscr, scratch_sizes(hb), a))) return rs;
@@ -1016,39 +1017,46 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
         float t = 0;
         CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
         *ms = t / 2;
-        trials.push_back(dnni_tune_trial{rs_, bt_, *ms, ww_});
+        trials.push_back(dnni_tune_trial{rs_, bt_, *ms, ww_, fg_});
         return DNNI_OK;
     };
     dnni_status rs = dnni_ensure(c, hbuf, sizeof(float) * std::max<int64_t>(out, 1));
     const int rs0 = given.small_radius ? given.small_radius : c->s.small_radius;
     const int bt0 = given.bin_target ? given.bin_target : (c->s.bin_target ? c->s.bin_target : 4);
     const int ww0 = given.span_window ? given.span_window : kSpanWindowWords;
+    const int fg0 = given.far_group ? given.far_group : kFarBlocksDefault + 1;
     float ms_default = 0, best_ms = 0;
-    int best_rs = rs0, best_bt = bt0, best_ww = ww0;
-    if (!rs) rs = trial(rs0, bt0, ww0, &ms_default);
+    int best_rs = rs0, best_bt = bt0, best_ww = ww0, best_fg = fg0;
+    if (!rs) rs = trial(rs0, bt0, ww0, fg0, &ms_default);
     best_ms = ms_default;
     // coordinate search: the bin size first, then the stencil/span split,
-    // then the span path's shared-memory window
+    // the span path's shared-memory window, and the far pass's pixel groups
     static const int kBinTargets[] = {2, 3, 4, 6, 8, 12};
     static const int kRadii[] = {1, 2, 3, 4, 5, 6};
     static const int kWindows[] = {1, 2048, 4096, 8192, 12288};   // 1: no window
     for (int bt_ : kBinTargets) {
         if (rs || bt_ == bt0) continue;
         float ms = 0;
-        rs = trial(rs0, bt_, ww0, &ms);
+        rs = trial(rs0, bt_, ww0, fg0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_bt = bt_; }
     }
     for (int r_ : kRadii) {
         if (rs || r_ == rs0 || r_ > kMaxSmallRadius) continue;
         float ms = 0;
-        rs = trial(r_, best_bt, ww0, &ms);
+        rs = trial(r_, best_bt, ww0, fg0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_rs = r_; }
     }
     for (int w_ : kWindows) {
         if (rs || w_ == ww0) continue;
         float ms = 0;
-        rs = trial(best_rs, best_bt, w_, &ms);
+        rs = trial(best_rs, best_bt, w_, fg0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_ww = w_; }
+    }
+    for (int f_ = 1; f_ <= 2; ++f_) {
+        if (rs || f_ == fg0) continue;
+        float ms = 0;
+        rs = trial(best_rs, best_bt, best_ww, f_, &ms);
+        if (!rs && ms < best_ms) { best_ms = ms; best_fg = f_; }
     }
     release_scratch(c, tscr);
     dnni_release(hbuf, c);
@@ -1056,6 +1064,7 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     options->small_radius = best_rs;
     options->bin_target = best_bt;
     options->span_window = best_ww;
+    options->far_group = best_fg;
     if (report) {
         memset(report, 0, sizeof(*report));
         report->ntrials = (int32_t)std::min<size_t>(trials.size(), 32);
@@ -1064,7 +1073,7 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
         for (int k = 0; k < report->ntrials; ++k) {
             report->trial[k] = trials[k];
             if (trials[k].small_radius == best_rs && trials[k].bin_target == best_bt &&
-                trials[k].span_window == best_ww)
+                trials[k].span_window == best_ww && trials[k].far_group == best_fg)
                 report->best = k;
         }
     }

@@ -177,7 +177,7 @@ class Peaks(ctypes.Structure):
 
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
-                ("span_window", ctypes.c_int32)]
+                ("span_window", ctypes.c_int32), ("far_group", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 class TuneReport(ctypes.Structure):
@@ -186,7 +186,8 @@ class TuneReport(ctypes.Structure):
 
     def as_dict(self):
         t = [{"small_radius": self.trial[k].small_radius, "bin_target": self.trial[k].bin_target,
-              "span_window": self.trial[k].span_window, "ms": self.trial[k].ms} for k in range(self.ntrials)]
+              "span_window": self.trial[k].span_window, "far_group": self.trial[k].far_group,
+              "ms": self.trial[k].ms} for k in range(self.ntrials)]
         return {"sample_tiles": self.sample_tiles, "ms_default": self.ms_default,
                 "best": t[self.best] if t else None, "trials": t}
 
@@ -409,8 +410,8 @@ class Engine:
         rep = TuneReport()
         self._check(lib().dnni_batch_autotune(self._h, arr, len(tiles), _ptr(d_xyz), _ptr(d_gid), int(sample_tiles),
                                               ctypes.byref(opt), ctypes.byref(rep)))
-        return ({"small_radius": opt.small_radius, "bin_target": opt.bin_target, "span_window": opt.span_window},
-                rep.as_dict())
+        return ({"small_radius": opt.small_radius, "bin_target": opt.bin_target, "span_window": opt.span_window,
+                 "far_group": opt.far_group}, rep.as_dict())
 
     def segment_run(self, xyz, ncols, nrows, cell_size, origin=(0, 0), tile=0, halo=0, tiles_per_batch=0,
                     z_scale=0.01, z_offset=0.0, nodata=-9999.0, small_radius=0, site=False, out_h=None, part=0,
