@@ -957,10 +957,10 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
                                                         const Scalars* __restrict__ sc,
                                                         unsigned long long* __restrict__ D_all,
                                                         int* __restrict__ Dc_all, int win_words) {
-    extern __shared__ unsigned long long sw[];
+    extern __shared__ int swin[];              // 2 x win_words: z - zbase sums, then counts
     __shared__ int red[8];
     const int t = find_tile(bt.rt_base, bt.ntiles, blockIdx.x);
-    const TileParams& T = bt.tiles[t];
+    const TileParams T = bt.tiles[t];          // by value: the loops below keep what they use in registers
     const int lt = blockIdx.x - __ldg(&bt.rt_base[t]);
     const int ntx = (T.rw + kTileX - 1) / kTileX;
     const int i = (lt % ntx) * kTileX + threadIdx.x;
@@ -1030,8 +1030,9 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
         return;
     }
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    int* sz = reinterpret_cast<int*>(sw);     // z - zbase sums
-    int* scn = sz + win_words;                // counts
+    const int ncols = T.ncols;
+    int* sz = swin;                           // z - zbase sums
+    int* scn = swin + win_words;              // counts
 #pragma unroll 1
     for (int y0 = r0; y0 <= r1; y0 += CH) {
         const int y1 = min(y0 + CH - 1, r1);
@@ -1060,11 +1061,11 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
                     while (w * w > t2) --w;
                 }
                 const int a = max(px - (int)w, 0), b = px + (int)w + 1;
-                if (a > T.ncols - 1 || b <= 0) continue;   // this row's span misses the grid
+                if (a >= ncols || b <= 0) continue;       // this row's span misses the grid
                 const int row = (y - y0) * W - c0;     // a and b lie in [c0, c1]
                 atomicAdd(&sz[row + a], zr);
                 atomicAdd(&scn[row + a], 1);
-                if (b < T.ncols) {
+                if (b < ncols) {
                     atomicAdd(&sz[row + b], -zr);
                     atomicAdd(&scn[row + b], -1);
                 }
@@ -1073,7 +1074,7 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
         __syncthreads();
         // one packed word per touched cell: (sum zrel << K) + count, modulo 2^64
         for (int rr = threadIdx.y; rr <= y1 - y0; rr += 8) {
-            unsigned long long* dst = D + (int64_t)(y0 + rr) * T.ncols + c0;
+            unsigned long long* dst = D + (int64_t)(y0 + rr) * ncols + c0;
             for (int c = threadIdx.x; c < W; c += 32) {
                 const int zs = sz[rr * W + c], cn = scn[rr * W + c];
                 if (zs | cn)
