@@ -1161,7 +1161,7 @@ __global__ void __launch_bounds__(512) k_final(BatchTables bt, const int2* __res
     constexpr int TX = 32, TY = 16, SW = TX + 2 * H, SH = TY + 2 * H;
     __shared__ int2 tile[SH][SW];
     const int t = find_tile(bt.ct_base, bt.ntiles, blockIdx.x);
-    const TileParams& T = bt.tiles[t];
+    const TileParams T = bt.tiles[t];
     const int lt = blockIdx.x - __ldg(&bt.ct_base[t]);
     const int nctx = (T.ncols + TX - 1) / TX;
     const int cx0 = (lt % nctx) * TX, cy0 = (lt / nctx) * TY;
