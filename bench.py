@@ -40,8 +40,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "DEM cells/s batched vs plain GPU NNI at ≤1e-4 m err vs FP64; p50/p99 tile latency"
 UNIT = "cells/s"
-KERNELS_PER_CALL = 17      # own kernel launches per single-work-package call with points
-KERNELS_PER_BATCH = 16     # per batch run (the bounding boxes come with the bin counts)
+KERNELS_PER_CALL = 16      # own kernel launches per single-work-package call with points
+KERNELS_PER_BATCH = 15     # per batch run (the bounding boxes come with the bin counts)
 FALLBACK_HBM_GBS = 6650.0
 BASE_SEED = 20261203
 

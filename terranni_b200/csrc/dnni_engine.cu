@@ -115,17 +115,17 @@ void release_scratch(dnni_ctx* c, Scratch& s) {
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
 
-// Stencil + finalize, for the batch's stencil radius.
-void launch_final(const BatchTables& bt, int ncta, int rs, const int2* pix, Scalars* sc,
-                  const unsigned long long* S, const int* Sc, float* h, cudaStream_t st) {
+// Row scan, stencil and finalize, for the batch's stencil radius.
+void launch_rows_final(const BatchTables& bt, int ncta, int rs, const int2* pix, Scalars* sc,
+                       const unsigned long long* S, const int* Sc, float* h, cudaStream_t st) {
     dim3 blk(32, 16);
     switch (rs) {
-        case 1: k_final<1><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
-        case 2: k_final<2><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
-        case 4: k_final<4><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
-        case 5: k_final<5><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
-        case 6: k_final<6><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
-        default: k_final<3><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 1: k_rows_final<1><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 2: k_rows_final<2><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 4: k_rows_final<4><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 5: k_rows_final<5><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        case 6: k_rows_final<6><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
+        default: k_rows_final<3><<<ncta, blk, 0, st>>>(bt, pix, sc, S, Sc, h); break;
     }
 }
 
@@ -194,9 +194,7 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     k_scatter_window<<<nrt, dim3(32, 8), sizeof(unsigned long long) * hb.win_words, st>>>(bt, a.pix, a.sc, a.D,
                                                                                          a.Dc, hb.win_words);
     if (ev) cudaEventRecord(ev[2], st);
-    const int ngrow = hb.grow_base.back();
-    k_rowscan<<<ngrow, kScanThreads, 0, st>>>(bt, a.D, a.Dc, a.sc);
-    launch_final(bt, hb.ct_base.back(), hb.rs, a.pix, a.sc, a.D, a.Dc, d_h, st);
+    launch_rows_final(bt, hb.band_base.back(), hb.rs, a.pix, a.sc, a.D, a.Dc, d_h, st);
 }
 
 // Sums the per-tile scalars into dnni_stats.

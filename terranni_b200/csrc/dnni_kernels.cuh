@@ -7,9 +7,9 @@
 //     colour buffer)                       -> k_bin_* + k_near_dense/far
 //   nni.cpp:794-820 performNNIQueries / nni.cpp:483-534 makeBlocks and
 //     cuda_nni.cu:407-488 calcNNI (query planes OR-blended into bit masks,
-//     then per-pixel int32 atomics)        -> k_scatter_window + k_final stencil
+//     then per-pixel int32 atomics)        -> k_scatter_window + k_rows_final stencil
 //   cuda_nni.cu:491-503 divide, cuda_nni.cu:399-402 zeroValues
-//                                          -> k_rowscan + k_final
+//                                          -> k_rows_final
 //
 // Every kernel covers all tiles of a batch in one launch: its blocks (or
 // warps, or threads) are numbered across the tiles and an exclusive prefix
@@ -53,6 +53,7 @@ struct BatchTables {
     const int* rt_base;          // 32 x kTileY raster tiles
     const int* ct_base;          // 32 x 16 cell tiles
     const int* grow_base;        // grid rows
+    const int* band_base;        // bands of 16 grid rows
 };
 
 struct BatchCounters {
@@ -1150,60 +1151,88 @@ __device__ __forceinline__ float finalize_height(long long Z, long long C, doubl
     return __double2float_rn(__dadd_rn(__dmul_rn(q, zs), zo));
 }
 
-// Stencil path + finalize: each cell gathers the small discs (R2 <= H^2) of
-// the pixels within H, adds the prefix-summed span words, and divides.  One
-// CTA per 32 x 16 cell tile of a work package.
+// Row scan, stencil and finalize in one pass: one CTA (32 x 16 threads) per
+// band of 16 grid rows of a work package, walking the band's columns in
+// chunks of 32.  Each warp owns one row: it prefix-sums the row's span words
+// (the per-row difference form of the span path) chunk by chunk, carrying
+// the running sum in a register, so the prefix is never written back; each
+// cell then gathers the small discs (R2 <= H^2) of the pixels within H from
+// the chunk's pixel records in shared memory, adds its prefix, and divides.
 template <int H>
-__global__ void __launch_bounds__(512) k_final(BatchTables bt, const int2* __restrict__ pix,
-                                               Scalars* __restrict__ sc,
-                                               const unsigned long long* __restrict__ S_all,
-                                               const int* __restrict__ Sc_all, float* __restrict__ h_all) {
+__global__ void __launch_bounds__(512) k_rows_final(BatchTables bt, const int2* __restrict__ pix,
+                                                    Scalars* __restrict__ sc,
+                                                    const unsigned long long* __restrict__ S_all,
+                                                    const int* __restrict__ Sc_all, float* __restrict__ h_all) {
     constexpr int TX = 32, TY = 16, SW = TX + 2 * H, SH = TY + 2 * H;
     __shared__ int2 tile[SH][SW];
-    const int t = find_tile(bt.ct_base, bt.ntiles, blockIdx.x);
+    const int t = find_tile(bt.band_base, bt.ntiles, blockIdx.x);
     const TileParams T = bt.tiles[t];
-    const int lt = blockIdx.x - __ldg(&bt.ct_base[t]);
-    const int nctx = (T.ncols + TX - 1) / TX;
-    const int cx0 = (lt % nctx) * TX, cy0 = (lt / nctx) * TY;
+    const int cy0 = (blockIdx.x - __ldg(&bt.band_base[t])) * TY;
     const int2* P = pix + T.pix_off;
-    for (int idx = threadIdx.y * TX + threadIdx.x; idx < SW * SH; idx += TX * TY) {
-        const int ly = idx / SW, lx = idx - ly * SW;
-        const int rxi = cx0 - H + lx - T.rx0, ryi = cy0 - H + ly - T.ry0;
-        int2 v = make_int2(0, -1);
-        if (rxi >= 0 && rxi < T.rw && ryi >= 0 && ryi < T.rh) v = P[(int64_t)ryi * T.rw + rxi];
-        tile[ly][lx] = v;
-    }
-    __syncthreads();
-    const int qx = cx0 + threadIdx.x, qy = cy0 + threadIdx.y;
-    const bool in = qx < T.ncols && qy < T.nrows;
-    long long Z = 0, C = 0;
-#pragma unroll
-    for (int dy = -H; dy <= H; ++dy)
-#pragma unroll
-        for (int dx = -H; dx <= H; ++dx) {
-            if (dx * dx + dy * dy > H * H) continue;
-            const int2 p = tile[threadIdx.y + H + dy][threadIdx.x + H + dx];
-            if (p.y >= dx * dx + dy * dy && p.y <= H * H) { Z += p.x; C += 1; }
-        }
-    unsigned nod = 0;
     Scalars* s = sc + t;
-    if (in) {
-        const int64_t q = (int64_t)qy * T.ncols + qx;
-        const unsigned long long w = S_all[T.cell_off + q];
-        if (s->packed) {
-            long long zb, cb;
-            decode_span_word(w, s->kbits, s->zbase, zb, cb);
-            Z += zb;
-            C += cb;
-        } else {
-            Z += (long long)w;
-            C += Sc_all[T.cell_off + q];
+    const bool packed = s->packed != 0;
+    const int K = s->kbits;
+    const long long zbase = s->zbase;
+    const int lane = threadIdx.x;
+    const int qy = cy0 + threadIdx.y;
+    const bool row_in = qy < T.nrows;
+    unsigned long long carry = 0;   // running prefix of the row's span words (Z when unpacked)
+    int carry_c = 0;                // running prefix of the counts (unpacked)
+    unsigned nod = 0;
+#pragma unroll 1
+    for (int cx0 = 0; cx0 < T.ncols; cx0 += TX) {
+        if (cx0) __syncthreads();   // the previous chunk's stencil reads are over
+        for (int idx = threadIdx.y * TX + threadIdx.x; idx < SW * SH; idx += TX * TY) {
+            const int ly = idx / SW, lx = idx - ly * SW;
+            const int rxi = cx0 - H + lx - T.rx0, ryi = cy0 - H + ly - T.ry0;
+            int2 v = make_int2(0, -1);
+            if (rxi >= 0 && rxi < T.rw && ryi >= 0 && ryi < T.rh) v = P[(int64_t)ryi * T.rw + rxi];
+            tile[ly][lx] = v;
         }
-        h_all[T.out_off + q] = finalize_height(Z, C, T.z_scale, T.z_offset, T.nodata);
-        nod = C <= 0 ? 1u : 0u;
+        const int qx = cx0 + lane;
+        const bool in = row_in && qx < T.ncols;
+        const int64_t q = (int64_t)qy * T.ncols + qx;
+        unsigned long long w = in ? S_all[T.cell_off + q] : 0ull;
+        int wc = (in && !packed) ? Sc_all[T.cell_off + q] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+            const int yc = __shfl_up_sync(0xffffffffu, wc, o);
+            if (lane >= o) {
+                w += y;
+                wc += yc;
+            }
+        }
+        w += carry;
+        wc += carry_c;
+        carry = __shfl_sync(0xffffffffu, w, 31);
+        carry_c = __shfl_sync(0xffffffffu, wc, 31);
+        __syncthreads();
+        long long Z = 0, C = 0;
+#pragma unroll
+        for (int dy = -H; dy <= H; ++dy)
+#pragma unroll
+            for (int dx = -H; dx <= H; ++dx) {
+                if (dx * dx + dy * dy > H * H) continue;
+                const int2 p = tile[threadIdx.y + H + dy][lane + H + dx];
+                if (p.y >= dx * dx + dy * dy && p.y <= H * H) { Z += p.x; C += 1; }
+            }
+        if (in) {
+            if (packed) {
+                long long zb, cb;
+                decode_span_word(w, K, zbase, zb, cb);
+                Z += zb;
+                C += cb;
+            } else {
+                Z += (long long)w;
+                C += wc;
+            }
+            h_all[T.out_off + q] = finalize_height(Z, C, T.z_scale, T.z_offset, T.nodata);
+            nod += C <= 0 ? 1u : 0u;
+        }
     }
     nod = __reduce_add_sync(0xffffffffu, nod);
-    if ((threadIdx.x & 31) == 0 && nod) {
+    if (lane == 0 && nod) {
         const int slot = (blockIdx.x + threadIdx.y) & (kStatSlots - 1);
         atomicAdd(&s->nodata[slot], (unsigned long long)nod);
     }

@@ -118,7 +118,7 @@ constexpr int64_t kMaxLaunchIndex = INT32_MAX - 1024;
 
 struct HostBatch {
     std::vector<TileParams> tiles;
-    std::vector<int> chunk_base{0}, scan_base{0}, row1_base{0}, rt_base{0}, ct_base{0}, grow_base{0};
+    std::vector<int> chunk_base{0}, scan_base{0}, row1_base{0}, rt_base{0}, ct_base{0}, grow_base{0}, band_base{0};
     std::vector<int64_t> blk_base{0}, sup_base{0};
     int64_t n_rows = 0;                  // input point rows the tiles reference
     int64_t n_pts = 0, n_bins = 0, n_pix = 0, n_cells = 0, n_far = 0;
@@ -165,6 +165,7 @@ inline void batch_add(HostBatch& hb, TileParams t, int64_t pt_off, int64_t out_o
     add(hb.rt_base, (int64_t)((t.rw + kTileX - 1) / kTileX) * ((t.rh + kTileY - 1) / kTileY));
     add(hb.ct_base, (int64_t)((t.ncols + 31) / 32) * ((t.nrows + 15) / 16));
     add(hb.grow_base, t.nrows);
+    add(hb.band_base, (t.nrows + 15) / 16);
     hb.n_rows = std::max<int64_t>(hb.n_rows, pt_off + t.npts);
     hb.n_pts += t.npts;
     hb.n_pix += (int64_t)t.rw * t.rh;
@@ -231,7 +232,7 @@ inline std::vector<double> edt_2d(const unsigned char* occ, int nx, int ny) {
 
 // Byte layout of the device copy of a batch's tables (one upload).
 struct TableLayout {
-    size_t tiles, chunk, scan, blk, sup, row1, rt, ct, grow, total;
+    size_t tiles, chunk, scan, blk, sup, row1, rt, ct, grow, band, total;
     explicit TableLayout(int n) {
         size_t o = 0;
         auto take = [&](size_t b) { const size_t r = o; o = (o + b + 15) & ~(size_t)15; return r; };
@@ -244,6 +245,7 @@ struct TableLayout {
         rt = take(sizeof(int) * (n + 1));
         ct = take(sizeof(int) * (n + 1));
         grow = take(sizeof(int) * (n + 1));
+        band = take(sizeof(int) * (n + 1));
         total = o;
     }
 };
@@ -261,6 +263,7 @@ inline void pack_tables(const HostBatch& hb, unsigned char* dst) {
     memcpy(dst + L.rt, hb.rt_base.data(), sizeof(int) * (n + 1));
     memcpy(dst + L.ct, hb.ct_base.data(), sizeof(int) * (n + 1));
     memcpy(dst + L.grow, hb.grow_base.data(), sizeof(int) * (n + 1));
+    memcpy(dst + L.band, hb.band_base.data(), sizeof(int) * (n + 1));
 }
 
 // Device view of tables uploaded to `dev` (laid out as TableLayout).
@@ -277,6 +280,7 @@ inline BatchTables device_tables(const unsigned char* dev, int n) {
     bt.rt_base = (const int*)(dev + L.rt);
     bt.ct_base = (const int*)(dev + L.ct);
     bt.grow_base = (const int*)(dev + L.grow);
+    bt.band_base = (const int*)(dev + L.band);
     return bt;
 }
 

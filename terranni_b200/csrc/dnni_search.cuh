@@ -9,9 +9,9 @@
 //     colour buffer)                       -> k_bin_* + k_nearest
 //   nni.cpp:794-820 performNNIQueries / nni.cpp:483-534 makeBlocks and
 //     cuda_nni.cu:407-488 calcNNI (query planes OR-blended into bit masks,
-//     then per-pixel int32 atomics)        -> k_scatter_window + k_final stencil
+//     then per-pixel int32 atomics)        -> k_scatter_window + k_rows_final stencil
 //   cuda_nni.cu:491-503 divide, cuda_nni.cu:399-402 zeroValues
-//                                          -> k_rowscan + k_final
+//                                          -> k_rows_final
 //
 // Data layout in HBM (per call):
 //   sorted points  int4 {x-ox, y-oy, z, gid}, grouped by search bin;

@@ -224,7 +224,7 @@ __global__ void k_st_decide(Scalars* sc, int zmin, int zmax, long long npix, int
     }
 }
 
-// k_final over `layers` stacked pixel rasters (layer stride lstride): each
+// Stencil and divide over `layers` stacked pixel rasters (layer stride lstride): each
 // cell gathers the small discs of every slice, adds the prefix-summed span
 // words and divides.  One CTA per 32 x 16 cell tile.
 template <int H>
