@@ -1164,7 +1164,8 @@ __global__ void __launch_bounds__(512) k_rows_final(BatchTables bt, const int2* 
                                                     const unsigned long long* __restrict__ S_all,
                                                     const int* __restrict__ Sc_all, float* __restrict__ h_all) {
     constexpr int TX = 32, TY = 16, SW = TX + 2 * H, SH = TY + 2 * H;
-    __shared__ int2 tile[SH][SW];
+    constexpr int NL = (SW * SH + TX * TY - 1) / (TX * TY);   // pixel records each thread loads per chunk
+    __shared__ int2 tile[2][SH][SW];                          // double buffer: this chunk and the next
     const int t = find_tile(bt.band_base, bt.ntiles, blockIdx.x);
     const TileParams T = bt.tiles[t];
     const int cy0 = (blockIdx.x - __ldg(&bt.band_base[t])) * TY;
@@ -1173,27 +1174,59 @@ __global__ void __launch_bounds__(512) k_rows_final(BatchTables bt, const int2* 
     const bool packed = s->packed != 0;
     const int K = s->kbits;
     const long long zbase = s->zbase;
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x, tid = threadIdx.y * TX + threadIdx.x;
     const int qy = cy0 + threadIdx.y;
     const bool row_in = qy < T.nrows;
+    // the chunk starting at column cx: this thread's pixel records (into
+    // registers) and its cell's span words
+    int2 rec[NL];
+    auto load_tile = [&](int cx) {
+#pragma unroll
+        for (int k = 0; k < NL; ++k) {
+            const int idx = tid + k * TX * TY;
+            int2 v = make_int2(0, -1);
+            if (idx < SW * SH) {
+                const int ly = idx / SW, lx = idx - ly * SW;
+                const int rxi = cx - H + lx - T.rx0, ryi = cy0 - H + ly - T.ry0;
+                if (rxi >= 0 && rxi < T.rw && ryi >= 0 && ryi < T.rh) v = P[(int64_t)ryi * T.rw + rxi];
+            }
+            rec[k] = v;
+        }
+    };
+    auto store_tile = [&](int b) {
+#pragma unroll
+        for (int k = 0; k < NL; ++k) {
+            const int idx = tid + k * TX * TY;
+            if (idx < SW * SH) tile[b][idx / SW][idx % SW] = rec[k];
+        }
+    };
+    auto load_words = [&](int cx, unsigned long long& w, int& wc) {
+        const int qx = cx + lane;
+        const bool in = row_in && qx < T.ncols;
+        const int64_t q = (int64_t)qy * T.ncols + qx;
+        w = in ? S_all[T.cell_off + q] : 0ull;
+        wc = (in && !packed) ? Sc_all[T.cell_off + q] : 0;
+    };
     unsigned long long carry = 0;   // running prefix of the row's span words (Z when unpacked)
     int carry_c = 0;                // running prefix of the counts (unpacked)
     unsigned nod = 0;
+    unsigned long long w;
+    int wc;
+    load_tile(0);
+    store_tile(0);
+    load_words(0, w, wc);
+    __syncthreads();
+    int b = 0;
 #pragma unroll 1
-    for (int cx0 = 0; cx0 < T.ncols; cx0 += TX) {
-        if (cx0) __syncthreads();   // the previous chunk's stencil reads are over
-        for (int idx = threadIdx.y * TX + threadIdx.x; idx < SW * SH; idx += TX * TY) {
-            const int ly = idx / SW, lx = idx - ly * SW;
-            const int rxi = cx0 - H + lx - T.rx0, ryi = cy0 - H + ly - T.ry0;
-            int2 v = make_int2(0, -1);
-            if (rxi >= 0 && rxi < T.rw && ryi >= 0 && ryi < T.rh) v = P[(int64_t)ryi * T.rw + rxi];
-            tile[ly][lx] = v;
+    for (int cx0 = 0; cx0 < T.ncols; cx0 += TX, b ^= 1) {
+        // the next chunk's loads are in flight while this one computes
+        const bool more = cx0 + TX < T.ncols;
+        unsigned long long w_next = 0;
+        int wc_next = 0;
+        if (more) {
+            load_tile(cx0 + TX);
+            load_words(cx0 + TX, w_next, wc_next);
         }
-        const int qx = cx0 + lane;
-        const bool in = row_in && qx < T.ncols;
-        const int64_t q = (int64_t)qy * T.ncols + qx;
-        unsigned long long w = in ? S_all[T.cell_off + q] : 0ull;
-        int wc = (in && !packed) ? Sc_all[T.cell_off + q] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
@@ -1207,17 +1240,17 @@ __global__ void __launch_bounds__(512) k_rows_final(BatchTables bt, const int2* 
         wc += carry_c;
         carry = __shfl_sync(0xffffffffu, w, 31);
         carry_c = __shfl_sync(0xffffffffu, wc, 31);
-        __syncthreads();
         long long Z = 0, C = 0;
 #pragma unroll
         for (int dy = -H; dy <= H; ++dy)
 #pragma unroll
             for (int dx = -H; dx <= H; ++dx) {
                 if (dx * dx + dy * dy > H * H) continue;
-                const int2 p = tile[threadIdx.y + H + dy][lane + H + dx];
+                const int2 p = tile[b][threadIdx.y + H + dy][lane + H + dx];
                 if (p.y >= dx * dx + dy * dy && p.y <= H * H) { Z += p.x; C += 1; }
             }
-        if (in) {
+        const int qx = cx0 + lane;
+        if (row_in && qx < T.ncols) {
             if (packed) {
                 long long zb, cb;
                 decode_span_word(w, K, zbase, zb, cb);
@@ -1227,9 +1260,17 @@ __global__ void __launch_bounds__(512) k_rows_final(BatchTables bt, const int2* 
                 Z += (long long)w;
                 C += wc;
             }
-            h_all[T.out_off + q] = finalize_height(Z, C, T.z_scale, T.z_offset, T.nodata);
+            h_all[T.out_off + (int64_t)qy * T.ncols + qx] = finalize_height(Z, C, T.z_scale, T.z_offset, T.nodata);
             nod += C <= 0 ? 1u : 0u;
         }
+        if (more) {
+            // the other buffer's last readers (the chunk before this one)
+            // finished before the barrier that ended that chunk
+            store_tile(b ^ 1);
+            w = w_next;
+            wc = wc_next;
+        }
+        __syncthreads();
     }
     nod = __reduce_add_sync(0xffffffffu, nod);
     if (lane == 0 && nod) {
