@@ -400,13 +400,15 @@ __global__ void k_block_near(BatchTables bt, const int* __restrict__ rownear, in
 // nearest site per raster pixel
 // ---------------------------------------------------------------------------
 
-// Records a settled pixel: its record and (optionally) its site.
-__device__ __forceinline__ void settle_pixel(const TileParams& T, int i, int j, const Best& b, int2* __restrict__ pix,
-                                             uint32_t* __restrict__ site) {
+// Records a settled pixel: its record and (optionally) its site; returns
+// its R2.
+__device__ __forceinline__ int settle_pixel(const TileParams& T, int i, int j, const Best& b, int2* __restrict__ pix,
+                                            uint32_t* __restrict__ site) {
     const int R2 = r2_of(b.d2, (long long)T.cs * T.cs, T.r2cap);
     const int64_t o = (int64_t)j * T.rw + i;
     pix[T.pix_off + o] = make_int2(b.z, R2);
     if (site && T.site_off >= 0) site[T.site_off + o] = b.gid;
+    return R2;
 }
 
 // Statistics of settled pixels, accumulated per thread and flushed once per
@@ -585,8 +587,7 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
                 done = search_bins(g, pts, start, px, py, b);
             }
             if (done) {
-                settle_pixel(T, i, j, b, pix, site);
-                R2 = r2_of(b.d2, (long long)T.cs * T.cs, T.r2cap);
+                R2 = settle_pixel(T, i, j, b, pix, site);
             } else {
                 far_pixel = true;
             }
@@ -793,9 +794,16 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
                     const int64_t id = (blk << 6) + l;
                     const int s0 = __ldg(&start[id]), e0 = __ldg(&start[id + 1]);
                     if (act) b.nev += e0 - s0;
-                    for (int q = s0; q < e0; ++q) {
-                        const int4 p = __ldg(&pts[q]);
-                        if (act) consider(b, p, q, px, py);
+                    if (small) {
+                        for (int q = s0; q < e0; ++q) {
+                            const int4 p = __ldg(&pts[q]);
+                            if (act) consider_below31(b, p, q, px, py);
+                        }
+                    } else {
+                        for (int q = s0; q < e0; ++q) {
+                            const int4 p = __ldg(&pts[q]);
+                            if (act) consider(b, p, q, px, py);
+                        }
                     }
                 }
             }
@@ -867,10 +875,7 @@ __global__ void __launch_bounds__(256, 4) k_near_far(BatchTables bt, const int4*
         }
         search_disc_warp(g, pts, start, bmask, smask, act, px, py, b);
         int R2 = -1;
-        if (act) {
-            settle_pixel(T, i, j, b, pix, site);
-            R2 = r2_of(b.d2, (long long)T.cs * T.cs, T.r2cap);
-        }
+        if (act) R2 = settle_pixel(T, i, j, b, pix, site);
         StatAcc acc;
         acc.add(T, R2, b.nev);
         acc.flush(sc + t, blockIdx.x * 3 + (threadIdx.x >> 5), true);

@@ -168,6 +168,23 @@ DNNI_HD void consider(Best& b, const int4 p, int q, int px, int py) {
     }
 }
 
+// consider() for a pixel whose bound is below 2^31 (a real site found): a
+// candidate with |dx| or |dy| above 46340 lies beyond the bound, so the
+// distance and its comparison stay in 32-bit arithmetic.  Same result.
+DNNI_HD void consider_below31(Best& b, const int4 p, int q, int px, int py) {
+    const int dx = p.x - px, dy = p.y - py;      // |p.x|, |px| < 2^30
+    const unsigned ax = (unsigned)(dx < 0 ? -dx : dx), ay = (unsigned)(dy < 0 ? -dy : dy);
+    if (ax > 46340u || ay > 46340u) return;
+    const unsigned d2 = ax * ax + ay * ay, bd = (unsigned)b.d2;
+    const uint32_t g = (uint32_t)p.w;
+    if (d2 < bd || (d2 == bd && (g < b.gid || (g == b.gid && p.z < b.z)))) {
+        b.d2 = d2;
+        b.gid = g;
+        b.z = p.z;
+        b.idx = q;
+    }
+}
+
 DNNI_HD long long axis_gap(long long p, long long lo, long long hi) {
     long long d = p < lo ? lo - p : (p > hi ? p - hi : 0);
     return d < kDistCap ? d : kDistCap;
