@@ -156,15 +156,21 @@ struct Best {
     int nev;      // candidate distance evaluations made for this pixel
 };
 
+// Most candidates are farther than the best so far; one comparison of the
+// distance rejects them, and only the rest go through the full (d2, gid, z)
+// order (written as a branch expected not taken: on the far pass's wide
+// candidate sets this beat the flat three-key comparison).
 DNNI_HD void consider(Best& b, const int4 p, int q, int px, int py) {
     const int dx = p.x - px, dy = p.y - py;      // |p.x|, |px| < 2^30
     const long long d2 = (long long)dx * dx + (long long)dy * dy;
-    const uint32_t g = (uint32_t)p.w;
-    if (d2 < b.d2 || (d2 == b.d2 && (g < b.gid || (g == b.gid && p.z < b.z)))) {
-        b.d2 = d2;
-        b.gid = g;
-        b.z = p.z;
-        b.idx = q;
+    if (__builtin_expect(d2 <= b.d2, 0)) {
+        const uint32_t g = (uint32_t)p.w;
+        if (d2 < b.d2 || g < b.gid || (g == b.gid && p.z < b.z)) {
+            b.d2 = d2;
+            b.gid = g;
+            b.z = p.z;
+            b.idx = q;
+        }
     }
 }
 
@@ -176,12 +182,14 @@ DNNI_HD void consider_below31(Best& b, const int4 p, int q, int px, int py) {
     const unsigned ax = (unsigned)(dx < 0 ? -dx : dx), ay = (unsigned)(dy < 0 ? -dy : dy);
     if (ax > 46340u || ay > 46340u) return;
     const unsigned d2 = ax * ax + ay * ay, bd = (unsigned)b.d2;
-    const uint32_t g = (uint32_t)p.w;
-    if (d2 < bd || (d2 == bd && (g < b.gid || (g == b.gid && p.z < b.z)))) {
-        b.d2 = d2;
-        b.gid = g;
-        b.z = p.z;
-        b.idx = q;
+    if (__builtin_expect(d2 <= bd, 0)) {
+        const uint32_t g = (uint32_t)p.w;
+        if (d2 < bd || g < b.gid || (g == b.gid && p.z < b.z)) {
+            b.d2 = d2;
+            b.gid = g;
+            b.z = p.z;
+            b.idx = q;
+        }
     }
 }
 
