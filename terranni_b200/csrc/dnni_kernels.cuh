@@ -723,6 +723,44 @@ __device__ __forceinline__ uint64_t chord_mask8(bool act, long long px, long lon
     return m;
 }
 
+// chord_mask8 for a warp whose every active lane has a bound below 2^31 (a
+// real site found), in 32-bit arithmetic relative to the mask's origin: rx,
+// ry = pixel - origin (|rx|, |ry| < 2^30), u = cell width (8u <= 2^30).  The
+// row gap beyond 46340 units already exceeds any such bound.  The chord's
+// cell range is the same as chord_mask8's: floor(x / u) for 0 < x < 8u from
+// a float product with 1/u (within one of the quotient there), corrected
+// with exact integer products.
+__device__ __forceinline__ int floor_div8(int x, int u, float inv_u) {
+    int q = (int)((float)x * inv_u);
+    q -= q * u > x ? 1 : 0;
+    q += (q + 1) * u <= x ? 1 : 0;
+    return q;
+}
+
+__device__ __forceinline__ uint64_t chord_mask8_32(bool act, int rx, int ry, unsigned d2, int u, float inv_u) {
+    uint64_t m = 0;
+#pragma unroll 1
+    for (int r = 0; r < 8; ++r) {
+        int a = 8, e = -1;
+        if (act) {
+            const int y0 = r * u, y1 = y0 + u - 1;
+            const int gy = ry < y0 ? y0 - ry : (ry > y1 ? ry - y1 : 0);
+            if (gy <= 46340 && (unsigned)(gy * gy) <= d2) {
+                const int w = (int)sqrtf((float)(d2 - (unsigned)(gy * gy))) + 1;
+                const int lo = rx - w, hi = rx + w;
+                if (hi >= 0 && lo < 8 * u) {
+                    a = lo <= 0 ? 0 : floor_div8(lo, u, inv_u);
+                    e = hi >= 8 * u ? 7 : floor_div8(hi, u, inv_u);
+                }
+            }
+        }
+        a = __reduce_min_sync(0xffffffffu, a);
+        e = __reduce_max_sync(0xffffffffu, e);
+        if (a <= e) m |= (uint64_t)((0xFFu >> (7 - e)) & (0xFFu << a) & 0xFFu) << (8 * r);
+    }
+    return m;
+}
+
 // A candidate block with at most this many points is scanned whole, which
 // costs less than its bin mask.
 constexpr int kFarWholeBlock = 24;
@@ -744,6 +782,7 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
     const unsigned full = 0xffffffffu;
     const long long gx0 = g.gx0, gy0 = g.gy0, bs = g.bs;
     const long long u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
+    const float inv_u1 = 1.0f / (float)u1, inv_bs = 1.0f / (float)bs;
     const long long reach = act ? reach_of(b.d2) : 0;
     const long long xlo = warp_min64(act ? px - reach : LLONG_MAX), xhi = warp_max64(act ? px + reach : LLONG_MIN);
     const long long ylo = warp_min64(act ? py - reach : LLONG_MAX), yhi = warp_max64(act ? py + reach : LLONG_MIN);
@@ -767,9 +806,15 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
             const long long SX0 = gx0 + (long long)sx * u2;
             const bool need_s = act && box_lb(px, py, SX0, SX0 + u2 - 1, SY0, SY0 + u2 - 1) <= b.d2;
             if (!__any_sync(full, need_s)) continue;
-            // 32-bit square roots are within one unit while every bound is below 2^31
-            bool small = __all_sync(full, !act || b.d2 < (1LL << 31));
-            uint64_t cand = sm & chord_mask8(act, px, py, b.d2, SX0, SY0, u1, small);
+            // 32-bit arithmetic while every bound is below 2^31 and every
+            // active lane lies within 2^29 units of the superblock's origin
+            // (then within 2^30 of each of its blocks' origins)
+            const long long ox = px - SX0, oy = py - SY0;
+            const bool near = !act || (ox > -(1LL << 29) && ox < (1LL << 29) && oy > -(1LL << 29) && oy < (1LL << 29));
+            bool small = __all_sync(full, !act || (b.d2 < (1LL << 31) && near));
+            uint64_t cand = sm & (small ? chord_mask8_32(act, (int)(px - SX0), (int)(py - SY0), (unsigned)b.d2,
+                                                         (int)u1, inv_u1)
+                                        : chord_mask8(act, px, py, b.d2, SX0, SY0, u1, false));
             while (cand) {
                 const int m = ffs64(cand);
                 cand &= cand - 1;
@@ -786,8 +831,10 @@ __device__ void search_disc_warp(const BinGrid& g, const int4* __restrict__ pts,
                     continue;
                 }
                 const uint64_t bm = __ldg(&bmask[blk]);
-                small = __all_sync(full, !act || b.d2 < (1LL << 31));
-                uint64_t qc = bm & chord_mask8(act, px, py, b.d2, BX0, BY0, bs, small);
+                small = __all_sync(full, !act || (b.d2 < (1LL << 31) && near));
+                uint64_t qc = bm & (small ? chord_mask8_32(act, (int)(px - BX0), (int)(py - BY0), (unsigned)b.d2,
+                                                           (int)bs, inv_bs)
+                                          : chord_mask8(act, px, py, b.d2, BX0, BY0, bs, false));
                 while (qc) {
                     const int l = ffs64(qc);
                     qc &= qc - 1;
@@ -1009,7 +1056,7 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
     unsigned long long* D = D_all + T.cell_off;
     int* Dc = Dc_all + T.cell_off;
     const int W = c1 - c0 + 1;
-    const int CH = win_words / W;
+    const int CH = (win_words & ~3) / W;
     // the window sums z relative to zbase and the counts in two int32 arrays
     // (native shared-memory atomics); a window cell receives at most one
     // marker per pixel of the tile, so |sum| <= kTileX * kTileY * zabs must
@@ -1037,15 +1084,16 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
     }
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int ncols = T.ncols;
+    const int ww4 = win_words & ~3;           // whole int4s: the chunk is zeroed 16 bytes at a time
     int* sz = swin;                           // z - zbase sums
-    int* scn = swin + win_words;              // counts
+    int* scn = swin + ww4;                    // counts
 #pragma unroll 1
     for (int y0 = r0; y0 <= r1; y0 += CH) {
         const int y1 = min(y0 + CH - 1, r1);
         const int nw = (y1 - y0 + 1) * W;
-        for (int e = tid; e < nw; e += 256) {
-            sz[e] = 0;
-            scn[e] = 0;
+        for (int e = tid; e < (nw + 3) >> 2; e += 256) {
+            reinterpret_cast<int4*>(sz)[e] = make_int4(0, 0, 0, 0);
+            reinterpret_cast<int4*>(scn)[e] = make_int4(0, 0, 0, 0);
         }
         __syncthreads();
 #pragma unroll 1
@@ -1057,15 +1105,20 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
             if (ya > yb) continue;
             const unsigned R2 = (unsigned)R2v[sub];
             const int zr = (int)((long long)zv[sub] - s.zbase);
-            int dy = ya - py;
-            unsigned w = (unsigned)isqrt_i32((int)(R2 - (unsigned)(dy * dy)));
-            for (int y = ya; y <= yb; ++y, ++dy) {
+            // the lanes of a warp are 32 neighbouring pixels of one row, whose
+            // markers on a common row often fall on one cell (same-address
+            // atomics serialise); each lane starts its rows at its own offset
+            // so that the warp's markers spread over the chunk's rows.  The
+            // half-width floor(sqrt(t2)) comes from a float square root,
+            // within one of it for t2 < 2^31, and one exact step each way.
+            const int nrow = yb - ya + 1;
+            int y = ya + (int)(threadIdx.x % (unsigned)nrow);
+            for (int k = 0; k < nrow; ++k, y = (y == yb) ? ya : y + 1) {
+                const int dy = y - py;
                 const unsigned t2 = R2 - (unsigned)(dy * dy);
-                if (dy <= 0) {
-                    while ((w + 1) * (w + 1) <= t2) ++w;
-                } else {
-                    while (w * w > t2) --w;
-                }
+                unsigned w = (unsigned)sqrtf((float)t2);
+                w -= (w * w > t2) ? 1u : 0u;
+                w += ((w + 1) * (w + 1) <= t2) ? 1u : 0u;
                 const int a = max(px - (int)w, 0), b = px + (int)w + 1;
                 if (a >= ncols || b <= 0) continue;       // this row's span misses the grid
                 const int row = (y - y0) * W - c0;     // a and b lie in [c0, c1]

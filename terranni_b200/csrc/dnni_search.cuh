@@ -396,6 +396,7 @@ DNNI_HD long long best32_d2(const Best32& b) { return b.key == ~0ull ? LLONG_MAX
 
 DNNI_HD void scan_local32(Best32& b, const int4* lpts, int s, int e, int px, int py) {
     b.nev += e - s;
+#pragma unroll 2
     for (int q = s; q < e; ++q) consider32(b, lpts[q], q, px, py);
 }
 
