@@ -32,6 +32,8 @@
 //                  largest possible per-cell sums.
 #pragma once
 
+#include <cuda_pipeline_primitives.h>
+
 #include "dnni_search.cuh"
 
 namespace dnni {
@@ -498,19 +500,25 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
             break;
         }
         {
-            // per-bin counts -> local starts: warp w takes window rows w, w+8,
-            // ...; lanes take columns, with a warp scan along the row
+            // each window bin's global start and end, copied asynchronously
+            // (all of a band's copies in flight at once; a thread later reads
+            // only the entries it copied itself): warp w takes window rows w,
+            // w+8, ...; lanes take columns
+            for (int r = warp; r < wny; r += 8)
+                for (int c = lane; c < wnx; c += 32) {
+                    const int64_t id = bin_id(g, wx0 + c, wy0 + r);
+                    __pipeline_memcpy_async(&s_gstart[r * wnx + c], &start[id], sizeof(int));
+                    __pipeline_memcpy_async(&s_lstart[r * wnx + c], &start[id + 1], sizeof(int));
+                }
+            __pipeline_commit();
+            __pipeline_wait_prior(0);
+            // per-bin counts -> local starts, with a warp scan along the row
             for (int r = warp; r < wny; r += 8) {
                 int rowsum = 0;
                 for (int c0 = 0; c0 < wnx; c0 += 32) {
                     const int c = c0 + lane;
                     int cnt = 0;
-                    if (c < wnx) {
-                        const int64_t id = bin_id(g, wx0 + c, wy0 + r);
-                        const int gs = __ldg(&start[id]);
-                        cnt = __ldg(&start[id + 1]) - gs;
-                        s_gstart[r * wnx + c] = gs;
-                    }
+                    if (c < wnx) cnt = s_lstart[r * wnx + c] - s_gstart[r * wnx + c];
                     int x = cnt;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
@@ -550,9 +558,10 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
             }
             staged = s_total <= kWinMaxPts;
             if (staged) {
-                // copy the window's points run by run: the bins of one window
-                // row inside one block are consecutive in both layouts; one
-                // warp per run, lanes striding over its points
+                // copy the window's points run by run (asynchronous 16-byte
+                // copies, all in flight before one wait): the bins of one
+                // window row inside one block are consecutive in both layouts;
+                // one warp per run, lanes striding over its points
                 const int cb0 = wx0 >> 3, cb1 = (wx0 + wnx - 1) >> 3;
                 const int nseg = cb1 - cb0 + 1, nrun = nseg * wny;
                 for (int run = warp; run < nrun; run += 8) {
@@ -561,8 +570,10 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
                     const int xb = (cb0 + sg) * 8 + 7 < wx0 + wnx - 1 ? (cb0 + sg) * 8 + 7 : wx0 + wnx - 1;
                     const int lk0 = r * wnx + (xa - wx0), lk1 = r * wnx + (xb - wx0);
                     const int l0 = s_lstart[lk0], cntp = s_lstart[lk1 + 1] - l0, g0 = s_gstart[lk0];
-                    for (int q = lane; q < cntp; q += 32) s_pts[l0 + q] = __ldg(&pts[g0 + q]);
+                    for (int q = lane; q < cntp; q += 32) __pipeline_memcpy_async(&s_pts[l0 + q], &pts[g0 + q], sizeof(int4));
                 }
+                __pipeline_commit();
+                __pipeline_wait_prior(0);
             }
             __syncthreads();
         }
