@@ -730,6 +730,7 @@ def run_engine_mixed(args, world, rank, local):
                        "form": "batched: all tiles in one CUDA-graph launch sequence per step",
                        "small_radius": opts["small_radius"] or 3, "bin_target": opts["bin_target"] or 4,
                        "span_window": opts["span_window"] or 4096, "far_group": opts.get("far_group") or 2,
+                       "dense_band": opts.get("dense_band") or 64,
                        "order_by_cost": True, "autotune": tune,
                        "l2": f"inputs larger than L2 ({xyz.nbytes / 1e9:.1f} GB points per step)",
                        "parallelism": f"dp{world} (independent tiles)"},

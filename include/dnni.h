@@ -157,7 +157,7 @@ dnni_status dnni_interpolate_segment_device(dnni_ctx *ctx, const dnni_workpackag
  * loads the library holds it until the process exits.
  *
  * Limit: the work package must fit that array, at about 12 B per grid cell +
- * 24 B per raster pixel + 20 B per point + 8.2 B per search bin (about one
+ * 24 B per raster pixel + 16 B per point + 8.2 B per search bin (about one
  * bin per four points), each region rounded up to 256 B; e.g. a 512 x 512
  * grid with 500k points fits.  Larger work packages return DNNI_E_SCRATCH, before
  * any work is queued or, for the search bins (sized from the point bounding
@@ -220,6 +220,11 @@ typedef struct dnni_batch_options {
     int32_t far_group;             /* pixels the far pass searches together:
                                       1 = 32 x 1 rows, 2 = 8 x 4 blocks;
                                       0 = default (2) */
+    int32_t dense_band;            /* ring search: rows of the 32-pixel-wide
+                                      block that shares one bin window staged
+                                      in shared memory (8, 16, 32 or 64; a
+                                      window that does not fit halves it);
+                                      0 = default (64) */
 } dnni_batch_options;
 
 /* Plans the tiles and allocates the batch's device scratch (allocates). */
@@ -372,17 +377,20 @@ dnni_status dnni_server_destroy(dnni_server *srv);
 
 /* ---- autotuning of the batch options (no counterpart in the reference) ----
  *
- * Times candidate settings of the search-bin size (bin_target: points per
- * bin) and of the split between the stencil path and the span path
- * (small_radius: discs up to this radius are gathered by the stencil, larger
- * ones spill into row spans) on a sample of the tiles stratified by size, on
- * device buffers that already hold the points, and writes the fastest pair
- * into *options (use_graph and order_by_cost are left as given).  Results do
- * not depend on either setting; only the time does. */
+ * Times candidate settings, by coordinate search, of the search-bin size
+ * (bin_target: points per bin), the split between the stencil path and the
+ * span path (small_radius: discs up to this radius are gathered by the
+ * stencil, larger ones spill into row spans), the span path's shared-memory
+ * window (span_window), the far pass's pixel groups (far_group) and the
+ * ring search's pixel-block shape (dense_band: 32 x 8..64 pixels per staged
+ * bin window) on a sample of the tiles stratified by size, on device buffers
+ * that already hold the points, and writes the fastest settings into
+ * *options (use_graph and order_by_cost are left as given).  Results do not
+ * depend on any of these settings; only the time does. */
 typedef struct dnni_tune_trial {
     int32_t small_radius, bin_target;
     float ms;                          /* device time of one run of the sample */
-    int32_t span_window, far_group, pad;
+    int32_t span_window, far_group, dense_band;
 } dnni_tune_trial;
 
 typedef struct dnni_tune_report {

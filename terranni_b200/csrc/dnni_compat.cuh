@@ -296,7 +296,7 @@ static dnni_status compat_run(dnni_ctx* c, const dnni_compat_settings* s, const 
     const size_t tbytes = sizeof(long long) * (size_t)(nt + 1) + 2 * sizeof(int) * (size_t)nt;
     if ((rs = dnni_ensure(c, c->scr.D, sizeof(unsigned long long) * (size_t)(xp * yp))) ||
         (rs = dnni_ensure(c, c->scr.cnt, tbytes)) ||
-        (rs = dnni_ensure(c, c->scr.rank, sizeof(uint32_t) * (size_t)list_n)) ||
+        (rs = dnni_ensure(c, c->scr.list, sizeof(uint32_t) * (size_t)list_n)) ||
         (!device && ((rs = dnni_ensure(c, c->in_xyz, sizeof(double) * 3 * (size_t)std::max<int64_t>(n, 1))) ||
                      (rs = dnni_ensure(c, c->out_h, sizeof(float) * (size_t)cells)) ||
                      (res_out && (rs = dnni_ensure(c, c->out_site, sizeof(int32_t) * (size_t)cells))))))
@@ -315,9 +315,9 @@ static dnni_status compat_run(dnni_ctx* c, const dnni_compat_settings* s, const 
     }
     k_compat_offsets<<<1, 1024, 0, st>>>(tcnt, nt, toff, tcur);
     if (n > 0)
-        k_compat_fill<<<c->sm_count * 8, 256, 0, st>>>(G, dxyz, n, ntx, toff, tcur, (uint32_t*)c->scr.rank.p, list_n);
+        k_compat_fill<<<c->sm_count * 8, 256, 0, st>>>(G, dxyz, n, ntx, toff, tcur, (uint32_t*)c->scr.list.p, list_n);
     CK(cudaFuncSetAttribute(k_compat_sites, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCpTileSmem));
-    k_compat_sites<<<nt, 256, kCpTileSmem, st>>>(G, dxyz, ntx, toff, (const uint32_t*)c->scr.rank.p, list_n, key);
+    k_compat_sites<<<nt, 256, kCpTileSmem, st>>>(G, dxyz, ntx, toff, (const uint32_t*)c->scr.list.p, list_n, key);
     k_compat_cells<<<(int)((cells + 255) / 256), 256, 0, st>>>(G, dxyz, key, dh, dres);
     CK(cudaGetLastError());
     if (!device) {

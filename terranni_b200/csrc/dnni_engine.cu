@@ -55,14 +55,13 @@ struct DeviceGuard {
 
 // Every scratch array a batch needs, in bytes.
 struct ScratchSizes {
-    size_t sorted, rank, cnt, bsum, bmask, smask, rownear, near, pix, far, D, Dc, sc, ctr, tables;
+    size_t sorted, cnt, bsum, bmask, smask, rownear, near, pix, far, D, Dc, sc, ctr, tables;
 };
 
 ScratchSizes scratch_sizes(const HostBatch& hb) {
     const int n = (int)hb.tiles.size();
     ScratchSizes z;
     z.sorted = sizeof(int4) * std::max<int64_t>(hb.n_pts, 1);
-    z.rank = sizeof(int) * std::max<int64_t>(hb.n_pts, 1);
     z.cnt = sizeof(int) * std::max<int64_t>(hb.n_bins, 1);
     z.bsum = sizeof(int) * std::max<int64_t>(hb.scan_base.back(), 1);
     z.bmask = sizeof(uint64_t) * std::max<int64_t>(hb.blk_base.back(), 1);
@@ -81,8 +80,7 @@ ScratchSizes scratch_sizes(const HostBatch& hb) {
 
 dnni_status ensure_scratch(dnni_ctx* c, Scratch& s, const ScratchSizes& z, DevArrays& a) {
     dnni_status rs;
-    if ((rs = dnni_ensure(c, s.sorted, z.sorted)) || (rs = dnni_ensure(c, s.rank, z.rank)) ||
-        (rs = dnni_ensure(c, s.cnt, z.cnt)) || (rs = dnni_ensure(c, s.start, z.cnt)) ||
+    if ((rs = dnni_ensure(c, s.sorted, z.sorted)) || (rs = dnni_ensure(c, s.cnt, z.cnt)) || (rs = dnni_ensure(c, s.start, z.cnt)) ||
         (rs = dnni_ensure(c, s.bsum, z.bsum)) || (rs = dnni_ensure(c, s.bmask, z.bmask)) ||
         (rs = dnni_ensure(c, s.smask, z.smask)) || (rs = dnni_ensure(c, s.rownear, z.rownear)) ||
         (rs = dnni_ensure(c, s.near, z.near)) || (rs = dnni_ensure(c, s.pix, z.pix)) ||
@@ -91,7 +89,6 @@ dnni_status ensure_scratch(dnni_ctx* c, Scratch& s, const ScratchSizes& z, DevAr
         (rs = dnni_ensure(c, s.tables, z.tables)))
         return rs;
     a.sorted = (int4*)s.sorted.p;
-    a.rank = (int*)s.rank.p;
     a.cnt = (int*)s.cnt.p;
     a.start = (int*)s.start.p;
     a.bsum = (int*)s.bsum.p;
@@ -110,7 +107,7 @@ dnni_status ensure_scratch(dnni_ctx* c, Scratch& s, const ScratchSizes& z, DevAr
 }
 
 void release_scratch(dnni_ctx* c, Scratch& s) {
-    DevBuf* bufs[] = {&s.sorted, &s.rank, &s.cnt, &s.start, &s.bsum, &s.bmask, &s.smask, &s.rownear,
+    DevBuf* bufs[] = {&s.sorted, &s.list, &s.cnt, &s.start, &s.bsum, &s.bmask, &s.smask, &s.rownear,
                       &s.near, &s.pix, &s.far, &s.D, &s.Dc, &s.sc, &s.ctr, &s.tables};
     for (DevBuf* b : bufs) dnni_release(*b, c);
 }
@@ -166,12 +163,12 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     const int64_t nblk = hb.blk_base.back(), nsup = hb.sup_base.back();
     if (nchunk > 0) {
         cudaMemsetAsync(a.cnt, 0, sizeof(int) * hb.n_bins, st);
-        k_bin_count<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.cnt, a.rank, a.sc, a.ctr, bbox_in_count ? 1 : 0);
+        k_bin_count<<<nchunk, 256, 0, st>>>(bt, d_xyz, a.cnt, a.sc, a.ctr, bbox_in_count ? 1 : 0);
         const int nscan = hb.scan_base.back();
         k_scan_partial<<<nscan, kScanThreads, 0, st>>>(bt, a.cnt, a.bsum);
         k_scan_bsum<<<(int)hb.tiles.size(), 1024, 0, st>>>(bt, a.bsum);
         k_scan_final<<<nscan, kScanThreads, 0, st>>>(bt, a.cnt, a.bsum, a.start);
-        k_bin_scatter<<<nchunk, 256, 0, st>>>(bt, d_xyz, d_gid, a.start, a.rank, a.sorted);
+        k_bin_scatter<<<nchunk, 256, 0, st>>>(bt, d_xyz, d_gid, a.start, a.cnt, a.sorted);
         if (nblk > 0) k_block_masks<<<(int)((nblk * 32 + 255) / 256), 256, 0, st>>>(bt, a.start, a.bmask);
         if (nsup > 0) k_super_masks<<<(int)((nsup * 32 + 255) / 256), 256, 0, st>>>(bt, a.bmask, a.smask);
         const int nrow1 = hb.row1_base.back();
@@ -181,7 +178,7 @@ void launch_body(const HostBatch& hb, const BatchTables& bt, const DevArrays& a,
     if (ev) cudaEventRecord(ev[0], st);
     const int nrt = hb.rt_base.back();
     k_near_dense<<<nrt, dim3(32, 8), kDenseSmem, st>>>(bt, a.sorted, a.start, a.pix, d_site, a.far, a.sc, a.ctr,
-                                                       hb.far_blocks);
+                                                       hb.far_blocks, hb.dense_band);
     if (ev) cudaEventRecord(ev[4], st);
     if (nchunk > 0)
         k_near_far<<<sms * 6, 256, 0, st>>>(bt, a.sorted, a.start, a.bmask, a.smask, a.near, a.far, a.pix, d_site,
@@ -363,9 +360,11 @@ static dnni_status plan_batch(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
     const int bt_ = o.bin_target ? o.bin_target : c->s.bin_target;
     const int ww_ = o.span_window ? o.span_window : kSpanWindowWords;
     if (rs_ < 1 || rs_ > kMaxSmallRadius || bt_ < 0 || (ww_ != 1 && ww_ < 256) || ww_ > kSpanWindowMaxWords ||
-        o.far_group < 0 || o.far_group > 2)
+        o.far_group < 0 || o.far_group > 2 ||
+        (o.dense_band != 0 && o.dense_band != 8 && o.dense_band != 16 && o.dense_band != 32 && o.dense_band != 64))
         return set_err(c, DNNI_E_INVAL, "bad batch options");
     const int fb_ = o.far_group ? o.far_group - 1 : kFarBlocksDefault;
+    const int db_ = o.dense_band ? o.dense_band : kTileY;
     std::vector<TileParams> plan(ntiles);
     std::vector<int64_t> cost(ntiles);
     for (int k = 0; k < ntiles; ++k) {
@@ -404,6 +403,7 @@ static dnni_status plan_batch(dnni_ctx* c, const dnni_tile* tiles, int32_t ntile
     hb.rs = rs_;
     hb.win_words = ww_;
     hb.far_blocks = fb_;
+    hb.dense_band = db_;
     for (int k : order) batch_add(hb, plan[k], tiles[k].pt_offset, tiles[k].out_offset, tiles[k].site_offset);
     if (hb.too_big) return set_err(c, DNNI_E_INVAL, "batch too large for one launch sequence: split it");
     return DNNI_OK;
@@ -795,7 +795,6 @@ static dnni_status plan_slices(dnni_batch* b) {
             const HostBatch& h = sl.hb;
             DevArrays v = full;
             v.sorted += pts;
-            v.rank += pts;
             v.cnt += bins;
             v.start += bins;
             v.bsum += scan;
@@ -993,12 +992,13 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     std::vector<int> order;
     std::vector<dnni_tune_trial> trials;
     cudaStream_t st = c->stream;
-    auto trial = [&](int rs_, int bt_, int ww_, int fg_, float* ms) -> dnni_status {
+    auto trial = [&](int rs_, int bt_, int ww_, int fg_, int db_, float* ms) -> dnni_status {
         dnni_batch_options o = given;
         o.small_radius = rs_;
         o.bin_target = bt_;
         o.span_window = ww_;
         o.far_group = fg_;
+        o.dense_band = db_;
         dnni_status rs = plan_batch(c, smp.data(), m, o, hb, order);
         if (rs) return rs;
         if ((rs = ensure_scratch(c, tscr, scratch_sizes(hb), a))) return rs;
@@ -1015,7 +1015,7 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
         float t = 0;
         CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
         *ms = t / 2;
-        trials.push_back(dnni_tune_trial{rs_, bt_, *ms, ww_, fg_});
+        trials.push_back(dnni_tune_trial{rs_, bt_, *ms, ww_, fg_, db_});
         return DNNI_OK;
     };
     dnni_status rs = dnni_ensure(c, hbuf, sizeof(float) * std::max<int64_t>(out, 1));
@@ -1023,38 +1023,47 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     const int bt0 = given.bin_target ? given.bin_target : (c->s.bin_target ? c->s.bin_target : 4);
     const int ww0 = given.span_window ? given.span_window : kSpanWindowWords;
     const int fg0 = given.far_group ? given.far_group : kFarBlocksDefault + 1;
+    const int db0 = given.dense_band ? given.dense_band : kTileY;
     float ms_default = 0, best_ms = 0;
-    int best_rs = rs0, best_bt = bt0, best_ww = ww0, best_fg = fg0;
-    if (!rs) rs = trial(rs0, bt0, ww0, fg0, &ms_default);
+    int best_rs = rs0, best_bt = bt0, best_ww = ww0, best_fg = fg0, best_db = db0;
+    if (!rs) rs = trial(rs0, bt0, ww0, fg0, db0, &ms_default);
     best_ms = ms_default;
     // coordinate search: the bin size first, then the stencil/span split,
-    // the span path's shared-memory window, and the far pass's pixel groups
+    // the span path's shared-memory window, the far pass's pixel groups and
+    // the ring search's pixel-block shape
     static const int kBinTargets[] = {2, 3, 4, 6, 8, 12};
     static const int kRadii[] = {1, 2, 3, 4, 5, 6};
     static const int kWindows[] = {1, 2048, 4096, 8192, 12288};   // 1: no window
+    static const int kBands[] = {16, 32, 64};
     for (int bt_ : kBinTargets) {
         if (rs || bt_ == bt0) continue;
         float ms = 0;
-        rs = trial(rs0, bt_, ww0, fg0, &ms);
+        rs = trial(rs0, bt_, ww0, fg0, db0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_bt = bt_; }
     }
     for (int r_ : kRadii) {
         if (rs || r_ == rs0 || r_ > kMaxSmallRadius) continue;
         float ms = 0;
-        rs = trial(r_, best_bt, ww0, fg0, &ms);
+        rs = trial(r_, best_bt, ww0, fg0, db0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_rs = r_; }
     }
     for (int w_ : kWindows) {
         if (rs || w_ == ww0) continue;
         float ms = 0;
-        rs = trial(best_rs, best_bt, w_, fg0, &ms);
+        rs = trial(best_rs, best_bt, w_, fg0, db0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_ww = w_; }
     }
     for (int f_ = 1; f_ <= 2; ++f_) {
         if (rs || f_ == fg0) continue;
         float ms = 0;
-        rs = trial(best_rs, best_bt, best_ww, f_, &ms);
+        rs = trial(best_rs, best_bt, best_ww, f_, db0, &ms);
         if (!rs && ms < best_ms) { best_ms = ms; best_fg = f_; }
+    }
+    for (int d_ : kBands) {
+        if (rs || d_ == db0) continue;
+        float ms = 0;
+        rs = trial(best_rs, best_bt, best_ww, best_fg, d_, &ms);
+        if (!rs && ms < best_ms) { best_ms = ms; best_db = d_; }
     }
     release_scratch(c, tscr);
     dnni_release(hbuf, c);
@@ -1063,6 +1072,7 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     options->bin_target = best_bt;
     options->span_window = best_ww;
     options->far_group = best_fg;
+    options->dense_band = best_db;
     if (report) {
         memset(report, 0, sizeof(*report));
         report->ntrials = (int32_t)std::min<size_t>(trials.size(), 32);
@@ -1071,7 +1081,8 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
         for (int k = 0; k < report->ntrials; ++k) {
             report->trial[k] = trials[k];
             if (trials[k].small_radius == best_rs && trials[k].bin_target == best_bt &&
-                trials[k].span_window == best_ww && trials[k].far_group == best_fg)
+                trials[k].span_window == best_ww && trials[k].far_group == best_fg &&
+                trials[k].dense_band == best_db)
                 report->best = k;
         }
     }
@@ -1159,7 +1170,6 @@ bool carve_noalloc(unsigned char* base, const ScratchSizes& z, DevArrays& a) {
     a.D = (unsigned long long*)take(z.D);
     a.Dc = (int*)take(z.Dc);
     a.sorted = (int4*)take(z.sorted);
-    a.rank = (int*)take(z.rank);
     a.cnt = (int*)take(z.cnt);
     a.start = (int*)take(z.cnt);
     a.bsum = (int*)take(z.bsum);

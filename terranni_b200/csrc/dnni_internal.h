@@ -19,15 +19,15 @@ struct DevBuf {
     size_t cap = 0;
 };
 
-// Device scratch of one batch (or of the context's single work packages).
+// Device scratch of one batch (or of the context's single work packages);
+// `list` serves only the reference-default mode (its per-tile point lists).
 struct Scratch {
-    DevBuf sorted, rank, cnt, start, bsum, bmask, smask, rownear, near, pix, far, D, Dc, sc, ctr, tables;
+    DevBuf sorted, list, cnt, start, bsum, bmask, smask, rownear, near, pix, far, D, Dc, sc, ctr, tables;
 };
 
 // Raw device pointers of a scratch set for one launch sequence.
 struct DevArrays {
     int4* sorted = nullptr;
-    int* rank = nullptr;
     int* cnt = nullptr;
     int* start = nullptr;
     int* bsum = nullptr;

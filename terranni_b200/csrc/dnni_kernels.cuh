@@ -154,12 +154,13 @@ __device__ __forceinline__ int64_t point_bin_checked(const BinGrid& g, int xr, i
     return bin_id(g, bx, by);
 }
 
-// Counting-sort pass 1: per-bin counts; each point keeps its rank in its bin.
-// with_bbox: also the bounding box and range checks of k_bbox (batches,
-// whose bin grids are planned before any point is seen, skip k_bbox).
+// Counting-sort pass 1: per-bin counts, with reductions whose result is not
+// returned (no round trip per point).  with_bbox: also the bounding box and
+// range checks of k_bbox (batches, whose bin grids are planned before any
+// point is seen, skip k_bbox).
 __global__ void __launch_bounds__(256) k_bin_count(BatchTables bt, const int32_t* __restrict__ xyz,
-                                                   int* __restrict__ cnt, int* __restrict__ rank, Scalars* sc,
-                                                   BatchCounters* ctr, int with_bbox) {
+                                                   int* __restrict__ cnt, Scalars* sc, BatchCounters* ctr,
+                                                   int with_bbox) {
     const int t = find_tile(bt.chunk_base, bt.ntiles, blockIdx.x);
     const TileParams& T = bt.tiles[t];
     const int64_t c0 = (int64_t)(blockIdx.x - __ldg(&bt.chunk_base[t])) * kChunk;
@@ -172,27 +173,33 @@ __global__ void __launch_bounds__(256) k_bin_count(BatchTables bt, const int32_t
         const int xr = p[3 * i], yr = p[3 * i + 1];
         if (with_bbox) bbox_point(T, xr, yr, p[3 * i + 2], acc);
         const int64_t id = point_bin_checked(T.bg, rel_coord(xr, T.ox), rel_coord(yr, T.oy), bad);
-        rank[T.srt_off + i] = atomicAdd(&c[id], 1);
+        atomicAdd(&c[id], 1);
     }
     if (with_bbox) bbox_flush(acc, sc + t, ctr);
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&ctr->err, kErrRange);
 }
 
-// Counting-sort pass 3: place every point at start[bin] + rank.
+// Counting-sort pass 3: each point takes a slot of its bin by counting the
+// bin's count down (cnt ends at zero), at start[bin] + the count taken - 1.
+// The order of the points inside a bin is therefore arbitrary, which no
+// result depends on: every comparison of sites orders them by (distance,
+// gid, z), never by position.
 __global__ void __launch_bounds__(256) k_bin_scatter(BatchTables bt, const int32_t* __restrict__ xyz,
                                                      const uint32_t* __restrict__ gid, const int* __restrict__ start,
-                                                     const int* __restrict__ rank, int4* __restrict__ sorted) {
+                                                     int* __restrict__ cnt, int4* __restrict__ sorted) {
     const int t = find_tile(bt.chunk_base, bt.ntiles, blockIdx.x);
     const TileParams& T = bt.tiles[t];
     const int64_t c0 = (int64_t)(blockIdx.x - __ldg(&bt.chunk_base[t])) * kChunk;
     const int64_t c1 = c0 + kChunk < T.npts ? c0 + kChunk : T.npts;
     const int32_t* p = xyz + 3 * T.pt_off;
     const int* st = start + T.bin_off;
+    int* c = cnt + T.bin_off;
     int4* out = sorted + T.srt_off;
     unsigned bad = 0;
     for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
         const int xr = rel_coord(p[3 * i], T.ox), yr = rel_coord(p[3 * i + 1], T.oy);
-        const int pos = st[point_bin_checked(T.bg, xr, yr, bad)] + rank[T.srt_off + i];
+        const int64_t id = point_bin_checked(T.bg, xr, yr, bad);
+        const int pos = st[id] + atomicSub(&c[id], 1) - 1;
         const uint32_t g = gid ? gid[T.pt_off + i] : (uint32_t)i;
         out[pos] = make_int4(xr, yr, p[3 * i + 2], (int)g);
     }
@@ -467,7 +474,7 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
                                                        const int* __restrict__ start_all, int2* __restrict__ pix,
                                                        uint32_t* __restrict__ site, FarSlot* __restrict__ far,
                                                        Scalars* __restrict__ sc, BatchCounters* __restrict__ ctr,
-                                                       int far_blocks) {
+                                                       int far_blocks, int band0) {
     extern __shared__ int4 smem[];
     int4* s_pts = smem;
     int* s_lstart = (int*)(smem + kWinMaxPts);
@@ -485,10 +492,12 @@ __global__ void __launch_bounds__(256, 4) k_near_dense(BatchTables bt, const int
     const int i0 = (lt % ntx) * kTileX, j0 = (lt / ntx) * kTileY;
     const int i = i0 + threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    // the tile's rows go in bands, each with its own staged window: the whole
-    // tile when its window fits shared memory, else halves, down to 8 rows
+    // the tile's rows go in bands, each with its own staged window: band0
+    // rows (8, 16, 32 or 64: the shape of the pixel block that shares one
+    // window, a tuning choice) when that window fits shared memory, else
+    // halves, down to 8 rows
     StatAcc acc;
-    int band = kTileY;
+    int band = band0;
     for (int jb = 0; jb < kTileY && j0 + jb < T.rh; jb += band) {
     int wx0 = 0, wy0 = 0, wnx = 0, wny = 0;
     bool staged = false;
@@ -757,7 +766,7 @@ __device__ __forceinline__ uint64_t chord_mask8_32(bool act, int rx, int ry, uns
             const int y0 = r * u, y1 = y0 + u - 1;
             const int gy = ry < y0 ? y0 - ry : (ry > y1 ? ry - y1 : 0);
             if (gy <= 46340 && (unsigned)(gy * gy) <= d2) {
-                const int w = (int)sqrtf((float)(d2 - (unsigned)(gy * gy))) + 1;
+                const int w = (int)sqrt_est((float)(d2 - (unsigned)(gy * gy))) + 1;
                 const int lo = rx - w, hi = rx + w;
                 if (hi >= 0 && lo < 8 * u) {
                     a = lo <= 0 ? 0 : floor_div8(lo, u, inv_u);
@@ -1120,14 +1129,15 @@ __global__ void __launch_bounds__(256) k_scatter_window(BatchTables bt, const in
             // markers on a common row often fall on one cell (same-address
             // atomics serialise); each lane starts its rows at its own offset
             // so that the warp's markers spread over the chunk's rows.  The
-            // half-width floor(sqrt(t2)) comes from a float square root,
-            // within one of it for t2 < 2^31, and one exact step each way.
+            // half-width floor(sqrt(t2)) comes from the hardware square-root
+            // estimate, within one of it for t2 < 2^31, and one exact step
+            // each way.
             const int nrow = yb - ya + 1;
             int y = ya + (int)(threadIdx.x % (unsigned)nrow);
             for (int k = 0; k < nrow; ++k, y = (y == yb) ? ya : y + 1) {
                 const int dy = y - py;
                 const unsigned t2 = R2 - (unsigned)(dy * dy);
-                unsigned w = (unsigned)sqrtf((float)t2);
+                unsigned w = (unsigned)sqrt_est((float)t2);
                 w -= (w * w > t2) ? 1u : 0u;
                 w += ((w + 1) * (w + 1) <= t2) ? 1u : 0u;
                 const int a = max(px - (int)w, 0), b = px + (int)w + 1;

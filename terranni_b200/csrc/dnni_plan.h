@@ -127,6 +127,7 @@ struct HostBatch {
     int rs = 3;                          // stencil radius shared by the batch
     int win_words = kSpanWindowWords;    // shared-memory words of the span window per CTA
     int far_blocks = kFarBlocksDefault;  // far groups: 1 = 8 x 4 pixel blocks, 0 = 32 x 1 rows
+    int dense_band = kTileY;             // ring search: pixel rows of a 32-wide band sharing one staged window
     bool too_big = false;                // a launch index or the far worklist would pass int32
 };
 

@@ -112,9 +112,26 @@ struct Scalars {
 // small device helpers
 // ---------------------------------------------------------------------------
 
+#ifdef __CUDACC__
+// Square-root estimate of a non-negative float from the hardware
+// approximation (PTX sqrt.approx.ftz.f32; relative error a few units of
+// 2^-23), for callers that correct the result with exact integer products or
+// need it only within a fraction of one unit (below 2^31 the absolute error
+// stays under 0.05).
+__device__ __forceinline__ float sqrt_est(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+#endif
+
 DNNI_HD int isqrt_i32(int v) {
     // floor(sqrt(v)) for 0 <= v < 2^31: float estimate, exact integer fix-up
+#ifdef __CUDA_ARCH__
+    int s = (int)sqrt_est((float)v);
+#else
     int s = (int)sqrtf((float)v);
+#endif
     while ((long long)s * s > v) --s;
     while ((long long)(s + 1) * (s + 1) <= v) ++s;
     return s;

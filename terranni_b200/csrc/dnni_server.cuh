@@ -218,7 +218,7 @@ size_t srv_footprint(const HostBatch& hb, int64_t pts, int64_t out, int64_t site
     const ScratchSizes z = scratch_sizes(hb);
     size_t b = al256(12 * (size_t)pts) + al256(4 * (size_t)pts) + al256(4 * (size_t)out) + al256(4 * (size_t)site) +
                al256(sizeof(SegChunk) * nchunks);
-    const size_t parts[] = {z.tables, z.sc, z.ctr, z.pix, z.far, z.D, z.Dc, z.sorted, z.rank, z.cnt, z.cnt, z.bsum,
+    const size_t parts[] = {z.tables, z.sc, z.ctr, z.pix, z.far, z.D, z.Dc, z.sorted, z.cnt, z.cnt, z.bsum,
                             z.bmask, z.smask, z.rownear, z.near};
     for (size_t p : parts) b += al256(p);
     return b;
@@ -262,7 +262,6 @@ dnni_status srv_launch(dnni_server* s, SrvSlot& sl, std::vector<SrvItem>& items,
     a.D = (unsigned long long*)take(z.D);
     a.Dc = (int*)take(z.Dc);
     a.sorted = (int4*)take(z.sorted);
-    a.rank = (int*)take(z.rank);
     a.cnt = (int*)take(z.cnt);
     a.start = (int*)take(z.cnt);
     a.bsum = (int*)take(z.bsum);

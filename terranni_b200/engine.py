@@ -80,7 +80,8 @@ class Tile(ctypes.Structure):
 class BatchOptions(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32), ("order_by_cost", ctypes.c_int32),
-                ("span_window", ctypes.c_int32), ("far_group", ctypes.c_int32)]
+                ("span_window", ctypes.c_int32), ("far_group", ctypes.c_int32),
+                ("dense_band", ctypes.c_int32)]
 
 
 class Segment(ctypes.Structure):
@@ -177,7 +178,7 @@ class Peaks(ctypes.Structure):
 
 class TuneTrial(ctypes.Structure):
     _fields_ = [("small_radius", ctypes.c_int32), ("bin_target", ctypes.c_int32), ("ms", ctypes.c_float),
-                ("span_window", ctypes.c_int32), ("far_group", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("span_window", ctypes.c_int32), ("far_group", ctypes.c_int32), ("dense_band", ctypes.c_int32)]
 
 
 class TuneReport(ctypes.Structure):
@@ -187,7 +188,7 @@ class TuneReport(ctypes.Structure):
     def as_dict(self):
         t = [{"small_radius": self.trial[k].small_radius, "bin_target": self.trial[k].bin_target,
               "span_window": self.trial[k].span_window, "far_group": self.trial[k].far_group,
-              "ms": self.trial[k].ms} for k in range(self.ntrials)]
+              "dense_band": self.trial[k].dense_band, "ms": self.trial[k].ms} for k in range(self.ntrials)]
         return {"sample_tiles": self.sample_tiles, "ms_default": self.ms_default,
                 "best": t[self.best] if t else None, "trials": t}
 
@@ -398,20 +399,22 @@ class Engine:
         return st
 
     def batch(self, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False, span_window=0,
-              far_group=0):
+              far_group=0, dense_band=0):
         """Plans a batch of tiles (dnni_batch_create) -> Batch."""
-        return Batch(self, tiles, small_radius, bin_target, use_graph, order_by_cost, span_window, far_group)
+        return Batch(self, tiles, small_radius, bin_target, use_graph, order_by_cost, span_window, far_group,
+                     dense_band)
 
     def autotune(self, tiles, d_xyz, d_gid=None, sample_tiles=256, small_radius=0, bin_target=0, span_window=0,
-                 far_group=0):
-        """dnni_batch_autotune -> (dict(small_radius, bin_target, span_window), report dict)."""
+                 far_group=0, dense_band=0):
+        """dnni_batch_autotune -> (dict of the chosen batch options, report dict)."""
         arr = (Tile * len(tiles))(*tiles)
-        opt = BatchOptions(int(small_radius), int(bin_target), 0, 0, int(span_window), int(far_group))
+        opt = BatchOptions(int(small_radius), int(bin_target), 0, 0, int(span_window), int(far_group),
+                           int(dense_band))
         rep = TuneReport()
         self._check(lib().dnni_batch_autotune(self._h, arr, len(tiles), _ptr(d_xyz), _ptr(d_gid), int(sample_tiles),
                                               ctypes.byref(opt), ctypes.byref(rep)))
         return ({"small_radius": opt.small_radius, "bin_target": opt.bin_target, "span_window": opt.span_window,
-                 "far_group": opt.far_group}, rep.as_dict())
+                 "far_group": opt.far_group, "dense_band": opt.dense_band}, rep.as_dict())
 
     def segment_run(self, xyz, ncols, nrows, cell_size, origin=(0, 0), tile=0, halo=0, tiles_per_batch=0,
                     z_scale=0.01, z_offset=0.0, nodata=-9999.0, small_radius=0, site=False, out_h=None, part=0,
@@ -473,11 +476,11 @@ class Batch:
     """A planned batch of tiles (dnni_batch); runs many times."""
 
     def __init__(self, eng: Engine, tiles, small_radius=0, bin_target=0, use_graph=False, order_by_cost=False,
-                 span_window=0, far_group=0):
+                 span_window=0, far_group=0, dense_band=0):
         self._eng = eng
         arr = (Tile * len(tiles))(*tiles)
         opt = BatchOptions(int(small_radius), int(bin_target), int(bool(use_graph)), int(bool(order_by_cost)),
-                           int(span_window), int(far_group))
+                           int(span_window), int(far_group), int(dense_band))
         h = _P()
         eng._check(lib().dnni_batch_create(eng.handle, arr, len(tiles), ctypes.byref(opt), ctypes.byref(h)))
         self._h = h

@@ -207,6 +207,32 @@ def test_autotuned_options_give_the_same_heights(eng):
     with eng.batch(tiles, use_graph=True, **opts) as b:
         h, s, _ = _run_device(b, xyz, nout, nsite)
     _check(meta, ref, h, s)
+    assert opts["dense_band"] in (16, 32, 64)
+    assert {t["dense_band"] for t in rep["trials"]} == {16, 32, 64}
+
+
+@pytest.mark.parametrize("dense_band,far_group", [(8, 2), (16, 1), (32, 2)])
+def test_ring_search_block_shapes_give_the_same_result(eng, dense_band, far_group):
+    """The ring search's pixel block (32 x dense_band pixels per staged bin
+    window) is a tuning choice: every shape gives the per-tile result bit for
+    bit, dense tiles included (a 200 x 200 tile at 8 points per cell, whose
+    64-row windows do not fit in shared memory)."""
+    from terranni_b200 import engine
+    cases = _tiles(seed=31, count=8)
+    dense = terrain_case(4242, 200, 320_000, lakes=2, lake_r=(10.0, 40.0))
+    cases.insert(0, {"wp": engine.make_wp(200, 200, 100, raster=(-3, -3, 203, 203)), "xyz": dense})
+    xyz, tiles, meta, nout, nsite = _layout(cases)
+    ref = _per_tile(eng, xyz, meta)
+    with eng.batch(tiles, use_graph=True, dense_band=dense_band, far_group=far_group) as b:
+        h, s, _ = _run_device(b, xyz, nout, nsite)
+    _check(meta, ref, h, s)
+
+
+def test_bad_ring_search_block_shape_is_refused(eng):
+    from terranni_b200 import engine
+    xyz, tiles, meta, nout, nsite = _layout(_tiles(seed=5, count=2), share_rows=False)
+    with pytest.raises(engine.DnniError):
+        eng.batch(tiles, dense_band=24)
 
 
 @pytest.mark.parametrize("reverse_out,ntiles", [(False, 20), (True, 20), (False, 6)])
