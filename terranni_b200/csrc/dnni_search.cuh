@@ -661,8 +661,25 @@ DNNI_HD int64_t block_index(const BinGrid& g, int cx, int cy) {
     return ((int64_t)((cy >> 3) * g.n2x + (cx >> 3)) << 6) + (((cy & 7) << 3) | (cx & 7));
 }
 
-// A first bound from the nearest non-empty block map: the points of the bin
-// of block `nb` (in bmask order) whose box is closest to the pixel.
+// 8 x 8 mask of the cells [a0,a1] x [b0,b1] of a block (x = bit & 7,
+// y = bit >> 3), clipped to the block; 0 when the range is empty.
+DNNI_HD uint64_t cell_box_mask8(int a0, int a1, int b0, int b1) {
+    a0 = a0 > 0 ? a0 : 0;
+    b0 = b0 > 0 ? b0 : 0;
+    a1 = a1 < 7 ? a1 : 7;
+    b1 = b1 < 7 ? b1 : 7;
+    if (a0 > a1 || b0 > b1) return 0;
+    const uint64_t row = (0xFFull >> (7 - a1 + a0)) << a0;
+    return (row * 0x0101010101010101ull) & (~0ull >> (8 * (7 - b1))) & (~0ull << (8 * b0));
+}
+
+// A first bound from the nearest non-empty block map: the points of a
+// non-empty bin of block `nb` (in bmask order) close to the pixel.  The
+// pixel's cell in the block (clamped to the block) is the centre of square
+// rings of bins; the first ring that holds a non-empty bin gives the
+// candidates, and the one whose box is closest to the pixel is scanned.  Any
+// non-empty bin gives a real site, so the search stays exact; a near one
+// keeps the disc that the search then walks small.
 DNNI_HD void seed_from_block(const BinGrid& g, const int4* __restrict__ pts, const int* __restrict__ start,
                              const uint64_t* __restrict__ bmask, int64_t nb, int px, int py, Best& b) {
     const long long bs = g.bs, u1 = bs * kBinsPerBlockEdge, u2 = bs * kBinsPerSuperEdge;
@@ -670,12 +687,17 @@ DNNI_HD void seed_from_block(const BinGrid& g, const int4* __restrict__ pts, con
     const int m = (int)(nb & 63);
     const long long BX0 = g.gx0 + (long long)(sidx % g.n2x) * u2 + (long long)(m & 7) * u1;
     const long long BY0 = g.gy0 + (long long)(sidx / g.n2x) * u2 + (long long)(m >> 3) * u1;
-    uint64_t bm = DNNI_LDG(&bmask[nb]);
+    const uint64_t bm = DNNI_LDG(&bmask[nb]);
+    const long long dx = (long long)px - BX0, dy = (long long)py - BY0;
+    const int cx = dx < 0 ? 0 : (dx >= u1 ? 7 : udiv32(dx, bs));
+    const int cy = dy < 0 ? 0 : (dy >= u1 ? 7 : udiv32(dy, bs));
+    uint64_t hit = 0;
+    for (int r = 0; r < 8 && !hit; ++r) hit = bm & cell_box_mask8(cx - r, cx + r, cy - r, cy + r);
     long long qlb = LLONG_MAX;
     int q_idx = 0;
-    while (bm) {
-        const int l = ffs64(bm);
-        bm &= bm - 1;
+    while (hit) {
+        const int l = ffs64(hit);
+        hit &= hit - 1;
         const long long QX0 = BX0 + (long long)(l & 7) * bs, QY0 = BY0 + (long long)(l >> 3) * bs;
         const long long lb = box_lb(px, py, QX0, QX0 + bs - 1, QY0, QY0 + bs - 1);
         if (lb < qlb) { qlb = lb; q_idx = l; }
