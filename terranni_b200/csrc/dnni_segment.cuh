@@ -407,7 +407,6 @@ dnni_status segment_run(dnni_ctx* c, const dnni_segment& s, const int32_t* h_xyz
     cudaStream_t st = c->stream;
     const int nbx = (s.ncols + kSegBucketCells - 1) / kSegBucketCells;
     const int nby = (s.nrows + kSegBucketCells - 1) / kSegBucketCells;
-    const int nb = nbx * nby;
     const SegGrid G{s.origin_x, s.origin_y, (long long)kSegBucketCells * s.cell_size, nbx, nby};
     dnni_status rs;
     std::vector<long long> start;

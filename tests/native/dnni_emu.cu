@@ -250,6 +250,11 @@ extern "C" int emu_interpolate(const dnni_workpackage* wp, const int32_t* xyz, c
 // exposes the device helpers r2_of and udiv32 for direct tests
 extern "C" int emu_r2_of(long long d2, long long cs2, int cap) { return r2_of(d2, cs2, cap); }
 
+// exposes the block cell-box mask that the far pass's seed uses
+extern "C" unsigned long long emu_cell_box_mask8(int a0, int a1, int b0, int b1) {
+    return cell_box_mask8(a0, a1, b0, b1);
+}
+
 // exposes the planning distance transform used for the segment driver's halos
 extern "C" void emu_edt_2d(const unsigned char* occ, int nx, int ny, double* out) {
     const std::vector<double> g = edt_2d(occ, nx, ny);

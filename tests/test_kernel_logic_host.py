@@ -109,6 +109,22 @@ def test_host_build_window_fallbacks(emu, oracle, k):
     assert rc == 0 and np.array_equal(r["site"], ref["site"]) and _same(r["h"], ref["h"])
 
 
+def test_cell_box_mask_matches_cell_by_cell(emu):
+    # the seed of a far pixel takes the non-empty bins of square rings of a
+    # block's 8 x 8 bins: every clipped range, including empty ones
+    import ctypes, itertools, os
+    L = ctypes.CDLL(os.path.join(os.path.dirname(__file__), "native", "libdnni_emu.so"))
+    L.emu_cell_box_mask8.argtypes = [ctypes.c_int] * 4
+    L.emu_cell_box_mask8.restype = ctypes.c_ulonglong
+    for a0, a1, b0, b1 in itertools.product(range(-9, 17, 2), range(-3, 12), range(-9, 17, 2), range(-3, 12)):
+        want = 0
+        for y in range(8):
+            for x in range(8):
+                if a0 <= x <= a1 and b0 <= y <= b1:
+                    want |= 1 << (8 * y + x)
+        assert L.emu_cell_box_mask8(a0, a1, b0, b1) == want, (a0, a1, b0, b1)
+
+
 def test_r2_of_is_exact_floor_division():
     import ctypes, os
     L = ctypes.CDLL(os.path.join(os.path.dirname(__file__), "native", "libdnni_emu.so"))
