@@ -1031,7 +1031,7 @@ dnni_status dnni_batch_autotune(dnni_ctx* c, const dnni_tile* tiles, int32_t nti
     // coordinate search: the bin size first, then the stencil/span split,
     // the span path's shared-memory window, the far pass's pixel groups and
     // the ring search's pixel-block shape
-    static const int kBinTargets[] = {2, 3, 4, 6, 8, 12};
+    static const int kBinTargets[] = {1, 2, 3, 4, 6, 8, 12};
     static const int kRadii[] = {1, 2, 3, 4, 5, 6};
     static const int kWindows[] = {1, 2048, 4096, 8192, 12288};   // 1: no window
     static const int kBands[] = {16, 32, 64};
