@@ -128,3 +128,36 @@ def test_pinned_host_allocation():
     buf[0], buf[(1 << 20) - 1] = 7, 9
     assert buf[0] == 7 and buf[(1 << 20) - 1] == 9
     assert L.dnni_host_free(p) == 0
+
+
+def test_python_binding_layouts_match_the_header(tmp_path):
+    # every ctypes structure of the binding has the size and field offsets of
+    # the C struct it stands for (a C99 program prints offsetof/sizeof)
+    import subprocess
+    from terranni_b200 import engine
+    pairs = {"Settings": "dnni_settings", "WorkPackage": "dnni_workpackage", "Stats": "dnni_stats",
+             "Tile": "dnni_tile", "BatchOptions": "dnni_batch_options", "Segment": "dnni_segment",
+             "SegmentStats": "dnni_segment_stats", "ServerOptions": "dnni_server_options",
+             "Request": "dnni_request", "RequestResult": "dnni_request_result", "ServerStats": "dnni_server_stats",
+             "LasHeader": "dnni_las_header", "CompatSettings": "dnni_compat_settings", "StOptions": "dnni_st_options",
+             "CompatWP": "dnni_compat_wp", "Peaks": "dnni_peaks", "TuneTrial": "dnni_tune_trial",
+             "TuneReport": "dnni_tune_report"}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", "#include \"dnni.h\"", "int main(void) {"]
+    want = []
+    for py, c in pairs.items():
+        cls = getattr(engine, py)
+        lines.append(f"    printf(\"%zu\\n\", sizeof({c}));")
+        want.append((f"sizeof {c}", ctypes.sizeof(cls)))
+        for name, *_ in cls._fields_:
+            lines.append(f"    printf(\"%zu\\n\", offsetof({c}, {name}));")
+            want.append((f"{c}.{name}", getattr(cls, name).offset))
+    lines.append("    return 0;\n}\n")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True, text=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert len(got) == len(want)
+    bad = [(k, g, w) for (k, w), g in zip(want, got) if g != w]
+    assert not bad, bad
