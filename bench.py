@@ -162,6 +162,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def host_cpu():
+    """The host's CPU model and logical core count, for the CPU baselines."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
 def dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -186,7 +200,7 @@ def cpu_baseline(xyz, side, window, seed_note):
     t0 = time.perf_counter()
     oracle.interpolate(wp, sub)
     dt = time.perf_counter() - t0
-    return {"value": window * window / dt, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": window * window / dt, "unit": UNIT, "cores": 1, "kind": "port", "host": host_cpu(),
             "sample": f"{window}x{window}-cell lower-left window ({sub.shape[0]} points) of the {seed_note}; "
                       f"single-thread C oracle (k-d tree nearest site + row-span scatter), {dt:.2f} s"}
 
@@ -319,7 +333,8 @@ def run_reference_tile4096(args, world, rank):
         "warmup": args.warmup, "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
         "config": {"workload": "tile4096", "side": args.side, "points": args.points, "cell_m": 1.0},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "host": host_cpu(),
+                         "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -524,7 +539,7 @@ def cpu_baseline_mixed(w, h_gpu, budget_s):
     e = np.concatenate(errs) if errs else np.zeros(1)
     acc = {"tiles_checked": ntile, "cells_checked": cells, "bit_exact_vs_oracle": exact,
            "max_abs_err_m": float(e.max(initial=0.0)), "rms_err_m": float(np.sqrt(np.mean(e * e)))}
-    base = {"value": cells / spent, "unit": UNIT, "cores": 1, "kind": "port",
+    base = {"value": cells / spent, "unit": UNIT, "cores": 1, "kind": "port", "host": host_cpu(),
             "sample": f"{ntile} tiles ({cells} cells) of the same batch in a fixed stride order, "
                       f"single-thread C oracle (k-d tree nearest site + row-span scatter), {spent:.1f} s"}
     return base, acc
@@ -573,7 +588,8 @@ def run_reference_mixed(args, world, rank):
         "warmup": args.warmup, "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
         "config": {"workload": f"mixed{args.tiles}", "tiles": args.tiles, "sample_tiles": len(sample)},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "host": host_cpu(),
+                         "sample": desc},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
